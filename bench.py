@@ -1,0 +1,371 @@
+#!/usr/bin/env python
+"""Benchmark of the all-pairs softened gravity path on B200.
+
+Workload (the single-large-system configuration): Plummer sphere, N = 262144,
+seed 2, eps = 1e-3, KDK leapfrog dt = 5e-4, FP32-compensated pair arithmetic.
+A "step" is one leapfrog step = one force evaluation (N(N-1) ordered pairs)
+plus the fused kick/drift.  Metric: GPairs/s = pairs evaluated / device time.
+
+Output: ONE JSON line on stdout (rank 0).  Keys beyond the base contract:
+  roofline      the force kernel against the FP32 FMA-pipe roofline
+                (16 FMA-pipe operations per pair, 128 FP32 lanes per SM);
+  cpu_baseline  the reference's own CPU kernel on this host's cores;
+  fp64          the FP64 drop-in kernel's GPairs/s in the same run;
+  accuracy      FP32C vs FP64 per-particle force error and energy drift;
+  e2e           the same metric through the C ABI with host buffers
+                (upload, one step, download per step);
+  clocks        nvidia-smi samples taken during the timed region.
+
+--impl reference times the reference's CPU implementation instead (rank 0).
+--gpus N (under torchrun) shards the receivers of the one system over N GPUs
+with an NCCL all-gather of positions per step.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "n-body-ring-solver_b200")
+ORACLE = os.path.join(ROOT, "oracle")
+sys.path.insert(0, PKG)
+
+METRIC = "GPairs/s FP32-compensated vs FP64 on 1 B200 at median force rel err <=1e-6"
+UNIT = "GPairs/s"
+SMS = 148
+FMA_OPS_PER_PAIR = 16
+PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "force_fp32c_plummer262144.json")
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--n", type=int, default=262144)
+    p.add_argument("--seed", type=int, default=2)
+    p.add_argument("--eps", type=float, default=1e-3)
+    p.add_argument("--dt", type=float, default=5e-4)
+    p.add_argument("--precision", choices=["fp32c", "fp64"], default="fp32c")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-accuracy", action="store_true")
+    return p.parse_args()
+
+
+def workload_config(a, extra=None):
+    cfg = {"workload": f"plummer_n{a.n}_seed{a.seed}_eps{a.eps:g}_kdk_dt{a.dt:g}",
+           "n": a.n, "ic": "plummer", "seed": a.seed, "eps": a.eps, "dt": a.dt,
+           "scheme": "kdk", "pairs_per_step": a.n * (a.n - 1),
+           "l2": "flushed between timed steps (256 MiB write); j-stream 12.6 MB is L2-resident within a step"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+# ------------------------------------------------------------------ clocks --
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [t.strip() for t in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        loaded = [v for v in sm if v >= 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(mx), "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+# ------------------------------------------------------------ CPU baseline --
+def cpu_reference_sample(n, seed, target_s, max_s):
+    """The reference's fastest CPU force kernel (AVX-512 rsqrt 4i, or AVX2
+    blocked on a host without AVX-512) on this host's cores, on rank 0's share
+    of its own ring decomposition (hybrid_ring_solver) of one N-particle force
+    evaluation: N(N-1)/comm_sz effective pairs per share.  comm_sz is the
+    smallest power of two whose share takes at most target_s."""
+    sys.path.insert(0, ORACLE)
+    import nbr
+    from oracle import Reference, reference_available
+    if not reference_available():
+        return None
+    ref = Reference()
+    ref.set_threads(os.cpu_count() or 1)
+    s = nbr.plummer(n, seed)
+    # calibrate on a small share
+    comm = 1
+    while comm < n and n % (comm * 2) == 0 and comm < 256:
+        comm *= 2
+    t = ref.ring_share(s, comm)
+    while comm > 1 and t * 2 <= target_s:
+        comm //= 2
+        t = ref.ring_share(s, comm)
+    reps, total, pairs = 0, 0.0, 0.0
+    while total < target_s and total + t <= max_s or reps == 0:
+        tt = ref.ring_share(s, comm)
+        total += tt
+        pairs += n * (n - 1) / comm
+        reps += 1
+        if total >= target_s:
+            break
+    kernel = "AVX512-RSQRT-4I" if ref.has_avx512 else "AVX2-blocked"
+    return {"value": pairs / total / 1e9, "unit": UNIT, "cores": ref.threads(), "kind": "reference",
+            "seconds": total,
+            "sample": f"{reps} x rank-0 share (1/{comm}) of one N={n} force evaluation of the reference's "
+                      f"{kernel} kernel (ring decomposition of hybrid_ring_solver, eps=0, FP64), "
+                      f"{ref.threads()} OpenMP threads"}
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sys.path.insert(0, ORACLE)
+    from oracle import reference_available
+    if not reference_available():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "reference CPU solver (oracle/_ref) was not built here"}))
+        return
+    import nbr
+    from oracle import Reference
+    ref = Reference()
+    ref.set_threads(os.cpu_count() or 1)
+    n = a.n
+    s = nbr.plummer(n, a.seed)
+    # per-step budget so that warmup + steps end within about two minutes
+    per_step = min(3.0, 120.0 / max(1, a.steps + a.warmup))
+    comm = 1
+    while comm < n and n % (comm * 2) == 0 and comm < 1024:
+        comm *= 2
+    t = ref.ring_share(s, comm)
+    while comm > 1 and t * 2 <= per_step:
+        comm //= 2
+        t = ref.ring_share(s, comm)
+    for _ in range(a.warmup):
+        ref.ring_share(s, comm)
+    secs = [ref.ring_share(s, comm) for _ in range(a.steps)]
+    total = sum(secs)
+    pairs = a.steps * n * (n - 1) / comm
+    value = pairs / total / 1e9
+    kernel = "AVX512-RSQRT-4I" if ref.has_avx512 else "AVX2-blocked"
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * total / a.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": workload_config(a, {"reference_kernel": kernel,
+                                                               "comm_sz": comm}),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": ref.threads(), "kind": "reference",
+                             "sample": f"each step: rank-0 share (1/{comm}) of one N={n} force evaluation "
+                                       f"of the reference's {kernel} kernel (hybrid_ring_solver's ring "
+                                       f"decomposition), eps=0 FP64, {ref.threads()} threads"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# -------------------------------------------------------------------- ours --
+def profile_traffic():
+    try:
+        with open(PROFILE_SUMMARY) as f:
+            return json.load(f).get("dram_bytes_per_launch")
+    except (OSError, ValueError):
+        return None
+
+
+def run_ours(a):
+    import numpy as np
+    import torch
+    import nbr
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        return run_sharded(a, rank, world, local)
+    torch.cuda.set_device(local)
+    prec = nbr.FP32C if a.precision == "fp32c" else nbr.FP64
+    eps2 = a.eps * a.eps
+    n = a.n
+    pairs = float(n) * float(n - 1)
+    s = nbr.plummer(n, a.seed)
+    ctx = nbr.Context(local)
+    ctx.upload(s)
+    ext = torch.cuda.ExternalStream(ctx.stream)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")
+
+    def l2_flush():
+        flush.zero_()
+        torch.cuda.synchronize()
+
+    def time_kernel(p, launches):
+        ctx.forces_device(p, eps2=eps2)  # pack + warm
+        ctx.forces_device(p, eps2=eps2)
+        ctx.synchronize()
+        ts = []
+        for _ in range(launches):
+            l2_flush()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(ext)
+            ctx.forces_device(p, eps2=eps2)
+            e1.record(ext)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1) * 1e-3)
+        return ts
+
+    # ---- kernel-level timing (roofline) for both precisions
+    k32 = time_kernel(nbr.FP32C, 5)
+    a32 = ctx.forces_download()
+    k64 = time_kernel(nbr.FP64, 3)
+    a64 = ctx.forces_download()
+    num = np.linalg.norm(a32 - a64, axis=0)
+    den = np.linalg.norm(a64, axis=0)
+    rel = num / np.where(den > 0, den, 1.0)
+
+    # ---- timed leapfrog steps
+    ctx.upload(s)
+    d0 = ctx.diagnostics(eps2=eps2)
+    for _ in range(a.warmup):
+        ctx.run(prec, nbr.KDK, 2, a.dt, 1, eps2=eps2)
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.5)
+    step_s, launches = [], 0
+    torch.cuda.synchronize()
+    t_wall0 = time.perf_counter()
+    for _ in range(a.steps):
+        l2_flush()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        st = ctx.run(prec, nbr.KDK, 2, a.dt, 1, eps2=eps2)
+        e1.record(ext)
+        e1.synchronize()
+        step_s.append(e0.elapsed_time(e1) * 1e-3)
+        launches += int(st["kernels"])
+        assert st["force_evals"] == 1
+    torch.cuda.synchronize()
+    t_wall = time.perf_counter() - t_wall0
+    clk = clocks.stop()
+    d1 = ctx.diagnostics(eps2=eps2)
+    t_total = sum(step_s)
+    value = a.steps * pairs / t_total / 1e9
+
+    # ---- energy drift of the same number of steps in FP64 (comparison)
+    acc = {"fp32c_vs_fp64_force_median_rel_err": float(np.median(rel)),
+           "fp32c_vs_fp64_force_max_rel_err": float(rel.max()),
+           "energy_drift": abs(d1["E"] - d0["E"]) / abs(d0["E"]),
+           "energy_drift_steps": a.warmup + a.steps}
+    if not a.no_accuracy and prec == nbr.FP32C:
+        ctx.upload(s)
+        for _ in range(a.warmup + a.steps):
+            ctx.run(nbr.FP64, nbr.KDK, 2, a.dt, 1, eps2=eps2)
+        d64 = ctx.diagnostics(eps2=eps2)
+        acc["energy_drift_fp64"] = abs(d64["E"] - d0["E"]) / abs(d0["E"])
+
+    # ---- end to end through the C ABI with pinned host buffers
+    host = {k: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy() for k in nbr.KEYS}
+    for k in nbr.KEYS:
+        host[k][:] = s[k]
+    e2e_s = []
+    for i in range(a.warmup + a.steps):
+        l2_flush()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        ctx.upload_raw(n, *[host[k] for k in nbr.KEYS])
+        st = ctx.run(prec, nbr.DKD, 2, a.dt, 1, eps2=eps2)
+        ctx.download_raw(*[host[k] for k in nbr.KEYS[:6]])
+        e1.record(ext)
+        e1.synchronize()
+        if i >= a.warmup:
+            e2e_s.append(e0.elapsed_time(e1) * 1e-3)
+            launches += 0
+    e2e_value = a.steps * pairs / sum(e2e_s) / 1e9
+
+    # ---- roofline of the force kernel
+    t_k = statistics.mean(k32)
+    achieved = pairs / t_k / 1e9
+    mhz = clk.get("sm_mhz") or 1965.0
+    peak = SMS * 128 * mhz * 1e6 / FMA_OPS_PER_PAIR / 1e9
+    roofline = {"bound": "fp32_fma_pipe", "achieved": achieved, "peak": peak, "unit": UNIT,
+                "frac": achieved / peak, "traffic": profile_traffic(),
+                "peak_source": "148 SMs x 128 FP32 lanes x median SM clock sampled in the timed region "
+                               "/ 16 FMA-pipe ops per pair (MEASURED_PEAKS.json has no FP32-pipe figure)",
+                "frac_at_max_clock": achieved / (SMS * 128 * 1965e6 / FMA_OPS_PER_PAIR / 1e9),
+                "kernel_ms": 1e3 * t_k, "mufu_peak": SMS * 16 * mhz * 1e6 / 1e9}
+    fp64 = {"value": pairs / statistics.mean(k64) / 1e9, "unit": UNIT, "kernel_ms": 1e3 * statistics.mean(k64)}
+    fp64["fp32c_over_fp64"] = achieved / fp64["value"]
+
+    cpu = None
+    if not a.no_cpu_baseline and rank == 0:
+        try:
+            cpu = cpu_reference_sample(n, a.seed, target_s=10.0, max_s=30.0)
+        except Exception as ex:  # the baseline is reported, never required
+            cpu = {"error": str(ex)}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": 1e3 * t_total / a.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32" if prec == nbr.FP32C else "f64",
+            "data": "synthetic", "config": workload_config(a, {"precision": a.precision}),
+            "gpu_launches": launches, "wall_s_timed": t_wall,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 7 * 8 * n,
+                    "d2h_bytes_per_step": 6 * 8 * n, "scheme": "dkd order 2 (reduced_solver_omp_lf's)",
+                    "ms_per_step": 1e3 * sum(e2e_s) / a.steps},
+            "roofline": roofline, "fp64": fp64, "accuracy": acc, "clocks": clk,
+            "cpu_baseline": cpu}
+    print(json.dumps(line))
+    ctx.close()
+
+
+def run_sharded(a, rank, world, local):
+    raise SystemExit("multi-GPU sharding is not built yet")
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

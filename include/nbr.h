@@ -1,0 +1,228 @@
+/* nbr.h -- C ABI of the B200 all-pairs N-body solver (libnbr.so).
+ *
+ * The solver is a drop-in for the force-and-integrate path of the reference
+ * CPU solver (pc2/n-body-ring-solver, directory CPU/).  Each entry point
+ * below names the reference interface it replaces.  Conventions:
+ *
+ *  - plain pointers and sizes only; every host array is a caller-owned
+ *    contiguous double array of length n (structure of arrays, the layout of
+ *    NBody_system, CPU/nbody_system.h:41-74);
+ *  - every function returns an nbr_status; nothing aborts and no exception
+ *    crosses the ABI (the reference has no error channel at all,
+ *    CPU/force_calculation.cpp:1129);
+ *  - one context = one GPU + one CUDA stream; a context is used by one host
+ *    thread at a time;
+ *  - units are the caller's: G is a parameter (the reference fixes G = 1,
+ *    CPU/nbody_system.h:11); eps2 is the Plummer softening length squared
+ *    (the reference has none: eps2 = 0 reproduces it, skipping coincident
+ *    pairs the way the reference skips q == k).
+ */
+#ifndef NBR_H
+#define NBR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum nbr_status {
+  NBR_OK = 0,
+  NBR_ERR_INVALID_ARG = 1,  /* bad pointer, size or enum value */
+  NBR_ERR_CUDA = 2,         /* a CUDA call failed; see nbr_last_error_string */
+  NBR_ERR_NO_MEMORY = 3,    /* device or host allocation failed */
+  NBR_ERR_TIMEOUT = 4,      /* a bounded device wait gave up (kernel aborted cleanly) */
+  NBR_ERR_NO_SYSTEM = 5,    /* no particles uploaded yet */
+  NBR_ERR_UNSUPPORTED = 6,  /* no CUDA device / unsupported configuration */
+  NBR_ERR_NONFINITE = 7     /* an input contains NaN or Inf */
+} nbr_status;
+
+/* Arithmetic of the pair interaction. */
+typedef enum nbr_precision {
+  NBR_FP64 = 0,  /* plain FP64: matches the reference's double-precision forces */
+  NBR_FP32C = 1  /* FP32 pair arithmetic on FP64 tile-relative coordinates,
+                    TwoSum-compensated cross-tile sums, FP64 integration */
+} nbr_precision;
+
+/* Leapfrog schedule. */
+typedef enum nbr_scheme {
+  NBR_KDK = 0,  /* kick-drift-kick, force reused across steps */
+  NBR_DKD = 1,  /* drift-kick-drift with Yoshida c/d coefficients, the schedule of
+                   reduced_solver_omp_lf (CPU/omp_solver.cpp:257-456) */
+  NBR_EULER = 2 /* explicit Euler, x += v dt then v += a dt: reduced_solver_omp
+                   (CPU/omp_solver.cpp:16-178), the reference's default -i euler */
+} nbr_scheme;
+
+typedef struct nbr_ctx nbr_ctx;
+
+/* Conserved quantities of the current state, all in FP64.  U is the softened
+ * potential energy 1/2 sum_i m_i phi_i. */
+typedef struct nbr_diag {
+  double T, U, E;
+  double P[3];
+  double L[3];
+  double M;
+} nbr_diag;
+
+/* Per-call statistics of nbr_run / nbr_batch_run. */
+typedef struct nbr_run_stats {
+  double force_evals;   /* force evaluations launched */
+  double pairs;         /* ordered pairs i != j evaluated: force_evals * sum N(N-1) */
+  double gpu_ms;        /* device time of the launch sequence (CUDA events) */
+  double kernels;       /* kernel launches issued */
+} nbr_run_stats;
+
+/* ------------------------------------------------------------ context ---- */
+/* Creates a context on `device` (its own stream and device error word). */
+int nbr_ctx_create(int device, nbr_ctx** out);
+int nbr_ctx_destroy(nbr_ctx* ctx);
+/* Last error message of the context (or of the calling thread if ctx is NULL). */
+const char* nbr_last_error_string(const nbr_ctx* ctx);
+/* Library version, e.g. 1000 for 0.1.0. */
+int nbr_version(void);
+/* Number of visible CUDA devices (0 when none); never fails. */
+int nbr_device_count(void);
+/* The context's CUDA stream (a cudaStream_t as an opaque pointer), for callers
+ * that time or order their own work against the solver's. */
+void* nbr_ctx_stream(nbr_ctx* ctx);
+/* Waits for all work issued on the context's stream. */
+int nbr_ctx_synchronize(nbr_ctx* ctx);
+
+/* -------------------------------------------------------------- state ---- */
+/* Copies a system of n particles in (replaces NBody_system::alloc_particles +
+ * the initialisers' stores, CPU/nbody_system.cpp:177-193).  vx/vy/vz may be
+ * NULL (zero velocities).  Rejects NaN/Inf and negative masses. */
+int nbr_system_upload(nbr_ctx* ctx, size_t n, const double* x, const double* y, const double* z,
+                      const double* vx, const double* vy, const double* vz, const double* m);
+/* Copies the current state out; any pointer may be NULL. */
+int nbr_system_download(nbr_ctx* ctx, double* x, double* y, double* z, double* vx, double* vy,
+                        double* vz);
+/* Particle count of the uploaded system (0 if none). */
+size_t nbr_system_size(const nbr_ctx* ctx);
+
+/* ------------------------------------------------------------- forces ---- */
+/* Accelerations (want_force = 0) or forces m_i a_i (want_force = 1) of the
+ * uploaded system, a_i = G sum_{j != i} m_j (x_j - x_i) / (|x_j - x_i|^2 + eps2)^{3/2},
+ * written (overwrite, not accumulate) to the host arrays.  Replaces the force
+ * kernels compute_forces_simple / _avx2 / _avx2_blocked / _avx512_rsqrt(_4i)_blocked
+ * (CPU/force_calculation.h:7-14) with their Newton-3 split summed: the
+ * reference's force + recv_force (CPU/omp_solver.cpp:124-126). */
+int nbr_forces(nbr_ctx* ctx, int precision, double G, double eps2, int want_force, double* ax,
+               double* ay, double* az);
+
+/* The same evaluation left on the device: accelerations of the current state
+ * into the context's acceleration arrays (read back with nbr_forces_download).
+ * One force-kernel launch (plus a one-off pack of the FP32C records after an
+ * upload); for timing the kernel with the caller's own events on
+ * nbr_ctx_stream.  Asynchronous: returns after enqueueing. */
+int nbr_forces_device(nbr_ctx* ctx, int precision, double G, double eps2);
+/* Copies the accelerations left by nbr_forces_device / nbr_run to the host. */
+int nbr_forces_download(nbr_ctx* ctx, double* ax, double* ay, double* az);
+
+/* Accelerations or forces on n_i receivers from n_j sources (separate sets).
+ * The block-pair call the reference's ring decomposition makes for a received
+ * block (compute_forces_* with local_N, rank, comm_sz, recv_round,
+ * CPU/hybrid_solver.cpp:84-95), evaluated in full rather than as a Newton-3
+ * half.  mi (receiver masses) is needed only for want_force = 1.  Pairs at
+ * zero distance are skipped when eps2 = 0 (the reference skips q == k). */
+int nbr_accel_ij(nbr_ctx* ctx, int precision, size_t n_i, const double* xi, const double* yi,
+                 const double* zi, const double* mi, size_t n_j, const double* xj,
+                 const double* yj, const double* zj, const double* mj, double G, double eps2,
+                 int want_force, double* ax, double* ay, double* az);
+
+/* Per-particle softened potential phi_i = -G sum_{j != i} m_j / sqrt(r^2 + eps2)
+ * (phi may be NULL) and U = 1/2 sum m_i phi_i, in FP64.  At eps2 = 0 U equals
+ * calculate_potential_energy / compute_potential_energy_avx2
+ * (CPU/force_calculation.cpp:1749-1904). */
+int nbr_potential(nbr_ctx* ctx, double G, double eps2, double* phi, double* U);
+
+/* T, U, E, P, L, M of the current state (FP64, block-reduced on the GPU).
+ * T replaces compute_kinetic_energy (CPU/force_calculation.cpp:1740-1748). */
+int nbr_diagnostics(nbr_ctx* ctx, double G, double eps2, nbr_diag* out);
+
+/* ---------------------------------------------------------- integrate ---- */
+/* Advances the uploaded system by `steps` steps of size dt.
+ *   scheme NBR_DKD: Yoshida order 2/4/6/8, 2w-1 force evaluations per step,
+ *     the schedule of reduced_solver_omp_lf (CPU/omp_solver.cpp:257-456) with
+ *     the coefficients of omp_main (CPU/omp_solver.cpp:677-743);
+ *   scheme NBR_KDK: order must be 2; one force evaluation per step, the last
+ *     acceleration is reused by the next call (first-same-as-last);
+ *   scheme NBR_EULER: order ignored; one force evaluation per step.
+ * The launch sequence is captured in one CUDA graph.  diag (optional, 2
+ * entries) receives the diagnostics before and after; stats may be NULL. */
+int nbr_run(nbr_ctx* ctx, int precision, int scheme, int order, double dt, size_t steps, double G,
+            double eps2, nbr_diag* diag, nbr_run_stats* stats);
+
+/* Yoshida c[2w] / d[2w-1] of omp_main (CPU/omp_solver.cpp:677-726) for order
+ * 2, 4, 6 or 8; returns lf_steps = 2w, or 0 for an unsupported order. */
+int nbr_yoshida_coefficients(int order, double* c, double* d);
+
+/* ------------------------------------------------------------ tuning ---- */
+/* Forces a kernel configuration for the given precision (ni receivers per
+ * thread: 4 or 8; warps per CTA: 2, 4 or 8; split >= 1 or 0 = automatic).
+ * ni = 0 restores the autotuner. */
+int nbr_set_force_config(nbr_ctx* ctx, int precision, int ni, int warps, int split);
+/* Times the supported configurations for the uploaded system and stores the
+ * fastest in the autotune cache file (see nbr_tune_cache_path). */
+int nbr_autotune(nbr_ctx* ctx, int precision, double eps2);
+/* Path of the JSON autotune cache ($NBR_TUNE_CACHE or the library directory). */
+const char* nbr_tune_cache_path(void);
+
+/* ------------------------------------------------------- init conditions ---- */
+/* Deterministic samplers (xoshiro256** seeded through splitmix64; the same
+ * seed gives the same bits on every host).  N-body units G = M = 1. */
+/* Plummer sphere, scale radius a = 3 pi / 16, equal masses 1/n, positions by
+ * the inverse cumulative mass (mass fraction <= 0.999), speeds by von Neumann
+ * rejection from the isotropic distribution function; centre of mass and
+ * mean velocity moved to zero. */
+int nbr_ic_plummer(size_t n, uint64_t seed, double* x, double* y, double* z, double* vx,
+                   double* vy, double* vz, double* m);
+/* Uniform density in the unit ball, zero velocities, masses 1/n (not recentred). */
+int nbr_ic_uniform_ball(size_t n, uint64_t seed, double* x, double* y, double* z, double* vx,
+                        double* vy, double* vz, double* m);
+/* Plummer sphere whose first n_heavy particles weigh `ratio` times the others,
+ * total mass 1. */
+int nbr_ic_two_component(size_t n, size_t n_heavy, double ratio, uint64_t seed, double* x,
+                         double* y, double* z, double* vx, double* vy, double* vz, double* m);
+/* The reference's ring: n-1 equal masses on radius R plus a central mass
+ * ratio * m, exact circular orbit with angular velocity omega
+ * (init_stable_orbiting_particles, CPU/nbody_system.cpp:319-384).  f* (may be
+ * NULL) receive the analytic force. */
+int nbr_ic_ring(size_t n, double R, double omega, double ratio, double* x, double* y, double* z,
+                double* vx, double* vy, double* vz, double* m, double* fx, double* fy,
+                double* fz);
+/* Analytic rigid rotation of that ring after `step` of `steps_per_rev` steps
+ * (predict_stable_orbiting_particles, CPU/nbody_system.cpp:386-408). */
+int nbr_ic_ring_predict(size_t n, double R, double omega, size_t step, size_t steps_per_rev,
+                        double* x, double* y, double* z, double* vx, double* vy, double* vz);
+/* Sizes of nsys systems drawn log-uniform in [nmin, nmax] (seed). */
+int nbr_ic_batch_sizes(size_t nsys, uint64_t seed, size_t nmin, size_t nmax, size_t* sizes);
+/* Seed of system s of a batch drawn with `seed`. */
+uint64_t nbr_ic_system_seed(uint64_t seed, size_t s);
+
+/* ------------------------------------------------------------- batched ---- */
+/* Uploads nsys independent systems stored back to back: system s owns
+ * particles offsets[s] .. offsets[s+1]-1 (offsets has nsys+1 entries,
+ * offsets[0] = 0).  Systems never interact. */
+int nbr_batch_upload(nbr_ctx* ctx, size_t nsys, const size_t* offsets, const double* x,
+                     const double* y, const double* z, const double* vx, const double* vy,
+                     const double* vz, const double* m);
+/* Copies the batch state out (any pointer may be NULL). */
+int nbr_batch_download(nbr_ctx* ctx, double* x, double* y, double* z, double* vx, double* vy,
+                       double* vz);
+/* Accelerations of every batch particle (want_force as in nbr_forces). */
+int nbr_batch_forces(nbr_ctx* ctx, int precision, double G, double eps2, int want_force,
+                     double* ax, double* ay, double* az);
+/* KDK leapfrog of every system for `steps` steps: one persistent launch per
+ * step walking a device work queue of (system, receiver tile) items, the whole
+ * step loop captured in one CUDA graph. */
+int nbr_batch_run(nbr_ctx* ctx, int precision, double dt, size_t steps, double G, double eps2,
+                  nbr_run_stats* stats);
+/* Per-system diagnostics (out has nsys entries). */
+int nbr_batch_diagnostics(nbr_ctx* ctx, double G, double eps2, nbr_diag* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NBR_H */

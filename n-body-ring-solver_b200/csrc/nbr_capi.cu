@@ -1,0 +1,917 @@
+// nbr_capi.cu -- the C ABI (include/nbr.h): contexts, device state, the
+// leapfrog launch sequences and their CUDA-graph capture, diagnostics and the
+// autotune cache.  Host code; the kernels live in nbr_kernels.cu and
+// nbr_batch.cu.
+#include "nbr.h"
+#include "nbr_ctx.h"
+#include "nbr_device.cuh"
+#include "nbr_kernels.cuh"
+
+#include <dlfcn.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <vector>
+
+using namespace nbr;
+
+namespace nbr {
+
+thread_local std::string t_err;
+
+int fail(nbr_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  t_err = msg;
+  return code;
+}
+
+int cuda_fail(nbr_ctx* c, cudaError_t e, const char* where) {
+  std::string m = std::string(where) + ": " + cudaGetErrorString(e);
+  cudaGetLastError();  // clear a sticky launch error where possible
+  return fail(c, e == cudaErrorMemoryAllocation ? NBR_ERR_NO_MEMORY : NBR_ERR_CUDA, m);
+}
+
+void dfree(void* p) {
+  if (p) cudaFree(p);
+}
+
+cudaError_t dalloc(void** p, size_t bytes) {
+  *p = nullptr;
+  if (bytes == 0) bytes = 256;
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) return e;
+  return cudaMemset(*p, 0, bytes);
+}
+
+bool finite_array(const double* a, size_t n) {
+  bool ok = true;
+  for (size_t i = 0; i < n; ++i) ok &= std::isfinite(a[i]);
+  return ok;
+}
+
+void SysState::release() {
+  for (int b = 0; b < 2; ++b) {
+    for (int d = 0; d < 3; ++d) dfree(pos[b][d]);
+    dfree(rec[b]);
+    dfree(org[b]);
+  }
+  for (int d = 0; d < 3; ++d) { dfree(vel[d]); dfree(acc[d]); }
+  dfree(mass);
+  *this = SysState();
+}
+
+cudaError_t SysState::reserve(size_t n_) {
+  const size_t np = ((n_ + 1023) / 1024) * 1024;
+  if (np <= cap) {
+    n = n_;
+    n_pad = np;
+    ntiles = (int)((n_ + kTile - 1) / kTile);
+    return cudaSuccess;
+  }
+  release();
+  cudaError_t e = cudaSuccess;
+  auto A = [&](void** p, size_t bytes) {
+    if (e == cudaSuccess) e = dalloc(p, bytes);
+  };
+  for (int b = 0; b < 2; ++b) {
+    for (int d = 0; d < 3; ++d) A((void**)&pos[b][d], np * sizeof(double));
+    A((void**)&rec[b], np * 3 * sizeof(float4));
+    A((void**)&org[b], (np / kTile) * sizeof(double4));
+  }
+  for (int d = 0; d < 3; ++d) {
+    A((void**)&vel[d], np * sizeof(double));
+    A((void**)&acc[d], np * sizeof(double));
+  }
+  A((void**)&mass, np * sizeof(double));
+  if (e != cudaSuccess) {
+    release();
+    return e;
+  }
+  cap = np;
+  n = n_;
+  n_pad = np;
+  ntiles = (int)((n_ + kTile - 1) / kTile);
+  return cudaSuccess;
+}
+
+// Zeroes the padding of every array (entries n .. n_pad-1), so padding
+// particles have zero mass and sit at the origin of both buffers.
+cudaError_t SysState::clear_padding(cudaStream_t st) {
+  const size_t tail = n_pad - n;
+  cudaError_t e = cudaSuccess;
+  auto Z = [&](double* p) {
+    if (e == cudaSuccess && tail) e = cudaMemsetAsync(p + n, 0, tail * sizeof(double), st);
+  };
+  for (int b = 0; b < 2; ++b)
+    for (int d = 0; d < 3; ++d) Z(pos[b][d]);
+  for (int d = 0; d < 3; ++d) { Z(vel[d]); Z(acc[d]); }
+  Z(mass);
+  return e;
+}
+
+cudaError_t Scratch::need_part(size_t doubles) {
+  if (doubles <= part_cap) return cudaSuccess;
+  dfree(part);
+  part = nullptr;
+  part_cap = 0;
+  cudaError_t e = dalloc((void**)&part, doubles * sizeof(double));
+  if (e == cudaSuccess) part_cap = doubles;
+  return e;
+}
+cudaError_t Scratch::need_counters(size_t count) {
+  if (count <= cnt_cap) return cudaSuccess;
+  dfree(cnt);
+  cnt = nullptr;
+  cnt_cap = 0;
+  cudaError_t e = dalloc((void**)&cnt, count * sizeof(unsigned));
+  if (e == cudaSuccess) cnt_cap = count;
+  return e;
+}
+cudaError_t Scratch::need_red(size_t doubles) {
+  if (doubles <= red_cap) return cudaSuccess;
+  dfree(red);
+  red = nullptr;
+  red_cap = 0;
+  cudaError_t e = dalloc((void**)&red, doubles * sizeof(double));
+  if (e == cudaSuccess) red_cap = doubles;
+  return e;
+}
+void Scratch::release() {
+  dfree(part);
+  dfree(cnt);
+  dfree(red);
+  *this = Scratch();
+}
+
+// --------------------------------------------------------------- tuning ----
+namespace {
+
+std::mutex g_tune_mu;
+std::map<std::string, ForceConfig>* g_tune = nullptr;
+std::string g_tune_path;
+
+std::string lib_dir() {
+  Dl_info info;
+  if (dladdr((void*)&nbr_version, &info) && info.dli_fname) {
+    std::string p = info.dli_fname;
+    size_t s = p.find_last_of('/');
+    if (s != std::string::npos) return p.substr(0, s);
+  }
+  return ".";
+}
+
+std::string tune_key(int precision, long long n_i, int ntiles, bool excl) {
+  int bucket = 0;
+  while ((1LL << (bucket + 1)) <= n_i) ++bucket;
+  int jb = 0;
+  while ((1LL << (jb + 1)) <= (long long)ntiles) ++jb;
+  std::ostringstream k;
+  k << (precision == kFP32C ? "fp32c" : "fp64") << ":i" << bucket << ":j" << jb
+    << (excl ? ":e0" : "");
+  return k.str();
+}
+
+// The cache is a flat JSON object {"key": [ni, warps, split], ...}.
+void load_tune_locked() {
+  if (g_tune) return;
+  g_tune = new std::map<std::string, ForceConfig>();
+  const char* env = std::getenv("NBR_TUNE_CACHE");
+  g_tune_path = env && *env ? env : lib_dir() + "/nbr_tune_cache.json";
+  std::ifstream f(g_tune_path);
+  if (!f) return;
+  std::stringstream ss;
+  ss << f.rdbuf();
+  std::string s = ss.str();
+  size_t p = 0;
+  while ((p = s.find('"', p)) != std::string::npos) {
+    size_t q = s.find('"', p + 1);
+    if (q == std::string::npos) break;
+    std::string key = s.substr(p + 1, q - p - 1);
+    size_t lb = s.find('[', q), rb = s.find(']', q);
+    if (lb == std::string::npos || rb == std::string::npos) break;
+    ForceConfig c{0, 0, 0};
+    if (std::sscanf(s.c_str() + lb + 1, "%d , %d , %d", &c.ni, &c.warps, &c.split) == 3 &&
+        force_config_supported(0, c))
+      (*g_tune)[key] = c;
+    p = rb + 1;
+  }
+}
+
+void save_tune_locked() {
+  std::ofstream f(g_tune_path);
+  if (!f) return;
+  f << "{\n";
+  size_t k = 0;
+  for (auto& kv : *g_tune) {
+    f << "  \"" << kv.first << "\": [" << kv.second.ni << ", " << kv.second.warps << ", "
+      << kv.second.split << "]" << (++k < g_tune->size() ? ",\n" : "\n");
+  }
+  f << "}\n";
+}
+
+}  // namespace
+
+// Heuristic split: enough (chunk, split) units for ~8 waves of resident CTAs,
+// each split range at least 8 tiles.
+int auto_split(int precision, double eps2, const ForceConfig& c, long long n_i, int ntiles,
+               int sms) {
+  const long long chunk = 32LL * c.ni * c.warps;
+  const long long chunks = (n_i + chunk - 1) / chunk;
+  int per_sm = force_blocks_per_sm(precision, eps2, c);
+  if (per_sm < 1) per_sm = 1;
+  const long long slots = (long long)sms * per_sm;
+  long long s = (8 * slots + chunks - 1) / chunks;
+  const long long smax = std::max<long long>(1, ntiles / 8);
+  s = std::max<long long>(1, std::min(s, smax));
+  return (int)s;
+}
+
+ForceConfig choose_config(nbr_ctx* c, int precision, double eps2, long long n_i, int ntiles) {
+  ForceConfig cfg = c->override_cfg[precision];
+  if (cfg.ni == 0) {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    load_tune_locked();
+    auto it = g_tune->find(tune_key(precision, n_i, ntiles, eps2 == 0.0));
+    cfg = it != g_tune->end() ? it->second : ForceConfig{4, 4, 0};
+  }
+  if (cfg.split <= 0) cfg.split = auto_split(precision, eps2, cfg, n_i, ntiles, c->sms);
+  if (cfg.split > ntiles) cfg.split = std::max(1, ntiles);
+  return cfg;
+}
+
+// Prepares scratch for a force launch of `cfg` over n_i receivers.
+int prepare_split(nbr_ctx* c, const ForceConfig& cfg, long long n_pad_i) {
+  if (cfg.split <= 1) return NBR_OK;
+  cudaError_t e = c->scr.need_part((size_t)cfg.split * 3 * (size_t)n_pad_i);
+  if (e == cudaSuccess) e = c->scr.need_counters((size_t)(n_pad_i / 64 + 1));
+  return e == cudaSuccess ? NBR_OK : cuda_fail(c, e, "split scratch");
+}
+
+// Bounded-wait limit and the test hook of the tile pipeline, from the
+// environment: NBR_WAIT_LIMIT_MS (default 4000) and NBR_TEST_SKIP_TILE
+// (CTA-local tile index whose copy is never issued, so that its wait expires
+// and the launch reports NBR_ERR_TIMEOUT; default off).
+void pipeline_params(JStream& js) {
+  js.wait_ns = kWaitLimitNs;
+  js.skip_tile = -1;
+  if (const char* w = std::getenv("NBR_WAIT_LIMIT_MS")) {
+    const long long ms = std::atoll(w);
+    if (ms > 0) js.wait_ns = (unsigned long long)ms * 1000000ull;
+  }
+  if (const char* k = std::getenv("NBR_TEST_SKIP_TILE")) {
+    if (*k) js.skip_tile = std::atoi(k);
+  }
+}
+
+// Reads and clears the device error word; maps it to a status.
+int check_device_error(nbr_ctx* c) {
+  int h = 0;
+  cudaError_t e = cudaMemcpyAsync(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "kernel execution");
+  if (h != kErrNone) {
+    cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
+    if (c->scr.cnt) cudaMemsetAsync(c->scr.cnt, 0, c->scr.cnt_cap * sizeof(unsigned), c->stream);
+    cudaStreamSynchronize(c->stream);
+    c->acc_ok = false;
+    return fail(c, NBR_ERR_TIMEOUT,
+                h == kErrTileWait ? "a j-tile copy did not complete within the wait limit"
+                                  : "device wait limit exceeded (code " + std::to_string(h) + ")");
+  }
+  return NBR_OK;
+}
+
+// Makes the FP32C records of position buffer b valid.
+cudaError_t ensure_records(nbr_ctx* c, int b, int* kernels) {
+  SysState& s = c->sys;
+  if (s.rec_ok[b]) return cudaSuccess;
+  cudaError_t e = launch_kick_drift((long long)s.n, (long long)s.n_pad, s.pos[b][0], s.pos[b][1],
+                                    s.pos[b][2], s.mass, nullptr, nullptr, nullptr, 0.0, 0.0,
+                                    nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, s.rec[b],
+                                    s.org[b], c->stream);
+  if (kernels) ++*kernels;
+  if (e == cudaSuccess) s.rec_ok[b] = true;
+  return e;
+}
+
+// One force evaluation of the uploaded system on its current buffer with the
+// given epilogue (mode 1 writes the next buffer, which becomes current).
+int eval_system(nbr_ctx* c, int precision, double G, double eps2, int mode, double kick,
+                double drift, int want_force, int* kernels) {
+  SysState& s = c->sys;
+  const int a = s.cur, b = 1 - s.cur;
+  cudaError_t e = cudaSuccess;
+  if (precision == kFP32C) e = ensure_records(c, a, kernels);
+  if (e != cudaSuccess) return cuda_fail(c, e, "pack");
+  ForceConfig cfg = choose_config(c, precision, eps2, (long long)s.n, s.ntiles);
+  int rc = prepare_split(c, cfg, (long long)s.n_pad);
+  if (rc) return rc;
+  IParticles ip{s.pos[a][0], s.pos[a][1], s.pos[a][2], s.mass, (long long)s.n};
+  JStream js{s.pos[a][0], s.pos[a][1], s.pos[a][2], s.mass, s.rec[a], s.org[a], s.ntiles, 0, -1};
+  pipeline_params(js);
+  Epilogue ep{};
+  ep.mode = mode;
+  ep.G = G;
+  ep.ax = s.acc[0]; ep.ay = s.acc[1]; ep.az = s.acc[2];
+  ep.want_force = want_force;
+  ep.kick = kick;
+  ep.drift = drift;
+  ep.vx = s.vel[0]; ep.vy = s.vel[1]; ep.vz = s.vel[2];
+  ep.xn = s.pos[b][0]; ep.yn = s.pos[b][1]; ep.zn = s.pos[b][2];
+  ep.rec_next = (mode != 0 && precision == kFP32C) ? s.rec[b] : nullptr;
+  ep.origin_next = s.org[b];
+  ep.part = c->scr.part;
+  ep.counters = c->scr.cnt;
+  ep.n_pad = (long long)s.n_pad;
+  ep.err = c->d_err;
+  e = launch_force(precision, eps2, cfg, ip, js, ep, c->stream);
+  if (kernels) ++*kernels;
+  if (e != cudaSuccess) return cuda_fail(c, e, "force launch");
+  if (mode != 0) {
+    s.cur = b;
+    s.rec_ok[b] = (precision == kFP32C);
+    s.rec_ok[a] = false;
+  }
+  return NBR_OK;
+}
+
+// Standalone kick (v += kick a) + drift (x' = x + drift v into the other
+// buffer), packing records of x' when the next evaluation is FP32C.
+int kick_drift_system(nbr_ctx* c, bool pack, double kick, double drift, bool use_acc,
+                      int* kernels) {
+  SysState& s = c->sys;
+  const int a = s.cur, b = 1 - s.cur;
+  cudaError_t e = launch_kick_drift(
+      (long long)s.n, (long long)s.n_pad, s.pos[a][0], s.pos[a][1], s.pos[a][2], s.mass,
+      use_acc ? s.acc[0] : nullptr, use_acc ? s.acc[1] : nullptr, use_acc ? s.acc[2] : nullptr,
+      kick, drift, s.vel[0], s.vel[1], s.vel[2], s.pos[b][0], s.pos[b][1], s.pos[b][2],
+      pack ? s.rec[b] : nullptr, pack ? s.org[b] : nullptr, c->stream);
+  if (kernels) ++*kernels;
+  if (e != cudaSuccess) return cuda_fail(c, e, "kick-drift launch");
+  s.cur = b;
+  s.rec_ok[b] = pack;
+  s.rec_ok[a] = false;
+  return NBR_OK;
+}
+
+int diag_system(nbr_ctx* c, double G, double eps2, nbr_diag* out) {
+  SysState& s = c->sys;
+  const int a = s.cur;
+  const int nb = (int)((s.n + 127) / 128);
+  cudaError_t e = c->scr.need_red((size_t)nb * 9 + 16);
+  if (e != cudaSuccess) return cuda_fail(c, e, "diag scratch");
+  double* part = c->scr.red;
+  double* pot = c->scr.red + (size_t)nb * 8;
+  double* res = c->scr.red + (size_t)nb * 9;
+  e = launch_moments((long long)s.n, (long long)s.n_pad, s.pos[a][0], s.pos[a][1], s.pos[a][2],
+                     s.vel[0], s.vel[1], s.vel[2], s.mass, part, c->stream);
+  if (e == cudaSuccess) e = launch_rowsum(part, nb, 8, res, c->stream);
+  if (e == cudaSuccess)
+    e = launch_potential((long long)s.n, (long long)s.n_pad, s.pos[a][0], s.pos[a][1],
+                         s.pos[a][2], s.mass, G, eps2, nullptr, pot, c->stream);
+  if (e == cudaSuccess) e = launch_rowsum(pot, nb, 1, res + 8, c->stream);
+  double h[9];
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(h, res, sizeof(h), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "diagnostics");
+  out->T = h[0];
+  out->P[0] = h[1]; out->P[1] = h[2]; out->P[2] = h[3];
+  out->L[0] = h[4]; out->L[1] = h[5]; out->L[2] = h[6];
+  out->M = h[7];
+  out->U = h[8];
+  out->E = out->T + out->U;
+  return NBR_OK;
+}
+
+// Yoshida weights -> c/d (order 2/4/6/8), the construction of omp_main
+// (CPU/omp_solver.cpp:677-726): c_0 = c_{2w-1} = w_{w-1}/2,
+// c_i = c_{2w-1-i} = (w_{w-i} + w_{w-1-i})/2, d_i = d_{2w-2-i} = w_{w-1-i}.
+int yoshida(int order, double* c, double* d) {
+  const double cb = std::cbrt(2.0);
+  double w2[1] = {1.0};
+  double w4[2] = {-cb / (2.0 - cb), 1.0 / (2.0 - cb)};
+  double w6[4] = {1.0, -1.17767998417887, 0.235573213359357, 0.78451361047756};
+  double w8[8] = {1.0, -0.161582374150097e1, -0.244699182370524e1, -0.716989419708120e-2,
+                  0.244002732616735e1, 0.157739928123617, 0.182020630970714e1,
+                  0.104242620869991e1};
+  for (int i = 1; i < 4; ++i) w6[0] -= 2.0 * w6[i];
+  for (int i = 1; i < 8; ++i) w8[0] -= 2.0 * w8[i];
+  const double* w;
+  int ws;
+  switch (order) {
+    case 2: w = w2; ws = 1; break;
+    case 4: w = w4; ws = 2; break;
+    case 6: w = w6; ws = 4; break;
+    case 8: w = w8; ws = 8; break;
+    default: return 0;
+  }
+  for (int i = 0; i < ws; ++i) {
+    const double ci = i == 0 ? w[ws - 1] / 2.0 : (w[ws - i] + w[ws - 1 - i]) / 2.0;
+    c[i] = c[2 * ws - 1 - i] = ci;
+    d[i] = d[2 * ws - 2 - i] = w[ws - 1 - i];
+  }
+  return 2 * ws;
+}
+
+}  // namespace nbr
+
+// ===================================================================== ABI ==
+extern "C" {
+
+int nbr_version(void) { return 1000; }
+
+int nbr_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+const char* nbr_last_error_string(const nbr_ctx* c) {
+  return c ? c->err.c_str() : t_err.c_str();
+}
+
+int nbr_ctx_create(int device, nbr_ctx** out) {
+  if (!out) return fail(nullptr, NBR_ERR_INVALID_ARG, "out is NULL");
+  *out = nullptr;
+  int nd = nbr_device_count();
+  if (nd == 0) return fail(nullptr, NBR_ERR_UNSUPPORTED, "no CUDA device");
+  if (device < 0 || device >= nd) return fail(nullptr, NBR_ERR_INVALID_ARG, "bad device index");
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaSetDevice");
+  cudaDeviceProp prop;
+  e = cudaGetDeviceProperties(&prop, device);
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaGetDeviceProperties");
+  if (prop.major < 10)
+    return fail(nullptr, NBR_ERR_UNSUPPORTED,
+                std::string("needs an sm_100 device, found ") + prop.name);
+  nbr_ctx* c = new nbr_ctx();
+  c->device = device;
+  c->sms = prop.multiProcessorCount;
+  e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
+  if (e == cudaSuccess) e = dalloc((void**)&c->d_err, sizeof(int) * 4);
+  if (e != cudaSuccess) {
+    int rc = cuda_fail(nullptr, e, "context setup");
+    nbr_ctx_destroy(c);
+    return rc;
+  }
+  *out = c;
+  return NBR_OK;
+}
+
+int nbr_ctx_destroy(nbr_ctx* c) {
+  if (!c) return NBR_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  c->sys.release();
+  c->bat.release();
+  c->scr.release();
+  c->ij.release();
+  dfree(c->d_err);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return NBR_OK;
+}
+
+void* nbr_ctx_stream(nbr_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int nbr_ctx_synchronize(nbr_ctx* c) {
+  if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  return e == cudaSuccess ? NBR_OK : cuda_fail(c, e, "synchronize");
+}
+
+size_t nbr_system_size(const nbr_ctx* c) { return c ? c->sys.n : 0; }
+
+int nbr_system_upload(nbr_ctx* c, size_t n, const double* x, const double* y, const double* z,
+                      const double* vx, const double* vy, const double* vz, const double* m) {
+  if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
+  if (n == 0 || !x || !y || !z || !m) return fail(c, NBR_ERR_INVALID_ARG, "empty system or NULL array");
+  if ((vx || vy || vz) && !(vx && vy && vz))
+    return fail(c, NBR_ERR_INVALID_ARG, "velocities must be all given or all NULL");
+  if (n > (size_t)1 << 31) return fail(c, NBR_ERR_INVALID_ARG, "n above 2^31");
+  if (!finite_array(x, n) || !finite_array(y, n) || !finite_array(z, n) || !finite_array(m, n) ||
+      (vx && (!finite_array(vx, n) || !finite_array(vy, n) || !finite_array(vz, n))))
+    return fail(c, NBR_ERR_NONFINITE, "input contains NaN or Inf");
+  for (size_t i = 0; i < n; ++i)
+    if (m[i] < 0.0) return fail(c, NBR_ERR_INVALID_ARG, "negative mass");
+  cudaSetDevice(c->device);
+  SysState& s = c->sys;
+  cudaError_t e = s.reserve(n);
+  if (e != cudaSuccess) return cuda_fail(c, e, "system allocation");
+  s.cur = 0;
+  s.rec_ok[0] = s.rec_ok[1] = false;
+  c->acc_ok = false;
+  const size_t B = n * sizeof(double);
+  auto H = [&](double* d, const double* h) {
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d, h, B, cudaMemcpyHostToDevice, c->stream);
+  };
+  H(s.pos[0][0], x); H(s.pos[0][1], y); H(s.pos[0][2], z);
+  H(s.mass, m);
+  if (vx) { H(s.vel[0], vx); H(s.vel[1], vy); H(s.vel[2], vz); }
+  else {
+    for (int d = 0; d < 3 && e == cudaSuccess; ++d)
+      e = cudaMemsetAsync(s.vel[d], 0, B, c->stream);
+  }
+  if (e == cudaSuccess) e = s.clear_padding(c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "upload");
+  return NBR_OK;
+}
+
+int nbr_system_download(nbr_ctx* c, double* x, double* y, double* z, double* vx, double* vy,
+                        double* vz) {
+  if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
+  SysState& s = c->sys;
+  if (s.n == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no system uploaded");
+  cudaSetDevice(c->device);
+  const size_t B = s.n * sizeof(double);
+  cudaError_t e = cudaSuccess;
+  auto D = [&](double* h, const double* d) {
+    if (h && e == cudaSuccess) e = cudaMemcpyAsync(h, d, B, cudaMemcpyDeviceToHost, c->stream);
+  };
+  D(x, s.pos[s.cur][0]); D(y, s.pos[s.cur][1]); D(z, s.pos[s.cur][2]);
+  D(vx, s.vel[0]); D(vy, s.vel[1]); D(vz, s.vel[2]);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  return e == cudaSuccess ? NBR_OK : cuda_fail(c, e, "download");
+}
+
+int nbr_forces(nbr_ctx* c, int precision, double G, double eps2, int want_force, double* ax,
+               double* ay, double* az) {
+  if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
+  if (precision != NBR_FP64 && precision != NBR_FP32C)
+    return fail(c, NBR_ERR_INVALID_ARG, "unknown precision");
+  if (!(eps2 >= 0.0) || !std::isfinite(eps2) || !std::isfinite(G))
+    return fail(c, NBR_ERR_INVALID_ARG, "eps2 must be finite and >= 0, G finite");
+  SysState& s = c->sys;
+  if (s.n == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no system uploaded");
+  cudaSetDevice(c->device);
+  int rc = eval_system(c, precision, G, eps2, 0, 0.0, 0.0, want_force, nullptr);
+  if (rc) return rc;
+  rc = check_device_error(c);
+  if (rc) return rc;
+  c->acc_ok = !want_force;
+  c->acc_prec = precision;
+  c->acc_G = G;
+  c->acc_eps2 = eps2;
+  const size_t B = s.n * sizeof(double);
+  cudaError_t e = cudaSuccess;
+  auto D = [&](double* h, const double* d) {
+    if (h && e == cudaSuccess) e = cudaMemcpyAsync(h, d, B, cudaMemcpyDeviceToHost, c->stream);
+  };
+  D(ax, s.acc[0]); D(ay, s.acc[1]); D(az, s.acc[2]);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  return e == cudaSuccess ? NBR_OK : cuda_fail(c, e, "forces download");
+}
+
+int nbr_forces_device(nbr_ctx* c, int precision, double G, double eps2) {
+  if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
+  if (precision != NBR_FP64 && precision != NBR_FP32C)
+    return fail(c, NBR_ERR_INVALID_ARG, "unknown precision");
+  if (!(eps2 >= 0.0) || !std::isfinite(eps2) || !std::isfinite(G))
+    return fail(c, NBR_ERR_INVALID_ARG, "eps2 must be finite and >= 0, G finite");
+  if (c->sys.n == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no system uploaded");
+  cudaSetDevice(c->device);
+  const int rc = eval_system(c, precision, G, eps2, 0, 0.0, 0.0, 0, nullptr);
+  if (rc) return rc;
+  c->acc_ok = true;
+  c->acc_prec = precision;
+  c->acc_G = G;
+  c->acc_eps2 = eps2;
+  return NBR_OK;
+}
+
+int nbr_forces_download(nbr_ctx* c, double* ax, double* ay, double* az) {
+  if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
+  SysState& s = c->sys;
+  if (s.n == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no system uploaded");
+  cudaSetDevice(c->device);
+  int rc = check_device_error(c);
+  if (rc) return rc;
+  const size_t B = s.n * sizeof(double);
+  cudaError_t e = cudaSuccess;
+  auto D = [&](double* h, const double* d) {
+    if (h && e == cudaSuccess) e = cudaMemcpyAsync(h, d, B, cudaMemcpyDeviceToHost, c->stream);
+  };
+  D(ax, s.acc[0]); D(ay, s.acc[1]); D(az, s.acc[2]);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  return e == cudaSuccess ? NBR_OK : cuda_fail(c, e, "forces download");
+}
+
+int nbr_accel_ij(nbr_ctx* c, int precision, size_t n_i, const double* xi, const double* yi,
+                 const double* zi, const double* mi, size_t n_j, const double* xj,
+                 const double* yj, const double* zj, const double* mj, double G, double eps2,
+                 int want_force, double* ax, double* ay, double* az) {
+  if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
+  if (precision != NBR_FP64 && precision != NBR_FP32C)
+    return fail(c, NBR_ERR_INVALID_ARG, "unknown precision");
+  if (n_i == 0) return NBR_OK;
+  if (!xi || !yi || !zi || !ax || !ay || !az || (want_force && !mi))
+    return fail(c, NBR_ERR_INVALID_ARG, "NULL receiver array");
+  if (n_j > 0 && (!xj || !yj || !zj || !mj)) return fail(c, NBR_ERR_INVALID_ARG, "NULL source array");
+  if (!(eps2 >= 0.0) || !std::isfinite(eps2) || !std::isfinite(G))
+    return fail(c, NBR_ERR_INVALID_ARG, "eps2 must be finite and >= 0, G finite");
+  if (n_i > (size_t)1 << 31 || n_j > (size_t)1 << 31) return fail(c, NBR_ERR_INVALID_ARG, "size above 2^31");
+  if (!finite_array(xi, n_i) || !finite_array(yi, n_i) || !finite_array(zi, n_i) ||
+      (mi && !finite_array(mi, n_i)) || !finite_array(xj, n_j) || !finite_array(yj, n_j) ||
+      !finite_array(zj, n_j) || !finite_array(mj, n_j))
+    return fail(c, NBR_ERR_NONFINITE, "input contains NaN or Inf");
+  if (n_j == 0) {
+    std::fill(ax, ax + n_i, 0.0); std::fill(ay, ay + n_i, 0.0); std::fill(az, az + n_i, 0.0);
+    return NBR_OK;
+  }
+  cudaSetDevice(c->device);
+  // Receivers live in ij.pos[0] (+ mass), sources in ij.pos[1] (+ j_mass).
+  SysState& r = c->ij;
+  const size_t nmax = std::max(n_i, n_j);
+  cudaError_t e = r.reserve(nmax);
+  if (e != cudaSuccess) return cuda_fail(c, e, "ij allocation");
+  const long long npi = (long long)(((n_i + 1023) / 1024) * 1024);
+  const long long npj = (long long)(((n_j + 1023) / 1024) * 1024);
+  auto H = [&](double* d, const double* h, size_t n, long long np) {
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d, h, n * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess && (long long)n < np)
+      e = cudaMemsetAsync(d + n, 0, (np - n) * sizeof(double), c->stream);
+  };
+  H(r.pos[0][0], xi, n_i, npi); H(r.pos[0][1], yi, n_i, npi); H(r.pos[0][2], zi, n_i, npi);
+  if (mi) H(r.mass, mi, n_i, npi);
+  H(r.pos[1][0], xj, n_j, npj); H(r.pos[1][1], yj, n_j, npj); H(r.pos[1][2], zj, n_j, npj);
+  H(r.vel[0], mj, n_j, npj);  // source masses
+  if (e != cudaSuccess) return cuda_fail(c, e, "ij upload");
+  const int ntiles = (int)((n_j + kTile - 1) / kTile);
+  if (precision == kFP32C) {
+    e = launch_kick_drift((long long)n_j, npj, r.pos[1][0], r.pos[1][1], r.pos[1][2], r.vel[0],
+                          nullptr, nullptr, nullptr, 0.0, 0.0, nullptr, nullptr, nullptr, nullptr,
+                          nullptr, nullptr, r.rec[1], r.org[1], c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "ij pack");
+  }
+  ForceConfig cfg = choose_config(c, precision, eps2, (long long)n_i, ntiles);
+  int rc = prepare_split(c, cfg, npi);
+  if (rc) return rc;
+  IParticles ip{r.pos[0][0], r.pos[0][1], r.pos[0][2], r.mass, (long long)n_i};
+  // (the source masses are staged in r.vel[0])
+  JStream js{r.pos[1][0], r.pos[1][1], r.pos[1][2], r.vel[0], r.rec[1], r.org[1], ntiles, 0, -1};
+  pipeline_params(js);
+  Epilogue ep{};
+  ep.mode = 0;
+  ep.G = G;
+  ep.ax = r.acc[0]; ep.ay = r.acc[1]; ep.az = r.acc[2];
+  ep.want_force = want_force;
+  ep.part = c->scr.part;
+  ep.counters = c->scr.cnt;
+  ep.n_pad = npi;
+  ep.err = c->d_err;
+  e = launch_force(precision, eps2, cfg, ip, js, ep, c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "ij force launch");
+  rc = check_device_error(c);
+  if (rc) return rc;
+  const size_t B = n_i * sizeof(double);
+  e = cudaMemcpyAsync(ax, r.acc[0], B, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ay, r.acc[1], B, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(az, r.acc[2], B, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  return e == cudaSuccess ? NBR_OK : cuda_fail(c, e, "ij download");
+}
+
+int nbr_potential(nbr_ctx* c, double G, double eps2, double* phi, double* U) {
+  if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
+  if (!(eps2 >= 0.0) || !std::isfinite(eps2)) return fail(c, NBR_ERR_INVALID_ARG, "bad eps2");
+  SysState& s = c->sys;
+  if (s.n == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no system uploaded");
+  cudaSetDevice(c->device);
+  const int nb = (int)((s.n + 127) / 128);
+  cudaError_t e = c->scr.need_red((size_t)nb + 16);
+  if (e != cudaSuccess) return cuda_fail(c, e, "potential scratch");
+  // phi goes to the (otherwise idle) acceleration x array only when requested.
+  double* dphi = phi ? s.acc[0] : nullptr;
+  if (phi) c->acc_ok = false;
+  e = launch_potential((long long)s.n, (long long)s.n_pad, s.pos[s.cur][0], s.pos[s.cur][1],
+                       s.pos[s.cur][2], s.mass, G, eps2, dphi, c->scr.red, c->stream);
+  if (e == cudaSuccess) e = launch_rowsum(c->scr.red, nb, 1, c->scr.red + nb, c->stream);
+  double u = 0.0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&u, c->scr.red + nb, sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess && phi)
+    e = cudaMemcpyAsync(phi, dphi, s.n * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "potential");
+  if (U) *U = u;
+  return NBR_OK;
+}
+
+int nbr_diagnostics(nbr_ctx* c, double G, double eps2, nbr_diag* out) {
+  if (!c || !out) return fail(c, NBR_ERR_INVALID_ARG, "NULL argument");
+  if (!(eps2 >= 0.0) || !std::isfinite(eps2)) return fail(c, NBR_ERR_INVALID_ARG, "bad eps2");
+  if (c->sys.n == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no system uploaded");
+  cudaSetDevice(c->device);
+  return diag_system(c, G, eps2, out);
+}
+
+int nbr_yoshida_coefficients(int order, double* cc, double* dd) {
+  if (!cc || !dd) return 0;
+  return yoshida(order, cc, dd);
+}
+
+int nbr_run(nbr_ctx* c, int precision, int scheme, int order, double dt, size_t steps, double G,
+            double eps2, nbr_diag* diag, nbr_run_stats* stats) {
+  if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
+  if (precision != NBR_FP64 && precision != NBR_FP32C)
+    return fail(c, NBR_ERR_INVALID_ARG, "unknown precision");
+  if (scheme != NBR_KDK && scheme != NBR_DKD && scheme != NBR_EULER)
+    return fail(c, NBR_ERR_INVALID_ARG, "unknown scheme");
+  if (scheme == NBR_KDK && order != 2) return fail(c, NBR_ERR_INVALID_ARG, "KDK is second order");
+  double cc[16], dd[16];
+  const int lf = scheme == NBR_DKD ? yoshida(order, cc, dd) : 2;
+  if (lf == 0) return fail(c, NBR_ERR_INVALID_ARG, "order must be 2, 4, 6 or 8");
+  if (!std::isfinite(dt) || !(eps2 >= 0.0) || !std::isfinite(eps2) || !std::isfinite(G))
+    return fail(c, NBR_ERR_INVALID_ARG, "dt, G must be finite, eps2 finite and >= 0");
+  SysState& s = c->sys;
+  if (s.n == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no system uploaded");
+  cudaSetDevice(c->device);
+  int rc;
+  if (diag) {
+    rc = diag_system(c, G, eps2, &diag[0]);
+    if (rc) return rc;
+  }
+  nbr_run_stats st{};
+  if (steps > 0) {
+    // Allocate everything the sequence needs before capture.
+    ForceConfig cfg = choose_config(c, precision, eps2, (long long)s.n, s.ntiles);
+    rc = prepare_split(c, cfg, (long long)s.n_pad);
+    if (rc) return rc;
+    const bool fsal = (scheme == NBR_KDK) && c->acc_ok && c->acc_prec == precision &&
+                      c->acc_G == G && c->acc_eps2 == eps2;
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_fail(c, e, "begin capture");
+    int kernels = 0;
+    double evals = 0;
+    const int cur0 = s.cur;
+    const bool rec0 = s.rec_ok[0], rec1 = s.rec_ok[1];
+    rc = NBR_OK;
+    const bool fp32 = precision == kFP32C;
+    if (scheme == NBR_KDK) {
+      if (fsal) {
+        rc = kick_drift_system(c, fp32, 0.5 * dt, dt, true, &kernels);
+      } else {
+        rc = eval_system(c, precision, G, eps2, 1, 0.5 * dt, dt, 0, &kernels);
+        evals += 1;
+      }
+      for (size_t k = 1; k < steps && rc == NBR_OK; ++k) {
+        rc = eval_system(c, precision, G, eps2, 1, dt, dt, 0, &kernels);
+        evals += 1;
+      }
+      if (rc == NBR_OK) {
+        rc = eval_system(c, precision, G, eps2, 1, 0.5 * dt, 0.0, 0, &kernels);
+        evals += 1;
+      }
+    } else if (scheme == NBR_EULER) {
+      for (size_t k = 0; k < steps && rc == NBR_OK; ++k) {
+        rc = eval_system(c, precision, G, eps2, 2, dt, dt, 0, &kernels);
+        evals += 1;
+      }
+    } else {
+      rc = kick_drift_system(c, fp32, 0.0, cc[0] * dt, false, &kernels);
+      for (size_t k = 0; k < steps && rc == NBR_OK; ++k) {
+        for (int sub = 0; sub < lf - 1 && rc == NBR_OK; ++sub) {
+          double drift;
+          if (sub < lf - 2) drift = cc[sub + 1];
+          else drift = (k + 1 < steps) ? cc[lf - 1] + cc[0] : cc[lf - 1];
+          rc = eval_system(c, precision, G, eps2, 1, dd[sub] * dt, drift * dt, 0, &kernels);
+          evals += 1;
+        }
+      }
+    }
+    cudaError_t ee = cudaStreamEndCapture(c->stream, &graph);
+    if (rc != NBR_OK || ee != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      s.cur = cur0;
+      s.rec_ok[0] = rec0;
+      s.rec_ok[1] = rec1;
+      return rc != NBR_OK ? rc : cuda_fail(c, ee, "end capture");
+    }
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      s.cur = cur0;
+      s.rec_ok[0] = rec0;
+      s.rec_ok[1] = rec1;
+      return cuda_fail(c, e, "graph instantiate");
+    }
+    e = cudaEventRecord(c->ev0, c->stream);
+    if (e == cudaSuccess) e = cudaGraphLaunch(exec, c->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(c->ev1, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaGraphExecDestroy(exec);
+    if (e != cudaSuccess) {
+      c->acc_ok = false;
+      return cuda_fail(c, e, "graph launch");
+    }
+    rc = check_device_error(c);
+    if (rc) return rc;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    st.gpu_ms = ms;
+    st.kernels = kernels;
+    st.force_evals = evals;
+    st.pairs = evals * double(s.n) * double(s.n - 1);
+    if (scheme == NBR_KDK) {
+      c->acc_ok = true;
+      c->acc_prec = precision;
+      c->acc_G = G;
+      c->acc_eps2 = eps2;
+    } else {
+      c->acc_ok = false;
+    }
+  }
+  if (diag) {
+    rc = diag_system(c, G, eps2, &diag[1]);
+    if (rc) return rc;
+  }
+  if (stats) *stats = st;
+  return NBR_OK;
+}
+
+int nbr_set_force_config(nbr_ctx* c, int precision, int ni, int warps, int split) {
+  if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
+  if (precision != NBR_FP64 && precision != NBR_FP32C)
+    return fail(c, NBR_ERR_INVALID_ARG, "unknown precision");
+  if (ni == 0) {
+    c->override_cfg[precision] = ForceConfig{0, 0, 0};
+    return NBR_OK;
+  }
+  ForceConfig cfg{ni, warps, split < 1 ? 1 : split};
+  if (!force_config_supported(precision, cfg))
+    return fail(c, NBR_ERR_INVALID_ARG, "unsupported (ni, warps)");
+  cfg.split = split;
+  c->override_cfg[precision] = cfg;
+  return NBR_OK;
+}
+
+const char* nbr_tune_cache_path(void) {
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  load_tune_locked();
+  return g_tune_path.c_str();
+}
+
+int nbr_autotune(nbr_ctx* c, int precision, double eps2) {
+  if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
+  if (precision != NBR_FP64 && precision != NBR_FP32C)
+    return fail(c, NBR_ERR_INVALID_ARG, "unknown precision");
+  SysState& s = c->sys;
+  if (s.n == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no system uploaded");
+  cudaSetDevice(c->device);
+  const ForceConfig saved = c->override_cfg[precision];
+  const int cand[][2] = {{4, 2}, {4, 4}, {4, 8}, {8, 2}, {8, 4}};
+  ForceConfig best{0, 0, 0};
+  float best_ms = 1e30f;
+  for (auto& cw : cand) {
+    ForceConfig base{cw[0], cw[1], 1};
+    const int s0 = auto_split(precision, eps2, base, (long long)s.n, s.ntiles, c->sms);
+    const int splits[] = {std::max(1, s0 / 2), s0, s0 * 2};
+    for (int sp : splits) {
+      if (sp > s.ntiles) continue;
+      c->override_cfg[precision] = ForceConfig{cw[0], cw[1], sp};
+      float tot = 0.f;
+      bool ok = true;
+      for (int rep = 0; rep < 3 && ok; ++rep) {
+        cudaEventRecord(c->ev0, c->stream);
+        ok = eval_system(c, precision, 1.0, eps2, 0, 0.0, 0.0, 0, nullptr) == NBR_OK;
+        cudaEventRecord(c->ev1, c->stream);
+        ok = ok && check_device_error(c) == NBR_OK;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        if (rep > 0) tot += ms;  // first repetition warms up
+      }
+      if (ok && tot < best_ms) {
+        best_ms = tot;
+        best = ForceConfig{cw[0], cw[1], sp};
+      }
+    }
+  }
+  c->override_cfg[precision] = saved;
+  c->acc_ok = false;
+  if (best.ni == 0) return fail(c, NBR_ERR_CUDA, "no configuration ran");
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  load_tune_locked();
+  (*g_tune)[tune_key(precision, (long long)s.n, s.ntiles, eps2 == 0.0)] = best;
+  save_tune_locked();
+  return NBR_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,99 @@
+// nbr_ctx.h -- internal definition of nbr_ctx and its device state.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "nbr.h"
+#include "nbr_kernels.cuh"
+
+namespace nbr {
+
+// Device state of one particle system (or of a batch of systems stored back to
+// back).  Positions are double-buffered: a force evaluation reads buffer
+// `cur` and its fused kick/drift epilogue writes buffer 1 - cur.  Every array
+// holds n_pad entries; entries >= n are zero-mass padding at the origin.
+struct SysState {
+  size_t n = 0, n_pad = 0, cap = 0;
+  int ntiles = 0;
+  double* pos[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+  double* vel[3] = {nullptr, nullptr, nullptr};
+  double* acc[3] = {nullptr, nullptr, nullptr};
+  double* mass = nullptr;
+  float4* rec[2] = {nullptr, nullptr};     // FP32C source records of each buffer
+  double4* org[2] = {nullptr, nullptr};    // FP64 tile origins of each buffer
+  int cur = 0;
+  bool rec_ok[2] = {false, false};
+
+  cudaError_t reserve(size_t n);
+  cudaError_t clear_padding(cudaStream_t st);
+  void release();
+};
+
+// Scratch reused across calls: split partial sums, split arrival counters,
+// diagnostic partial sums.
+struct Scratch {
+  double* part = nullptr;
+  size_t part_cap = 0;
+  unsigned* cnt = nullptr;
+  size_t cnt_cap = 0;
+  double* red = nullptr;
+  size_t red_cap = 0;
+
+  cudaError_t need_part(size_t doubles);
+  cudaError_t need_counters(size_t count);
+  cudaError_t need_red(size_t doubles);
+  void release();
+};
+
+// Batched independent systems (nbr_batch_*).  Each system is padded to whole
+// tiles, so a tile never mixes systems.
+struct BatchState {
+  SysState s;                        // all systems' particles (padded layout)
+  size_t nsys = 0;
+  size_t n_real = 0;                 // sum of the real sizes
+  std::vector<size_t> off;           // real offsets (host), nsys + 1
+  std::vector<long long> poff;       // padded offsets (host), nsys + 1
+  long long* d_poff = nullptr;       // padded offsets (device), nsys + 1
+  int* d_nreal = nullptr;            // real size of each system (device)
+  int* d_sys_of_tile = nullptr;      // system index of every padded tile
+  int2* d_items = nullptr;           // work queue: (system, first receiver tile)
+  int n_items = 0;
+  unsigned* d_head = nullptr;        // work-queue heads
+  double* d_red = nullptr;           // per-system diagnostic sums
+  bool acc_ok = false;
+  int acc_prec = 0;
+  double acc_G = 0.0, acc_eps2 = 0.0;
+  double pairs_per_eval = 0.0;
+
+  void release();
+};
+
+int fail(nbr_ctx* c, int code, const std::string& msg);
+int cuda_fail(nbr_ctx* c, cudaError_t e, const char* where);
+cudaError_t dalloc(void** p, size_t bytes);
+void dfree(void* p);
+bool finite_array(const double* a, size_t n);
+int check_device_error(nbr_ctx* c);
+
+}  // namespace nbr
+
+struct nbr_ctx {
+  int device = 0;
+  int sms = 148;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::string err;
+  nbr::SysState sys;       // the uploaded system
+  nbr::SysState ij;        // scratch for nbr_accel_ij
+  nbr::Scratch scr;
+  nbr::BatchState bat;
+  int* d_err = nullptr;    // device error word (nbr::kErr*)
+  // First-same-as-last: sys.acc holds G-scaled accelerations of the current
+  // positions for (acc_prec, acc_G, acc_eps2).
+  bool acc_ok = false;
+  int acc_prec = 0;
+  double acc_G = 0.0, acc_eps2 = 0.0;
+  nbr::ForceConfig override_cfg[2] = {{0, 0, 0}, {0, 0, 0}};
+};

@@ -1,0 +1,649 @@
+// nbr_kernels.cu -- all-pairs softened gravity on sm_100a.
+//
+// The hot path replaces the reference's force kernels (compute_forces_* in
+// CPU/force_calculation.cpp, e.g. compute_forces_avx2_blocked :477-690) and the
+// kick/drift loops of reduced_solver_omp_lf (CPU/omp_solver.cpp:320-420).
+//
+// Structure of a force launch (both precisions):
+//  * Each warp owns 32 * NI consecutive receivers ("i-block"); lane l keeps
+//    receivers ibase + l + 32k, k < NI, in registers.  A CTA of W warps shares
+//    one stream of source tiles ("j-tiles", kTile particles each).
+//  * j-tiles stream through a 4-stage shared-memory ring filled by 1-D TMA
+//    bulk copies (cp.async.bulk, mbarrier completion, one elected producer
+//    thread).  This is the single-GPU image of the reference's ring pass, where
+//    blocks of particles travel past every rank (CPU/hybrid_solver.cpp:79-107).
+//  * The j range can be split over gridDim.y CTAs; each writes its partial
+//    sums and the last CTA to finish a receiver chunk adds them in split order
+//    (deterministic) and runs the epilogue.
+//  * Epilogue: either write a (or m a), or the fused leapfrog update
+//    v += kick a; x' = x + drift v into the other position buffer, plus the
+//    FP32 records of x' for the next FP32C evaluation.
+//
+// FP32C pair arithmetic (per ordered pair; f32x2 instructions work on two
+// receivers at once):
+//     d  = x_j - x_i           3 sub      (relative to the tile's FP64 origin)
+//     r2 = d.d + eps^2         3 fma
+//     y  = rsqrt.approx(r2)    1 MUFU
+//     y2 = y*y; p = r2*y2      2 mul      (p = 1 - e, e the rsqrt error)
+//     mg = (-1.5 m) p + 2.5 m  1 fma      (m (1 + 3e/2): first-order Newton
+//     y3 = y2*y; s = y3*mg     2 mul       correction of y^3 with the mass folded in)
+//     acc += s d               3 fma
+// = 14 FP32-pipe operations + 1 MUFU per pair.  One Newton-Raphson step on
+// y followed by cubing gives y^3 (1 + 3e/2 + O(e^2)) as well; the form above
+// applies the same first-order correction to y^3 directly.  Tile partial sums
+// (kTile sources) are FP32; across tiles they are combined with Knuth
+// TwoSum into a (hi, lo) FP32 pair per component, and hi + lo is formed in
+// FP64 at the end.
+#include "nbr_device.cuh"
+#include "nbr_kernels.cuh"
+
+#include <cstdio>
+
+namespace nbr {
+
+namespace {
+
+constexpr int kStages = 4;
+constexpr int kRecBytes = kTile * 48;          // 3 x float4 per source
+constexpr int kStage32 = kRecBytes + 32;       // + FP64 tile origin (double4)
+constexpr int kStage64 = 4 * kTile * 8;        // x, y, z, m tiles
+constexpr int kSmemHead = 128;                 // mbarriers
+
+// ------------------------------------------------------------ pipeline ----
+// Runs body(stage) for the ntl tiles of this CTA's j range.  Thread 0 is the
+// producer: it issues the bulk copies of a tile once every thread has finished
+// with the stage it reuses.  Returns false if a tile wait timed out; the abort
+// is CTA-uniform (decided by __syncthreads_or), the error word is set, and the
+// copies that were issued but not consumed are drained (bounded wait) so that
+// none lands after the CTA exits.  js.skip_tile >= 0 makes the producer never
+// issue that tile: a test hook that lets a bounded wait expire on purpose.
+template <class Issue, class Body>
+__device__ __forceinline__ bool tile_pipeline(uint64_t* bars, int ntl, const JStream& js, int* err,
+                                              Issue issue, Body body) {
+  const int tid = threadIdx.x;
+  uint32_t pending = 0;  // producer only: stages with an issued, unconsumed copy
+  auto produce = [&](int st, int t) {
+    if (t == js.skip_tile) return;
+    issue(st, t);
+    pending |= 1u << st;
+  };
+  if (tid == 0) {
+    for (int st = 0; st < kStages; ++st) mbar_init(smem_u32(&bars[st]), 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  if (tid == 0)
+    for (int st = 0; st < kStages && st < ntl; ++st) produce(st, st);
+  int t = 0;
+  bool aborted = false;
+  for (; t < ntl; ++t) {
+    const int st = t % kStages;
+    const uint32_t par = (uint32_t)(t / kStages) & 1u;
+    const bool ok = mbar_wait_bounded(smem_u32(&bars[st]), par, js.wait_ns);
+    body(st);
+    if (__syncthreads_or(!ok)) {
+      aborted = true;
+      break;
+    }
+    if (tid == 0) {
+      pending &= ~(1u << st);
+      if (t + kStages < ntl) produce(st, t + kStages);
+    }
+  }
+  if (aborted && tid == 0) {
+    record_error(err, kErrTileWait);
+    for (int u = t; u < ntl && u < t + kStages; ++u) {
+      const int st = u % kStages;
+      if (!(pending & (1u << st))) continue;
+      if (!mbar_wait_bounded(smem_u32(&bars[st]), (uint32_t)(u / kStages) & 1u, js.wait_ns)) {
+        record_error(err, kErrDrainWait);
+        break;
+      }
+    }
+  }
+  return !aborted;
+}
+
+// --------------------------------------------------------- FP32C pack ----
+// Writes the FP32 source records of one warp's 32 * NI receivers (NI / 4 tiles
+// of kTile).  The tile origin is the FP64 mean of the tile's real particles;
+// each record holds (x-o, x-o, y-o, y-o), (z-o, z-o, -1.5 m, -1.5 m),
+// (2.5 m, 2.5 m, 0, 0) in FP32.  Padding entries get zeros (zero mass).
+template <int NI>
+__device__ __forceinline__ void pack_warp(long long n, long long ibase, int lane, const double* xn,
+                                          const double* yn, const double* zn, const double* m,
+                                          float4* rec, double4* org) {
+  static_assert(NI % 4 == 0, "a warp must cover whole tiles");
+#pragma unroll
+  for (int q = 0; q < NI / 4; ++q) {
+    double sx = 0.0, sy = 0.0, sz = 0.0, cnt = 0.0;
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) {
+      const int k = 4 * q + kk;
+      if (ibase + 32 * k < n) {
+        sx += xn[k]; sy += yn[k]; sz += zn[k]; cnt += 1.0;
+      }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      sx += __shfl_xor_sync(0xffffffffu, sx, off);
+      sy += __shfl_xor_sync(0xffffffffu, sy, off);
+      sz += __shfl_xor_sync(0xffffffffu, sz, off);
+      cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
+    }
+    const double ox = cnt > 0.0 ? sx / cnt : 0.0;
+    const double oy = cnt > 0.0 ? sy / cnt : 0.0;
+    const double oz = cnt > 0.0 ? sz / cnt : 0.0;
+    const long long tile = (ibase - lane + (long long)kTile * q) / kTile;
+    if (lane == 0) org[tile] = make_double4(ox, oy, oz, 0.0);
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) {
+      const int k = 4 * q + kk;
+      const long long i = ibase + 32 * k;
+      float fx = 0.f, fy = 0.f, fz = 0.f, fa = 0.f, fb = 0.f;
+      if (i < n) {
+        fx = __double2float_rn(xn[k] - ox);
+        fy = __double2float_rn(yn[k] - oy);
+        fz = __double2float_rn(zn[k] - oz);
+        fa = __double2float_rn(-1.5 * m[i]);
+        fb = __double2float_rn(2.5 * m[i]);
+      }
+      rec[3 * i + 0] = make_float4(fx, fx, fy, fy);
+      rec[3 * i + 1] = make_float4(fz, fz, fa, fa);
+      rec[3 * i + 2] = make_float4(fb, fb, 0.f, 0.f);
+    }
+  }
+}
+
+// ------------------------------------------------------------ epilogue ----
+template <int NI>
+__device__ __forceinline__ void epilogue(const IParticles& ip, const Epilogue& ep, long long ibase,
+                                         int lane, const double* xi, const double* yi,
+                                         const double* zi, const double* ax, const double* ay,
+                                         const double* az) {
+  if (ep.mode == 0) {
+#pragma unroll
+    for (int k = 0; k < NI; ++k) {
+      const long long i = ibase + 32 * k;
+      if (i < ip.n) {
+        const double sc = ep.want_force ? ep.G * ip.m[i] : ep.G;
+        ep.ax[i] = sc * ax[k];
+        ep.ay[i] = sc * ay[k];
+        ep.az[i] = sc * az[k];
+      }
+    }
+    return;
+  }
+  double xn[NI], yn[NI], zn[NI];
+#pragma unroll
+  for (int k = 0; k < NI; ++k) {
+    const long long i = ibase + 32 * k;
+    xn[k] = yn[k] = zn[k] = 0.0;
+    if (i < ip.n) {
+      const double gx = ep.G * ax[k], gy = ep.G * ay[k], gz = ep.G * az[k];
+      ep.ax[i] = gx; ep.ay[i] = gy; ep.az[i] = gz;
+      const double ux = ep.vx[i], uy = ep.vy[i], uz = ep.vz[i];
+      const double vx = ux + ep.kick * gx;
+      const double vy = uy + ep.kick * gy;
+      const double vz = uz + ep.kick * gz;
+      ep.vx[i] = vx; ep.vy[i] = vy; ep.vz[i] = vz;
+      // mode 1: drift with the kicked velocity (leapfrog); mode 2: with the
+      // old one (explicit Euler, reduced_solver_omp, CPU/omp_solver.cpp:121-135).
+      const bool euler = ep.mode == 2;
+      xn[k] = xi[k] + ep.drift * (euler ? ux : vx);
+      yn[k] = yi[k] + ep.drift * (euler ? uy : vy);
+      zn[k] = zi[k] + ep.drift * (euler ? uz : vz);
+      ep.xn[i] = xn[k]; ep.yn[i] = yn[k]; ep.zn[i] = zn[k];
+    }
+  }
+  if (ep.rec_next) pack_warp<NI>(ip.n, ibase, lane, xn, yn, zn, ip.m, ep.rec_next, ep.origin_next);
+}
+
+// Split reduction (if any) followed by the epilogue.
+template <int NI>
+__device__ __forceinline__ void finish(const IParticles& ip, const Epilogue& ep, long long ibase,
+                                       int lane, const double* xi, const double* yi,
+                                       const double* zi, double* ax, double* ay, double* az) {
+  if (gridDim.y > 1) {
+    __shared__ int s_last;
+    const long long np = ep.n_pad;
+    double* P = ep.part + (size_t)blockIdx.y * 3 * (size_t)np;
+#pragma unroll
+    for (int k = 0; k < NI; ++k) {
+      const long long i = ibase + 32 * k;
+      P[i] = ax[k];
+      P[np + i] = ay[k];
+      P[2 * np + i] = az[k];
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const unsigned prev = atomicAdd(&ep.counters[blockIdx.x], 1u);
+      s_last = (prev == gridDim.y - 1) ? 1 : 0;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+#pragma unroll
+    for (int k = 0; k < NI; ++k) {
+      const long long i = ibase + 32 * k;
+      double sx = 0.0, sy = 0.0, sz = 0.0;
+      for (int s = 0; s < (int)gridDim.y; ++s) {
+        const double* Q = ep.part + (size_t)s * 3 * (size_t)np;
+        sx += __ldcg(Q + i);
+        sy += __ldcg(Q + np + i);
+        sz += __ldcg(Q + 2 * np + i);
+      }
+      ax[k] = sx; ay[k] = sy; az[k] = sz;
+    }
+    if (threadIdx.x == 0) ep.counters[blockIdx.x] = 0u;
+  }
+  epilogue<NI>(ip, ep, ibase, lane, xi, yi, zi, ax, ay, az);
+}
+
+// ------------------------------------------------------ FP32C kernel ----
+template <int NI, int WARPS, bool EXCL>
+__global__ void __launch_bounds__(WARPS * 32)
+    k_force_f32c(const IParticles ip, const JStream js, const Epilogue ep, const float eps2f) {
+  constexpr int IPAIR = NI / 2;
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
+  unsigned char* stages = smem + kSmemHead;
+
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long long ibase = ((long long)blockIdx.x * WARPS + warp) * (32 * NI) + lane;
+  const int S = gridDim.y, sp = blockIdx.y;
+  const int t0 = (int)((long long)js.ntiles * sp / S);
+  const int t1 = (int)((long long)js.ntiles * (sp + 1) / S);
+
+  double xi[NI], yi[NI], zi[NI];
+#pragma unroll
+  for (int k = 0; k < NI; ++k) {
+    const long long i = ibase + 32 * k;
+    xi[k] = ip.x[i]; yi[k] = ip.y[i]; zi[k] = ip.z[i];
+  }
+  u64 hx[IPAIR], hy[IPAIR], hz[IPAIR], lx[IPAIR], ly[IPAIR], lz[IPAIR];
+#pragma unroll
+  for (int p = 0; p < IPAIR; ++p) hx[p] = hy[p] = hz[p] = lx[p] = ly[p] = lz[p] = 0ull;
+  const u64 EPS2 = pack2(eps2f, eps2f);
+
+  auto issue = [&](int st, int t) {
+    unsigned char* dst = stages + st * kStage32;
+    const uint32_t bar = smem_u32(&bars[st]);
+    mbar_expect_tx(bar, kStage32);
+    bulk_g2s(dst, js.rec + (size_t)(t0 + t) * kTile * 3, kRecBytes, bar);
+    bulk_g2s(dst + kRecBytes, js.origin + (t0 + t), 32, bar);
+  };
+  auto body = [&](int st) {
+    const unsigned char* base = stages + st * kStage32;
+    const double4 o = *reinterpret_cast<const double4*>(base + kRecBytes);
+    u64 XI[IPAIR], YI[IPAIR], ZI[IPAIR], AX[IPAIR], AY[IPAIR], AZ[IPAIR];
+#pragma unroll
+    for (int p = 0; p < IPAIR; ++p) {
+      XI[p] = pack2(__double2float_rn(xi[2 * p] - o.x), __double2float_rn(xi[2 * p + 1] - o.x));
+      YI[p] = pack2(__double2float_rn(yi[2 * p] - o.y), __double2float_rn(yi[2 * p + 1] - o.y));
+      ZI[p] = pack2(__double2float_rn(zi[2 * p] - o.z), __double2float_rn(zi[2 * p + 1] - o.z));
+      AX[p] = AY[p] = AZ[p] = 0ull;
+    }
+    const ulonglong2* R = reinterpret_cast<const ulonglong2*>(base);
+#pragma unroll 4
+    for (int j = 0; j < kTile; ++j) {
+      const ulonglong2 q0 = R[3 * j];
+      const ulonglong2 q1 = R[3 * j + 1];
+      const u64 bj = R[3 * j + 2].x;
+#pragma unroll
+      for (int p = 0; p < IPAIR; ++p) {
+        const u64 dx = sub2(q0.x, XI[p]);
+        const u64 dy = sub2(q0.y, YI[p]);
+        const u64 dz = sub2(q1.x, ZI[p]);
+        u64 r2 = fma2(dx, dx, EPS2);
+        r2 = fma2(dy, dy, r2);
+        r2 = fma2(dz, dz, r2);
+        u64 y;
+        if (EXCL) {
+          float rl, rh;
+          unpack2(r2, rl, rh);
+          y = pack2(rl > 0.f ? rsqrt_mufu(rl) : 0.f, rh > 0.f ? rsqrt_mufu(rh) : 0.f);
+        } else {
+          y = rsqrt2(r2);
+        }
+        const u64 y2 = mul2(y, y);
+        const u64 pr = mul2(r2, y2);
+        const u64 mg = fma2(q1.y, pr, bj);
+        const u64 y3 = mul2(y2, y);
+        const u64 s = mul2(y3, mg);
+        AX[p] = fma2(s, dx, AX[p]);
+        AY[p] = fma2(s, dy, AY[p]);
+        AZ[p] = fma2(s, dz, AZ[p]);
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < IPAIR; ++p) {
+      two_sum2(hx[p], lx[p], AX[p]);
+      two_sum2(hy[p], ly[p], AY[p]);
+      two_sum2(hz[p], lz[p], AZ[p]);
+    }
+  };
+  if (!tile_pipeline(bars, t1 - t0, js, ep.err, issue, body)) return;
+
+  double ax[NI], ay[NI], az[NI];
+#pragma unroll
+  for (int p = 0; p < IPAIR; ++p) {
+    float h0, h1, l0, l1;
+    unpack2(hx[p], h0, h1); unpack2(lx[p], l0, l1);
+    ax[2 * p] = (double)h0 + (double)l0; ax[2 * p + 1] = (double)h1 + (double)l1;
+    unpack2(hy[p], h0, h1); unpack2(ly[p], l0, l1);
+    ay[2 * p] = (double)h0 + (double)l0; ay[2 * p + 1] = (double)h1 + (double)l1;
+    unpack2(hz[p], h0, h1); unpack2(lz[p], l0, l1);
+    az[2 * p] = (double)h0 + (double)l0; az[2 * p + 1] = (double)h1 + (double)l1;
+  }
+  finish<NI>(ip, ep, ibase, lane, xi, yi, zi, ax, ay, az);
+}
+
+// ------------------------------------------------------- FP64 kernel ----
+// The drop-in form: every operation in FP64, the reciprocal square root from
+// CUDA's rsqrt(double).  Matches the reference's double-precision forces up to
+// summation order.
+template <int NI, int WARPS, bool EXCL>
+__global__ void __launch_bounds__(WARPS * 32)
+    k_force_f64(const IParticles ip, const JStream js, const Epilogue ep, const double eps2) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
+  unsigned char* stages = smem + kSmemHead;
+
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long long ibase = ((long long)blockIdx.x * WARPS + warp) * (32 * NI) + lane;
+  const int S = gridDim.y, sp = blockIdx.y;
+  const int t0 = (int)((long long)js.ntiles * sp / S);
+  const int t1 = (int)((long long)js.ntiles * (sp + 1) / S);
+
+  double xi[NI], yi[NI], zi[NI], ax[NI], ay[NI], az[NI];
+#pragma unroll
+  for (int k = 0; k < NI; ++k) {
+    const long long i = ibase + 32 * k;
+    xi[k] = ip.x[i]; yi[k] = ip.y[i]; zi[k] = ip.z[i];
+    ax[k] = ay[k] = az[k] = 0.0;
+  }
+
+  auto issue = [&](int st, int t) {
+    unsigned char* dst = stages + st * kStage64;
+    const uint32_t bar = smem_u32(&bars[st]);
+    const size_t off = (size_t)(t0 + t) * kTile;
+    mbar_expect_tx(bar, kStage64);
+    bulk_g2s(dst, js.x + off, kTile * 8, bar);
+    bulk_g2s(dst + kTile * 8, js.y + off, kTile * 8, bar);
+    bulk_g2s(dst + 2 * kTile * 8, js.z + off, kTile * 8, bar);
+    bulk_g2s(dst + 3 * kTile * 8, js.m + off, kTile * 8, bar);
+  };
+  auto body = [&](int st) {
+    const double* sx = reinterpret_cast<const double*>(stages + st * kStage64);
+    const double* sy = sx + kTile;
+    const double* sz = sy + kTile;
+    const double* sm = sz + kTile;
+#pragma unroll 2
+    for (int j = 0; j < kTile; ++j) {
+      const double xj = sx[j], yj = sy[j], zj = sz[j], mj = sm[j];
+#pragma unroll
+      for (int k = 0; k < NI; ++k) {
+        const double dx = xj - xi[k], dy = yj - yi[k], dz = zj - zi[k];
+        double r2 = fma(dx, dx, eps2);
+        r2 = fma(dy, dy, r2);
+        r2 = fma(dz, dz, r2);
+        double y = rsqrt(r2);
+        if (EXCL) y = r2 > 0.0 ? y : 0.0;
+        const double s = mj * (y * y * y);
+        ax[k] = fma(s, dx, ax[k]);
+        ay[k] = fma(s, dy, ay[k]);
+        az[k] = fma(s, dz, az[k]);
+      }
+    }
+  };
+  if (!tile_pipeline(bars, t1 - t0, js, ep.err, issue, body)) return;
+  finish<NI>(ip, ep, ibase, lane, xi, yi, zi, ax, ay, az);
+}
+
+// --------------------------------------------------- kick / drift / pack ----
+// One warp per kTile particles (4 per lane).  ax == nullptr: no kick;
+// xn == nullptr: positions are not written (pack of x itself, drift ignored).
+__global__ void __launch_bounds__(128)
+    k_kick_drift(long long n, long long n_pad, const double* __restrict__ x,
+                 const double* __restrict__ y, const double* __restrict__ z,
+                 const double* __restrict__ m, const double* __restrict__ ax,
+                 const double* __restrict__ ay, const double* __restrict__ az, double kick,
+                 double drift, double* vx, double* vy, double* vz, double* xn, double* yn,
+                 double* zn, float4* rec, double4* org) {
+  const int lane = threadIdx.x & 31;
+  const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long ibase = w * kTile + lane;
+  if (ibase - lane >= n_pad) return;
+  double px[4], py[4], pz[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const long long i = ibase + 32 * k;
+    px[k] = py[k] = pz[k] = 0.0;
+    if (i < n) {
+      px[k] = x[i]; py[k] = y[i]; pz[k] = z[i];
+      if (vx) {
+        double ux = vx[i], uy = vy[i], uz = vz[i];
+        if (ax) {
+          ux += kick * ax[i]; uy += kick * ay[i]; uz += kick * az[i];
+          vx[i] = ux; vy[i] = uy; vz[i] = uz;
+        }
+        if (xn) {
+          px[k] += drift * ux; py[k] += drift * uy; pz[k] += drift * uz;
+        }
+      }
+      if (xn) { xn[i] = px[k]; yn[i] = py[k]; zn[i] = pz[k]; }
+    }
+  }
+  if (rec) pack_warp<4>(n, ibase, lane, px, py, pz, m, rec, org);
+}
+
+// ----------------------------------------------------------- diagnostics ----
+// Fixed-order block tree reduction of `W` values per thread (blockDim 128).
+template <int W>
+__device__ __forceinline__ void block_reduce_store(double (&v)[W], double* out) {
+  __shared__ double red[W][128];
+#pragma unroll
+  for (int c = 0; c < W; ++c) red[c][threadIdx.x] = v[c];
+  __syncthreads();
+  for (int h = 64; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h) {
+#pragma unroll
+      for (int c = 0; c < W; ++c) red[c][threadIdx.x] += red[c][threadIdx.x + h];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int c = 0; c < W; ++c) out[(size_t)blockIdx.x * W + c] = red[c][0];
+  }
+}
+
+__global__ void __launch_bounds__(128)
+    k_potential(long long n, const double* __restrict__ x, const double* __restrict__ y,
+                const double* __restrict__ z, const double* __restrict__ m, double G, double eps2,
+                double* __restrict__ phi, double* __restrict__ blocksum) {
+  __shared__ double sx[128], sy[128], sz[128], sm[128];
+  const long long i = (long long)blockIdx.x * 128 + threadIdx.x;
+  const bool valid = i < n;
+  const double xi = valid ? x[i] : 0.0, yi = valid ? y[i] : 0.0, zi = valid ? z[i] : 0.0;
+  double acc = 0.0;
+  for (long long j0 = 0; j0 < n; j0 += 128) {
+    const long long jl = j0 + threadIdx.x;
+    __syncthreads();
+    sx[threadIdx.x] = jl < n ? x[jl] : 0.0;
+    sy[threadIdx.x] = jl < n ? y[jl] : 0.0;
+    sz[threadIdx.x] = jl < n ? z[jl] : 0.0;
+    sm[threadIdx.x] = jl < n ? m[jl] : 0.0;
+    __syncthreads();
+    const int cnt = (int)((n - j0) < 128 ? (n - j0) : 128);
+    for (int jj = 0; jj < cnt; ++jj) {
+      if (j0 + jj == i) continue;
+      const double dx = sx[jj] - xi, dy = sy[jj] - yi, dz = sz[jj] - zi;
+      acc += sm[jj] / sqrt(dx * dx + dy * dy + dz * dz + eps2);
+    }
+  }
+  const double p = -G * acc;
+  if (valid && phi) phi[i] = p;
+  double v[1] = {valid ? 0.5 * m[i] * p : 0.0};
+  block_reduce_store<1>(v, blocksum);
+}
+
+__global__ void __launch_bounds__(128)
+    k_moments(long long n, const double* __restrict__ x, const double* __restrict__ y,
+              const double* __restrict__ z, const double* __restrict__ vx,
+              const double* __restrict__ vy, const double* __restrict__ vz,
+              const double* __restrict__ m, double* __restrict__ part) {
+  const long long i = (long long)blockIdx.x * 128 + threadIdx.x;
+  double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (i < n) {
+    const double mi = m[i];
+    v[0] = 0.5 * mi * (vx[i] * vx[i] + vy[i] * vy[i] + vz[i] * vz[i]);
+    v[1] = mi * vx[i]; v[2] = mi * vy[i]; v[3] = mi * vz[i];
+    v[4] = mi * (y[i] * vz[i] - z[i] * vy[i]);
+    v[5] = mi * (z[i] * vx[i] - x[i] * vz[i]);
+    v[6] = mi * (x[i] * vy[i] - y[i] * vx[i]);
+    v[7] = mi;
+  }
+  block_reduce_store<8>(v, part);
+}
+
+__global__ void __launch_bounds__(256) k_rowsum(const double* __restrict__ part, int nblocks,
+                                                int width, double* __restrict__ out) {
+  __shared__ double red[256];
+  for (int c = 0; c < width; ++c) {
+    double s = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += 256) s += part[(size_t)b * width + c];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+      if ((int)threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[c] = red[0];
+    __syncthreads();
+  }
+}
+
+// -------------------------------------------------------------- dispatch ----
+template <int NI, int W, bool EX>
+cudaError_t launch_f32c_t(float eps2f, int split, const IParticles& ip, const JStream& js,
+                          const Epilogue& ep, cudaStream_t st) {
+  const size_t smem = kSmemHead + (size_t)kStages * kStage32;
+  const long long chunk = 32LL * NI * W;
+  const unsigned gx = (unsigned)((ip.n + chunk - 1) / chunk);
+  dim3 grid(gx, (unsigned)split);
+  k_force_f32c<NI, W, EX><<<grid, W * 32, smem, st>>>(ip, js, ep, eps2f);
+  return cudaGetLastError();
+}
+template <int NI, int W, bool EX>
+cudaError_t launch_f64_t(double eps2, int split, const IParticles& ip, const JStream& js,
+                         const Epilogue& ep, cudaStream_t st) {
+  const size_t smem = kSmemHead + (size_t)kStages * kStage64;
+  const long long chunk = 32LL * NI * W;
+  const unsigned gx = (unsigned)((ip.n + chunk - 1) / chunk);
+  dim3 grid(gx, (unsigned)split);
+  k_force_f64<NI, W, EX><<<grid, W * 32, smem, st>>>(ip, js, ep, eps2);
+  return cudaGetLastError();
+}
+
+#define NBR_CFG_LIST(X) X(4, 2) X(4, 4) X(4, 8) X(8, 2) X(8, 4)
+
+}  // namespace
+
+bool force_config_supported(int precision, const ForceConfig& c) {
+  (void)precision;
+#define NBR_MATCH(a, b) if (c.ni == a && c.warps == b) return c.split >= 1;
+  NBR_CFG_LIST(NBR_MATCH)
+#undef NBR_MATCH
+  return false;
+}
+
+int force_blocks_per_sm(int precision, double eps2, const ForceConfig& c) {
+  int nb = 0;
+  const size_t smem = force_smem_bytes(precision, c);
+  const bool ex = (eps2 == 0.0);
+#define NBR_OCC(a, b)                                                                          \
+  if (c.ni == a && c.warps == b) {                                                             \
+    const void* fn = precision == kFP32C                                                       \
+                         ? (ex ? (const void*)k_force_f32c<a, b, true>                         \
+                               : (const void*)k_force_f32c<a, b, false>)                       \
+                         : (ex ? (const void*)k_force_f64<a, b, true>                          \
+                               : (const void*)k_force_f64<a, b, false>);                       \
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, b * 32, smem) != cudaSuccess)   \
+      nb = 0;                                                                                  \
+    return nb;                                                                                 \
+  }
+  NBR_CFG_LIST(NBR_OCC)
+#undef NBR_OCC
+  return 0;
+}
+
+size_t force_smem_bytes(int precision, const ForceConfig&) {
+  return kSmemHead + (size_t)kStages * (precision == kFP32C ? kStage32 : kStage64);
+}
+
+cudaError_t launch_force(int precision, double eps2, const ForceConfig& c, const IParticles& ip,
+                         const JStream& js, const Epilogue& ep, cudaStream_t st) {
+  if (ip.n <= 0 || js.ntiles <= 0) return cudaSuccess;
+  const bool ex = (eps2 == 0.0);
+  if (precision == kFP32C) {
+    const float e = (float)eps2;
+#define NBR_GO(a, b)                                                                       \
+  if (c.ni == a && c.warps == b)                                                           \
+    return ex ? launch_f32c_t<a, b, true>(e, c.split, ip, js, ep, st)                      \
+              : launch_f32c_t<a, b, false>(e, c.split, ip, js, ep, st);
+    NBR_CFG_LIST(NBR_GO)
+#undef NBR_GO
+  } else {
+#define NBR_GO(a, b)                                                                       \
+  if (c.ni == a && c.warps == b)                                                           \
+    return ex ? launch_f64_t<a, b, true>(eps2, c.split, ip, js, ep, st)                    \
+              : launch_f64_t<a, b, false>(eps2, c.split, ip, js, ep, st);
+    NBR_CFG_LIST(NBR_GO)
+#undef NBR_GO
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_kick_drift(long long n, long long n_pad, const double* x, const double* y,
+                              const double* z, const double* m, const double* ax,
+                              const double* ay, const double* az, double kick, double drift,
+                              double* vx, double* vy, double* vz, double* xn, double* yn,
+                              double* zn, float4* rec, double4* org, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  const long long warps = (n + kTile - 1) / kTile;
+  const unsigned blocks = (unsigned)((warps + 3) / 4);
+  k_kick_drift<<<blocks, 128, 0, st>>>(n, n_pad, x, y, z, m, ax, ay, az, kick, drift, vx, vy, vz,
+                                       xn, yn, zn, rec, org);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_potential(long long n, long long n_pad, const double* x, const double* y,
+                             const double* z, const double* m, double G, double eps2, double* phi,
+                             double* blocksum, cudaStream_t st) {
+  (void)n_pad;
+  if (n <= 0) return cudaSuccess;
+  const unsigned blocks = (unsigned)((n + 127) / 128);
+  k_potential<<<blocks, 128, 0, st>>>(n, x, y, z, m, G, eps2, phi, blocksum);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_moments(long long n, long long n_pad, const double* x, const double* y,
+                           const double* z, const double* vx, const double* vy, const double* vz,
+                           const double* m, double* part, cudaStream_t st) {
+  (void)n_pad;
+  if (n <= 0) return cudaSuccess;
+  const unsigned blocks = (unsigned)((n + 127) / 128);
+  k_moments<<<blocks, 128, 0, st>>>(n, x, y, z, vx, vy, vz, m, part);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rowsum(const double* part, int nblocks, int width, double* out,
+                          cudaStream_t st) {
+  k_rowsum<<<1, 256, 0, st>>>(part, nblocks, width, out);
+  return cudaGetLastError();
+}
+
+}  // namespace nbr

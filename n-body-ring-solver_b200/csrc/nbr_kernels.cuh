@@ -1,0 +1,90 @@
+// nbr_kernels.cuh -- launch parameters shared by the kernels and the host.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace nbr {
+
+enum Precision : int { kFP64 = 0, kFP32C = 1 };
+
+// Receivers ("i" particles): FP64 positions, read-only during the launch.
+// Arrays are allocated to a multiple of 1024 entries.
+struct IParticles {
+  const double* x;
+  const double* y;
+  const double* z;
+  const double* m;  // receiver masses (used for force output and the pack)
+  long long n;      // real receivers; entries >= n are padding
+};
+
+// Sources ("j" particles), streamed tile by tile.  FP64 form: SoA arrays padded
+// with zero-mass particles to ntiles * kTile.  FP32C form: the pair-duplicated
+// records (3 x 16 B per particle) plus one FP64 origin per tile.
+struct JStream {
+  const double* x;
+  const double* y;
+  const double* z;
+  const double* m;
+  const float4* rec;
+  const double4* origin;
+  int ntiles;
+  unsigned long long wait_ns;  // limit of one bounded tile wait
+  int skip_tile;               // test hook: this CTA-local tile is never copied (-1: off)
+};
+
+// What happens to each receiver's summed acceleration.
+struct Epilogue {
+  int mode;            // 0: write a (or m a);  1: leapfrog kick then drift;
+                       // 2: Euler (drift with the old velocity, then kick)
+  double G;
+  double* ax; double* ay; double* az;   // acceleration (or force) out
+  int want_force;      // mode 0: multiply by the receiver mass
+  // mode 1: v += kick * a;  x' = x + drift * v  (x' into the other buffer)
+  double kick, drift;
+  double* vx; double* vy; double* vz;
+  double* xn; double* yn; double* zn;
+  float4* rec_next;    // FP32C records for x' (nullptr: not needed)
+  double4* origin_next;
+  // split-j reduction
+  double* part;        // [split][3][n_pad]
+  unsigned* counters;  // one per CTA chunk, zero between launches
+  long long n_pad;
+  int* err;            // device error word
+};
+
+struct ForceConfig {
+  int ni;      // receivers per thread (4 or 8)
+  int warps;   // warps per CTA (2, 4 or 8)
+  int split;   // j-range splits (>= 1)
+};
+
+// Host-side launchers (nbr_kernels.cu).
+cudaError_t launch_force(int precision, double eps2, const ForceConfig& cfg, const IParticles& ip,
+                         const JStream& js, const Epilogue& ep, cudaStream_t stream);
+// v += kick a; x' = x + drift v (x' may alias nothing; pass xn = x to pack in place
+// with drift = 0); writes FP32C records of x' when rec_next != nullptr.
+cudaError_t launch_kick_drift(long long n, long long n_pad, const double* x, const double* y,
+                              const double* z, const double* m, const double* ax,
+                              const double* ay, const double* az, double kick, double drift,
+                              double* vx, double* vy, double* vz, double* xn, double* yn,
+                              double* zn, float4* rec_next, double4* origin_next,
+                              cudaStream_t stream);
+// phi_i = -G sum_{j != i} m_j / sqrt(r^2 + eps2), FP64; per-block partial sums
+// of 1/2 m_i phi_i into blocksum[n_pad / 128].
+cudaError_t launch_potential(long long n, long long n_pad, const double* x, const double* y,
+                             const double* z, const double* m, double G, double eps2, double* phi,
+                             double* blocksum, cudaStream_t stream);
+// Per-block partial sums of T, P, L, M (FP64): 8 values per block into part.
+cudaError_t launch_moments(long long n, long long n_pad, const double* x, const double* y,
+                           const double* z, const double* vx, const double* vy, const double* vz,
+                           const double* m, double* part, cudaStream_t stream);
+// Sums nblocks rows of `width` doubles in block order (deterministic).
+cudaError_t launch_rowsum(const double* part, int nblocks, int width, double* out,
+                          cudaStream_t stream);
+size_t force_smem_bytes(int precision, const ForceConfig& cfg);
+// Resident CTAs per SM of the force kernel for this configuration (0 on error).
+int force_blocks_per_sm(int precision, double eps2, const ForceConfig& cfg);
+bool force_config_supported(int precision, const ForceConfig& cfg);
+
+}  // namespace nbr

@@ -1,0 +1,434 @@
+// nbr_main.cpp -- command-line driver with the reference's flag surface.
+//
+// Mirrors CPU/main.cpp: the same flags, defaults and validation
+// (get_arguments, :11-289), dispatch on -t (:291-356), and the reference's
+// experiment drivers re-targeted to the GPU through the C ABI:
+//   -t gpu           omp_main (CPU/omp_solver.cpp:635-797): ring system by
+//                    default, Euler or leapfrog of -order, MPairs/s and the
+//                    deviation from the initial state;
+//   -t gpu-bench     the scaling benchmark's CSV row (CPU/hybrid_solver.cpp:623-645);
+//   -t gpu-accuracy  omp_accuracy (CPU/omp_solver.cpp:899-993);
+//   -t gpu-ratio     omp_ratio_accuracy (CPU/omp_solver.cpp:995-1243);
+//   -t gpu-batch     many independent systems in one persistent launch.
+// Added flags: -eps (softening length), -dt (overrides T/s), -ic
+// ring|plummer|ball|twocomp|random, -seed, -scheme dkd|kdk, -G, -nsys, -nmin,
+// -nmax, -autotune.  -p accepts dp|sp (reference names) and fp64|fp32c;
+// sp selects the FP32-compensated kernel.
+#include <unistd.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <numeric>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "nbr.h"
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+
+struct Args {
+  size_t N = 1000, start_N = 1000, step_N = 1000, num_steps = 1, time_steps = 1000;
+  double T = 1.0, ratio = 100000.0, ratio_start = 1e6, ratio_stop = 1e9;
+  size_t ratio_steps = 3, rev_steps = 1000;
+  double max_error = 1.0;
+  bool verbose = false;
+  std::string output = "output.csv";
+  bool output_given = false;
+  std::string exec = "gpu";
+  std::string integ = "euler";
+  int order = 1;
+  int precision = NBR_FP64;
+  // added
+  double eps = 0.0, dt = 0.0, G = 1.0;
+  std::string ic = "ring";
+  uint64_t seed = 0;
+  int scheme = NBR_DKD;
+  size_t nsys = 4096, nmin = 64, nmax = 4096;
+  bool autotune = false;
+  int device = 0;
+};
+
+bool parse(int argc, char** argv, Args& a) {
+  for (int i = 1; i < argc; ++i) {
+    auto is = [&](const char* f) { return std::strcmp(argv[i], f) == 0 && i + 1 < argc; };
+    if (is("-N")) a.N = std::strtoull(argv[++i], nullptr, 10);
+    else if (is("-start")) a.start_N = std::strtoull(argv[++i], nullptr, 10);
+    else if (is("-step")) a.step_N = std::strtoull(argv[++i], nullptr, 10);
+    else if (is("-n")) a.num_steps = std::strtoull(argv[++i], nullptr, 10);
+    else if (is("-ratio-start")) a.ratio_start = std::atof(argv[++i]);
+    else if (is("-ratio-stop")) a.ratio_stop = std::atof(argv[++i]);
+    else if (is("-ratio-steps")) a.ratio_steps = std::strtoull(argv[++i], nullptr, 10);
+    else if (is("-rev-steps")) a.rev_steps = std::strtoull(argv[++i], nullptr, 10);
+    else if (is("-max-error")) a.max_error = std::atof(argv[++i]);
+    else if (is("-s")) a.time_steps = std::strtoull(argv[++i], nullptr, 10);
+    else if (is("-T")) a.T = std::atof(argv[++i]);
+    else if (is("-r")) a.ratio = std::atof(argv[++i]);
+    else if (std::strcmp(argv[i], "-v") == 0) a.verbose = true;
+    else if (std::strcmp(argv[i], "-autotune") == 0) a.autotune = true;
+    else if (is("-o")) { a.output = argv[++i]; a.output_given = true; }
+    else if (is("-t")) {
+      std::string t = argv[++i];
+      static const char* known[] = {"gpu", "gpu-bench", "gpu-accuracy", "gpu-ratio", "gpu-batch"};
+      bool ok = false;
+      for (auto k : known) ok |= (t == k);
+      if (!ok) {
+        std::printf("Unknown Execution type: %s\n Defaulting to gpu\n", t.c_str());
+        t = "gpu";
+      }
+      a.exec = t;
+    } else if (is("-i")) {
+      std::string k = argv[++i];
+      if (k != "euler" && k != "lf") {
+        std::printf("Unknown or unsupported Integration kind: %s\n Defaulting to euler\n", k.c_str());
+        k = "euler";
+      }
+      a.integ = k;
+    } else if (is("-V") || is("-S")) {
+      ++i;  // CPU vectorisation / Newton-3 choices have no GPU meaning
+    } else if (is("-p")) {
+      std::string k = argv[++i];
+      if (k == "dp" || k == "fp64") a.precision = NBR_FP64;
+      else if (k == "sp" || k == "fp32c") a.precision = NBR_FP32C;
+      else std::printf("Unknown Data type: %s\n Defaulting to double precision\n", k.c_str());
+    } else if (is("-order")) a.order = (int)std::strtoull(argv[++i], nullptr, 10);
+    else if (is("-eps")) a.eps = std::atof(argv[++i]);
+    else if (is("-dt")) a.dt = std::atof(argv[++i]);
+    else if (is("-G")) a.G = std::atof(argv[++i]);
+    else if (is("-ic")) a.ic = argv[++i];
+    else if (is("-seed")) a.seed = std::strtoull(argv[++i], nullptr, 10);
+    else if (is("-scheme")) a.scheme = std::strcmp(argv[++i], "kdk") == 0 ? NBR_KDK : NBR_DKD;
+    else if (is("-nsys")) a.nsys = std::strtoull(argv[++i], nullptr, 10);
+    else if (is("-nmin")) a.nmin = std::strtoull(argv[++i], nullptr, 10);
+    else if (is("-nmax")) a.nmax = std::strtoull(argv[++i], nullptr, 10);
+    else if (is("-device")) a.device = std::atoi(argv[++i]);
+  }
+  // Validation and resets of CPU/main.cpp:271-288.
+  if (a.N >= 100000000 || a.start_N >= 100000000 ||
+      a.start_N + a.step_N * a.num_steps >= 100000000) {
+    std::printf("Input problem size might be too large!\nMake sure to stay below 10^8 particles.\nResetting to defaults");
+    a.N = 1000; a.start_N = 1000; a.step_N = 1000; a.num_steps = 1;
+  }
+  if (a.T <= 0.0) { std::printf("T has to be >= 0!\n Resetting to 1.0\n"); a.T = 1.0; }
+  if (a.ratio < 0.0) { std::printf("ratio has to be >= 0!\n Resetting to 1e6\n"); a.ratio = 1e6; }
+  return true;
+}
+
+struct State {
+  size_t n = 0;
+  std::vector<double> x, y, z, vx, vy, vz, m, fx, fy, fz;
+  void resize(size_t k) {
+    n = k;
+    for (auto* v : {&x, &y, &z, &vx, &vy, &vz, &m, &fx, &fy, &fz}) v->assign(k, 0.0);
+  }
+};
+
+int make_ic(const Args& a, size_t n, double ratio, State& s) {
+  s.resize(n);
+  if (a.ic == "ring")
+    return nbr_ic_ring(n, 1.0, 2.0 * kPi, ratio, s.x.data(), s.y.data(), s.z.data(), s.vx.data(),
+                       s.vy.data(), s.vz.data(), s.m.data(), s.fx.data(), s.fy.data(), s.fz.data());
+  if (a.ic == "plummer")
+    return nbr_ic_plummer(n, a.seed, s.x.data(), s.y.data(), s.z.data(), s.vx.data(), s.vy.data(),
+                          s.vz.data(), s.m.data());
+  if (a.ic == "ball")
+    return nbr_ic_uniform_ball(n, a.seed, s.x.data(), s.y.data(), s.z.data(), s.vx.data(),
+                               s.vy.data(), s.vz.data(), s.m.data());
+  if (a.ic == "twocomp")
+    return nbr_ic_two_component(n, (size_t)std::llround(0.01 * double(n)), 1000.0, a.seed,
+                                s.x.data(), s.y.data(), s.z.data(), s.vx.data(), s.vy.data(),
+                                s.vz.data(), s.m.data());
+  if (a.ic == "random") {
+    // The reference's init_particles (CPU/nbody_system.cpp:238-274) with a seed:
+    // masses U(0, 1e6), positions U(-1, 1), velocities U(-0.01, 0.01).
+    std::mt19937_64 g(a.seed);
+    auto u = [&](double lo, double hi) { return lo + (hi - lo) * (double(g() >> 11) * 0x1.0p-53); };
+    for (size_t i = 0; i < n; ++i) {
+      s.m[i] = u(0.0, 1e6);
+      s.x[i] = u(-1, 1); s.y[i] = u(-1, 1); s.z[i] = u(-1, 1);
+      s.vx[i] = u(-0.01, 0.01); s.vy[i] = u(-0.01, 0.01); s.vz[i] = u(-0.01, 0.01);
+    }
+    return NBR_OK;
+  }
+  std::printf("Unknown initial condition %s\n", a.ic.c_str());
+  return NBR_ERR_INVALID_ARG;
+}
+
+// print_deviation (CPU/nbody_system.cpp:500-519): mean |calc - ref|.
+void print_deviation(const std::vector<double>& cx, const std::vector<double>& cy,
+                     const std::vector<double>& cz, const State& r, bool vel, const char* kind) {
+  const auto& rx = vel ? r.vx : r.x;
+  const auto& ry = vel ? r.vy : r.y;
+  const auto& rz = vel ? r.vz : r.z;
+  double mean = 0.0;
+  for (size_t i = 0; i < cx.size(); ++i)
+    mean += std::sqrt((cx[i] - rx[i]) * (cx[i] - rx[i]) + (cy[i] - ry[i]) * (cy[i] - ry[i]) +
+                      (cz[i] - rz[i]) * (cz[i] - rz[i]));
+  mean /= double(cx.size());
+  std::printf("Average %s deviation from reference: %.13f\n", kind, mean);
+}
+
+// calculate_deviation (CPU/nbody_system.cpp:521-540): mean distance and the
+// largest relative length error.
+void deviation(const double* cx, const double* cy, const double* cz, const double* rx,
+               const double* ry, const double* rz, size_t n, double& mean, double& maxlen) {
+  mean = 0.0;
+  maxlen = 0.0;
+  for (size_t i = 0; i < n; ++i) {
+    const double dx = cx[i] - rx[i], dy = cy[i] - ry[i], dz = cz[i] - rz[i];
+    mean += std::sqrt(dx * dx + dy * dy + dz * dz);
+    const double lc = std::sqrt(cx[i] * cx[i] + cy[i] * cy[i] + cz[i] * cz[i]);
+    const double lr = std::sqrt(rx[i] * rx[i] + ry[i] * ry[i] + rz[i] * rz[i]);
+    if (lr > 0.0 && std::fabs(lc - lr) / lr > maxlen) maxlen = std::fabs(lc - lr) / lr;
+  }
+  mean /= double(n);
+}
+
+bool file_exists(const std::string& p) { return access(p.c_str(), F_OK) != -1; }
+
+int run_gpu(nbr_ctx* ctx, const Args& a, bool bench) {
+  State s;
+  if (make_ic(a, a.N, a.ratio, s) != NBR_OK) return 1;
+  State ref = s;
+  const double dt = a.dt > 0.0 ? a.dt : a.T / double(a.time_steps);
+  const double eps2 = a.eps * a.eps;
+  std::printf("N = %zu, s = %zu\n", a.N, a.time_steps);
+  if (nbr_system_upload(ctx, s.n, s.x.data(), s.y.data(), s.z.data(), s.vx.data(), s.vy.data(),
+                        s.vz.data(), s.m.data()) != NBR_OK) {
+    std::printf("upload failed: %s\n", nbr_last_error_string(ctx));
+    return 1;
+  }
+  if (a.autotune) nbr_autotune(ctx, a.precision, eps2);
+  nbr_diag d[2];
+  nbr_run_stats st{};
+  int rc;
+  double evals_per_step = 1.0;
+  auto t0 = std::chrono::steady_clock::now();
+  if (a.integ == "lf") {
+    const int order = a.order < 2 ? 2 : a.order;
+    double c[16], dd[16];
+    const int lf = nbr_yoshida_coefficients(order, c, dd);
+    const int use_order = lf ? order : 2;
+    if (!lf) std::printf("Order %d not supported! Defaulting to 2nd order\n", order);
+    if (a.scheme == NBR_KDK && use_order != 2) {
+      std::printf("KDK is second order; using DKD for order %d\n", use_order);
+    }
+    const int scheme = use_order == 2 ? a.scheme : NBR_DKD;
+    evals_per_step = scheme == NBR_DKD ? double((lf ? lf : 2) - 1) : 1.0;
+    rc = nbr_run(ctx, a.precision, scheme, use_order, dt, a.time_steps, a.G, eps2, d, &st);
+  } else {
+    rc = nbr_run(ctx, a.precision, NBR_EULER, 1, dt, a.time_steps, a.G, eps2, d, &st);
+  }
+  auto t1 = std::chrono::steady_clock::now();
+  if (rc != NBR_OK) {
+    std::printf("run failed: %s\n", nbr_last_error_string(ctx));
+    return 1;
+  }
+  const double wall = std::chrono::duration<double>(t1 - t0).count();
+  const double t_gpu = st.gpu_ms * 1e-3;
+  const double pairs = double(a.time_steps) * evals_per_step * double(a.N) * double(a.N - 1);
+  const double mpairs = t_gpu > 0 ? pairs / (1e6 * t_gpu) : 0.0;
+  std::printf("GPU %s solver took %fs (wall %fs)\n", a.integ == "lf" ? "symplectic" : "Euler", t_gpu, wall);
+  std::printf("Performance: %fMPairs/s\n", mpairs);
+  std::printf("Energy: E0 = %.12e  E1 = %.12e  |dE/E0| = %.3e\n", d[0].E, d[1].E,
+              d[0].E != 0.0 ? std::fabs((d[1].E - d[0].E) / d[0].E) : 0.0);
+  std::vector<double> x(a.N), y(a.N), z(a.N), vx(a.N), vy(a.N), vz(a.N);
+  nbr_system_download(ctx, x.data(), y.data(), z.data(), vx.data(), vy.data(), vz.data());
+  print_deviation(x, y, z, ref, false, "position");
+  print_deviation(vx, vy, vz, ref, true, "velocity");
+  if (bench || a.output_given) {
+    const bool exists = file_exists(a.output);
+    FILE* f = std::fopen(a.output.c_str(), exists ? "a" : "w");
+    if (!f) {
+      std::perror("Failed to open output file: ");
+      return 1;
+    }
+    if (!exists)
+      std::fprintf(f, "#Nodes, Cores, N, t_total[s], performance[Mpairs/s], time_steps/s, ms/time_step\n");
+    std::fprintf(f, "%d,%d,%zu,%f,%f,%f,%f\n", 1, nbr_device_count() > 0 ? 148 : 0, a.N, t_gpu,
+                 mpairs, double(a.time_steps) / t_gpu, t_gpu * 1000.0 / double(a.time_steps));
+    std::fclose(f);
+  }
+  return 0;
+}
+
+// omp_accuracy on the GPU: one force evaluation of the permuted ring against
+// the analytic ring forces, averaged length and angle errors in percent.
+int run_accuracy(nbr_ctx* ctx, const Args& a) {
+  const bool exists = file_exists(a.output);
+  FILE* f = std::fopen(a.output.c_str(), exists ? "a" : "w");
+  if (!f) { std::perror("Failed to open output file: "); return 1; }
+  if (!exists)
+    std::fprintf(f, "N, precision, ratio, average_force_length_error[%%], average_force_angle_error[%%]\n");
+  const double root = std::pow(a.ratio_stop / a.ratio_start, 1.0 / double(a.ratio_steps));
+  for (size_t rs = 0; rs <= a.ratio_steps; ++rs) {
+    const double ratio = a.ratio_start * std::pow(root, double(rs));
+    for (size_t k = 0; k < a.num_steps; ++k) {
+      const size_t n = a.start_N * size_t(std::llround(std::pow(double(a.step_N), double(k))));
+      Args ring = a;
+      ring.ic = "ring";
+      State s;
+      make_ic(ring, n, ratio, s);
+      std::vector<size_t> perm(n);
+      std::iota(perm.begin(), perm.end(), 0);
+      std::mt19937_64 g(a.seed);
+      std::shuffle(perm.begin(), perm.end(), g);
+      State p = s;
+      for (size_t i = 0; i < n; ++i) {
+        p.x[i] = s.x[perm[i]]; p.y[i] = s.y[perm[i]]; p.z[i] = s.z[perm[i]];
+        p.m[i] = s.m[perm[i]];
+        p.fx[i] = s.fx[perm[i]]; p.fy[i] = s.fy[perm[i]]; p.fz[i] = s.fz[perm[i]];
+      }
+      if (nbr_system_upload(ctx, n, p.x.data(), p.y.data(), p.z.data(), nullptr, nullptr, nullptr,
+                            p.m.data()) != NBR_OK) {
+        std::printf("upload failed: %s\n", nbr_last_error_string(ctx));
+        std::fclose(f);
+        return 1;
+      }
+      std::vector<double> fx(n), fy(n), fz(n);
+      if (nbr_forces(ctx, a.precision, 1.0, 0.0, 1, fx.data(), fy.data(), fz.data()) != NBR_OK) {
+        std::printf("forces failed: %s\n", nbr_last_error_string(ctx));
+        std::fclose(f);
+        return 1;
+      }
+      // calculate_force_error (CPU/nbody_system.cpp:542-652): angle in the
+      // x-y plane, normalised by 2 pi; length error normalised by the length
+      // of particle 0's reference force.
+      double ang = 0.0, len = 0.0;
+      for (size_t i = 0; i < n; ++i) {
+        const double sl = std::sqrt(fx[i] * fx[i] + fy[i] * fy[i] + fz[i] * fz[i]);
+        const double rl = std::sqrt(p.fx[i] * p.fx[i] + p.fy[i] * p.fy[i] + p.fz[i] * p.fz[i]);
+        const double dot = fx[i] * p.fx[i] + fy[i] * p.fy[i];
+        const double det = fx[i] * p.fy[i] - fy[i] * p.fx[i];
+        if (p.fx[i] != 0.0 && p.fy[i] != 0.0) ang += std::fabs(std::atan2(det, dot));
+        len += std::fabs(sl - rl);
+      }
+      const double r0 = std::sqrt(p.fx[0] * p.fx[0] + p.fy[0] * p.fy[0] + p.fz[0] * p.fz[0]);
+      const double len_err = r0 > 0 ? len / (r0 * double(n)) : 0.0;
+      const double ang_err = ang / (2.0 * kPi * double(n));
+      std::printf("N = %zu ratio = %.3e: length error %.6e, angle error %.6e\n", n, ratio, len_err, ang_err);
+      std::fprintf(f, "%zu, %s, %.5e, %.5e, %.6e\n", n, a.precision == NBR_FP64 ? "dp" : "sp", ratio,
+                   len_err * 100.0, ang_err * 100.0);
+    }
+  }
+  std::fclose(f);
+  return 0;
+}
+
+// omp_ratio_accuracy on the GPU: DKD order 2 with dt = 1 / rev_steps, each
+// step compared with the analytic rigid rotation and the initial energy;
+// stops at the collapse criterion of CPU/omp_solver.cpp:1215.
+int run_ratio(nbr_ctx* ctx, const Args& a) {
+  const bool exists = file_exists(a.output);
+  FILE* f = std::fopen(a.output.c_str(), exists ? "a" : "w");
+  if (!f) { std::perror("Failed to open output file: "); return 1; }
+  if (!exists)
+    std::fprintf(f, "N, precision, s, s_collapse, ratio, max_error, last_E_dev, last_avg_pos_dev, last_avg_vel_dev, max_pos_dev, max_vel_dev\n");
+  const double dt = 1.0 / double(a.rev_steps);
+  for (size_t k = 0; k < a.num_steps; ++k) {
+    const size_t n = a.start_N + k * a.step_N;
+    const double root = std::pow(a.ratio_stop / a.ratio_start, 1.0 / double(a.ratio_steps));
+    for (size_t rs = 0; rs <= a.ratio_steps; ++rs) {
+      const double ratio = a.ratio_start * std::pow(root, double(rs));
+      Args ring = a;
+      ring.ic = "ring";
+      State s;
+      make_ic(ring, n, ratio, s);
+      if (nbr_system_upload(ctx, n, s.x.data(), s.y.data(), s.z.data(), s.vx.data(), s.vy.data(),
+                            s.vz.data(), s.m.data()) != NBR_OK) {
+        std::fclose(f);
+        return 1;
+      }
+      nbr_diag d0;
+      nbr_diagnostics(ctx, 1.0, 0.0, &d0);
+      size_t s_collapse = a.time_steps;
+      double e_sol = 0, ap = 0, av = 0, mp = 0, mv = 0;
+      std::vector<double> x(n), y(n), z(n), vx(n), vy(n), vz(n);
+      std::vector<double> px(n), py(n), pz(n), pvx(n), pvy(n), pvz(n);
+      for (size_t t = 1; t <= a.time_steps; ++t) {
+        nbr_diag d[2];
+        if (nbr_run(ctx, a.precision, NBR_DKD, 2, dt, 1, 1.0, 0.0, d, nullptr) != NBR_OK) {
+          std::printf("run failed: %s\n", nbr_last_error_string(ctx));
+          std::fclose(f);
+          return 1;
+        }
+        nbr_system_download(ctx, x.data(), y.data(), z.data(), vx.data(), vy.data(), vz.data());
+        nbr_ic_ring_predict(n, 1.0, 2.0 * kPi, t, a.rev_steps, px.data(), py.data(), pz.data(),
+                            pvx.data(), pvy.data(), pvz.data());
+        double pmean, pmax, vmean, vmax;
+        deviation(x.data(), y.data(), z.data(), px.data(), py.data(), pz.data(), n, pmean, pmax);
+        deviation(vx.data(), vy.data(), vz.data(), pvx.data(), pvy.data(), pvz.data(), n, vmean, vmax);
+        const double edev = std::fabs((d0.E - d[1].E) / d0.E);
+        if (edev >= 1.0 || pmax >= a.max_error || vmax >= a.max_error) {
+          s_collapse = t;
+          break;
+        }
+        e_sol = edev; ap = pmean; av = vmean; mp = pmax; mv = vmax;
+      }
+      std::printf("true solution = %zu\n", s_collapse);
+      std::fprintf(f, "%zu, %s, %zu, %zu, %f, %f, %f, %f, %f, %f, %f\n", n,
+                   a.precision == NBR_FP64 ? "dp" : "sp", a.time_steps, s_collapse, ratio,
+                   a.max_error, e_sol, ap, av, mp, mv);
+    }
+  }
+  std::fclose(f);
+  return 0;
+}
+
+int run_batch(nbr_ctx* ctx, const Args& a) {
+  std::vector<size_t> sizes(a.nsys), off(a.nsys + 1, 0);
+  nbr_ic_batch_sizes(a.nsys, a.seed, a.nmin, a.nmax, sizes.data());
+  for (size_t s = 0; s < a.nsys; ++s) off[s + 1] = off[s] + sizes[s];
+  const size_t n = off[a.nsys];
+  State st;
+  st.resize(n);
+  for (size_t s = 0; s < a.nsys; ++s) {
+    const size_t o = off[s];
+    nbr_ic_plummer(sizes[s], nbr_ic_system_seed(a.seed, s), st.x.data() + o, st.y.data() + o,
+                   st.z.data() + o, st.vx.data() + o, st.vy.data() + o, st.vz.data() + o,
+                   st.m.data() + o);
+  }
+  if (nbr_batch_upload(ctx, a.nsys, off.data(), st.x.data(), st.y.data(), st.z.data(), st.vx.data(),
+                       st.vy.data(), st.vz.data(), st.m.data()) != NBR_OK) {
+    std::printf("batch upload failed: %s\n", nbr_last_error_string(ctx));
+    return 1;
+  }
+  const double dt = a.dt > 0.0 ? a.dt : a.T / double(a.time_steps);
+  nbr_run_stats rs{};
+  if (nbr_batch_run(ctx, a.precision, dt, a.time_steps, a.G, a.eps * a.eps, &rs) != NBR_OK) {
+    std::printf("batch run failed: %s\n", nbr_last_error_string(ctx));
+    return 1;
+  }
+  const double secs = rs.gpu_ms * 1e-3;
+  std::printf("systems = %zu, particles = %zu, steps = %zu\n", a.nsys, n, a.time_steps);
+  std::printf("GPU batched solver took %fs: %.1f systems*steps/s, %.3f GPairs/s\n", secs,
+              double(a.nsys) * double(a.time_steps) / secs, rs.pairs / secs * 1e-9);
+  return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  Args a;
+  parse(argc, argv, a);
+  nbr_ctx* ctx = nullptr;
+  if (nbr_ctx_create(a.device, &ctx) != NBR_OK) {
+    std::printf("No GPU context: %s\n", nbr_last_error_string(nullptr));
+    return 1;
+  }
+  int rc = 0;
+  if (a.exec == "gpu") rc = run_gpu(ctx, a, false);
+  else if (a.exec == "gpu-bench") rc = run_gpu(ctx, a, true);
+  else if (a.exec == "gpu-accuracy") rc = run_accuracy(ctx, a);
+  else if (a.exec == "gpu-ratio") rc = run_ratio(ctx, a);
+  else if (a.exec == "gpu-batch") rc = run_batch(ctx, a);
+  nbr_ctx_destroy(ctx);
+  return rc;
+}

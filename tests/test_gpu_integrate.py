@@ -1,0 +1,221 @@
+"""GPU integrator parity through the C ABI.
+
+  * DKD (Yoshida order 2/4/6/8) and Euler against the reference's own solver
+    (golden fixtures from reduced_solver_omp_lf / reduced_solver_omp, eps = 0):
+    positions and velocities within 1e-11 of the value scale;
+  * KDK against the oracle on the softened Plummer workload (N = 2048, seed 0,
+    eps = 1e-3, dt = 1e-3, 100 steps): within 1e-10 absolute (chaotic growth
+    of rounding differences over 100 steps measured at ~1e-14 on the CPU);
+  * the reference's analytic ring rotation and energy conservation.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+FP64, FP32C = 0, 1
+KDK, DKD, EULER = 0, 1, 2
+KEYS6 = ("x", "y", "z", "vx", "vy", "vz")
+
+
+def _split(fx):
+    return {k[3:]: v for k, v in fx.items() if k.startswith("in_")}, \
+           {k[4:]: v for k, v in fx.items() if k.startswith("out_")}
+
+
+def assert_state_close(got, want, rel):
+    for k in KEYS6:
+        scale = max(np.abs(want[k]).max(), 1e-300)
+        assert np.abs(got[k] - want[k]).max() <= rel * scale, (k, np.abs(got[k] - want[k]).max() / scale)
+
+
+@pytest.mark.parametrize("order", [2, 4, 6, 8])
+def test_dkd_matches_reference_lf(ctx, order):
+    g = golden(f"ref_lf_order{order}_plummer_n256.npz")
+    s_in, s_out = _split(g)
+    ctx.upload(s_in)
+    st = ctx.run(FP64, DKD, order, float(g["dt"]), int(g["steps"]), eps2=0.0)
+    lf = {2: 2, 4: 4, 6: 8, 8: 16}[order]
+    assert st["force_evals"] == int(g["steps"]) * (lf - 1)
+    assert_state_close(ctx.download(), s_out, 1e-11)
+
+
+def test_euler_matches_reference(ctx):
+    g = golden("ref_euler_plummer_n256.npz")
+    s_in, s_out = _split(g)
+    ctx.upload(s_in)
+    ctx.run(FP64, EULER, 1, float(g["dt"]), int(g["steps"]), eps2=0.0)
+    assert_state_close(ctx.download(), s_out, 1e-11)
+
+
+def test_dkd_matches_live_reference_ring(ctx, nbr, reference):
+    r = nbr.ring(1001, ratio=1e5)
+    s = {k: r[k] for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+    want, _ = reference.lf(s, 1e-3, 20, order=2)
+    ctx.upload(s)
+    ctx.run(FP64, DKD, 2, 1e-3, 20, eps2=0.0)
+    assert_state_close(ctx.download(), want, 1e-11)
+
+
+def test_kdk_matches_oracle_plummer_2048(ctx, nbr, oracle):
+    s = nbr.plummer(2048, 0)
+    eps2 = 1e-6
+    want = oracle.kdk(s, 1e-3, 100, eps2=eps2)
+    ctx.upload(s)
+    st = ctx.run(FP64, KDK, 2, 1e-3, 100, eps2=eps2, diag=True)
+    assert st["force_evals"] == 101  # one initial evaluation, then one per step
+    got = ctx.download()
+    for k in KEYS6:
+        assert np.abs(got[k] - want[k]).max() <= 1e-10, k
+    e0, e1 = st["diag"]
+    ref0 = oracle.energy(s, eps2=eps2)
+    ref1 = oracle.energy(want, eps2=eps2)
+    assert abs(e0["E"] - ref0["E"]) <= 1e-12 * abs(ref0["E"])
+    assert abs(e1["E"] - ref1["E"]) <= 1e-9 * abs(ref1["E"])
+
+
+def test_kdk_first_same_as_last(ctx, nbr):
+    """Two runs of 25 steps equal one run of 50: the second reuses the force."""
+    s = nbr.plummer(3000, 6)
+    ctx.upload(s)
+    ctx.run(FP64, KDK, 2, 1e-3, 50, eps2=1e-6)
+    one = ctx.download()
+    ctx.upload(s)
+    a = ctx.run(FP64, KDK, 2, 1e-3, 25, eps2=1e-6)
+    b = ctx.run(FP64, KDK, 2, 1e-3, 25, eps2=1e-6)
+    assert a["force_evals"] == 26 and b["force_evals"] == 25
+    two = ctx.download()
+    for k in KEYS6:
+        np.testing.assert_allclose(two[k], one[k], rtol=0, atol=1e-13 * max(1.0, np.abs(one[k]).max()))
+
+
+def test_ring_rotation_known_answer(ctx, nbr):
+    """The reference's ring experiment: after one revolution (dt = 1/1000,
+    1000 DKD steps) every ring particle is back near its start
+    (CPU/omp_solver.cpp:1164-1228)."""
+    n = 257
+    r = nbr.ring(n, ratio=1e6)
+    s = {k: r[k] for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+    ctx.upload(s)
+    for chunk in range(4):
+        ctx.run(FP64, DKD, 2, 1e-3, 250, eps2=0.0)
+        want = nbr.ring_predict(n, 250 * (chunk + 1), 1000)
+        got = ctx.download()
+        d = np.sqrt((got["x"] - want["x"]) ** 2 + (got["y"] - want["y"]) ** 2)
+        assert d[:-1].max() < 1e-3, (chunk, d.max())
+
+
+@pytest.mark.parametrize("order", [4, 6, 8])
+def test_higher_order_is_more_accurate(ctx, nbr, order):
+    n = 129
+    r = nbr.ring(n, ratio=1e6)
+    s = {k: r[k] for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+    errs = {}
+    for o in (2, order):
+        ctx.upload(s)
+        ctx.run(FP64, DKD, o, 1e-2, 100, eps2=0.0)
+        got = ctx.download()
+        want = nbr.ring_predict(n, 100, 100)
+        errs[o] = np.sqrt((got["x"] - want["x"]) ** 2 + (got["y"] - want["y"]) ** 2)[:-1].max()
+    assert errs[order] < errs[2] / 10
+
+
+def test_fp32c_energy_drift_within_twice_fp64(ctx, nbr):
+    """Cold collapse of a uniform ball (N = 32768, eps = 1e-2, dt = 1e-4): the
+    FP32C run conserves energy as well as the FP64 run (within 2x, plus a
+    floor at the FP64 diagnostic's own precision)."""
+    s = nbr.uniform_ball(32768, 1)
+    drift = {}
+    for prec in (FP64, FP32C):
+        ctx.upload(s)
+        st = ctx.run(prec, KDK, 2, 1e-4, 200, eps2=1e-4, diag=True)
+        e0, e1 = st["diag"]
+        drift[prec] = abs(e1["E"] - e0["E"]) / abs(e0["E"])
+    assert drift[FP32C] <= 2 * drift[FP64] + 1e-9, drift
+
+
+def test_fp32c_trajectory_tracks_fp64(ctx, nbr):
+    s = nbr.plummer(2048, 0)
+    out = {}
+    for prec in (FP64, FP32C):
+        ctx.upload(s)
+        ctx.run(prec, KDK, 2, 1e-3, 100, eps2=1e-6)
+        out[prec] = ctx.download()
+    d = np.sqrt(sum((out[FP32C][k] - out[FP64][k]) ** 2 for k in ("x", "y", "z")))
+    assert np.median(d) <= 1e-7 and d.max() <= 1e-4
+
+
+def test_momentum_conserved(ctx, nbr):
+    s = nbr.two_component(8192, 82, 1000.0, 4)
+    ctx.upload(s)
+    st = ctx.run(FP32C, KDK, 2, 2e-4, 50, eps2=1e-6, diag=True)
+    e0, e1 = st["diag"]
+    assert np.abs(np.array(e1["P"]) - np.array(e0["P"])).max() <= 1e-9
+    assert np.abs(np.array(e1["L"]) - np.array(e0["L"])).max() <= 1e-8
+
+
+def test_run_rejects_bad_arguments(ctx, nbr):
+    ctx.upload(nbr.plummer(100, 1))
+    for args in ((FP64, KDK, 4), (FP64, DKD, 3), (FP64, 9, 2), (5, KDK, 2)):
+        with pytest.raises(nbr.NbrError):
+            ctx.run(*args, dt=1e-3, steps=1)
+    with pytest.raises(nbr.NbrError):
+        ctx.run(FP64, KDK, 2, dt=float("nan"), steps=1)
+    st = ctx.run(FP64, KDK, 2, dt=1e-3, steps=0)
+    assert st["force_evals"] == 0
+
+
+def test_adapter_drop_in(tmp_path, nbr):
+    """The reference-signature adapter (include/nbr_compute_forces.hpp) used the
+    way reduced_solver_omp and hybrid_ring_solver call compute_forces_*:
+    accumulating into force, recv_force untouched, ring rounds summed."""
+    import os
+    import subprocess
+    from conftest import PKG, ROOT
+    g = golden("ref_forces_random_n1000.npz")
+    src = tmp_path / "drop_in.cpp"
+    src.write_text(r'''
+#include <cstdio>
+#include <vector>
+#include "nbr_compute_forces.hpp"
+struct Sys { size_t N; double* mass; double* pos[3]; double* vel[3]; double* force[3];
+             static constexpr double G = 1; };
+int main(int argc, char** argv) {
+  size_t n = 1000; std::vector<double> buf(7 * n);
+  FILE* f = std::fopen(argv[1], "rb"); std::fread(buf.data(), 8, 4 * n, f); std::fclose(f);
+  Sys s; s.N = n; s.pos[0] = &buf[0]; s.pos[1] = &buf[n]; s.pos[2] = &buf[2 * n]; s.mass = &buf[3 * n];
+  for (int d = 0; d < 3; ++d) s.force[d] = &buf[(4 + d) * n];
+  std::vector<double> rf(3 * n, 0.0); double* recv_force[3] = {&rf[0], &rf[n], &rf[2 * n]};
+  // comm_sz = 1: the whole system (reduced_solver_omp's call)
+  for (size_t i = 0; i < 3 * n; ++i) buf[4 * n + i] = 0.0;
+  compute_forces_gpu(s, s.pos, recv_force, nullptr, nullptr, n, 0, 1, 0, 1);
+  if (nbr_dropin::last_status() != NBR_OK) return 2;
+  f = std::fopen(argv[2], "wb"); std::fwrite(&buf[4 * n], 8, 3 * n, f);
+  // comm_sz = 4, rank 0: four ring rounds over blocks of 250 (hybrid_ring_solver)
+  size_t L = n / 4;
+  for (size_t i = 0; i < 3 * n; ++i) buf[4 * n + i] = 0.0;
+  for (size_t r = 0; r < 4; ++r) {
+    double* rp[3] = {&buf[r * L], &buf[n + r * L], &buf[2 * n + r * L]};
+    compute_forces_gpu(s, rp, recv_force, nullptr, nullptr, L, 0, 4, r, 1);
+  }
+  std::fwrite(&buf[4 * n], 8, L, f); std::fwrite(&buf[5 * n], 8, L, f); std::fwrite(&buf[6 * n], 8, L, f);
+  std::fclose(f);
+  for (double v : rf) if (v != 0.0) return 3;
+  return nbr_dropin::last_status();
+}
+''')
+    exe = tmp_path / "drop_in"
+    subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include"), str(src),
+                    "-L", PKG, "-lnbr", f"-Wl,-rpath,{PKG}", "-o", str(exe)], check=True)
+    inp = tmp_path / "in.bin"
+    np.concatenate([g["x"], g["y"], g["z"], g["m"]]).tofile(inp)
+    out = tmp_path / "out.bin"
+    subprocess.run([str(exe), str(inp), str(out)], check=True)
+    res = np.fromfile(out)
+    F_full = res[:3000].reshape(3, 1000)
+    F_block = res[3000:].reshape(3, 250)
+    from conftest import rel_err
+    assert rel_err(F_full, g["F_simple"]).max() <= 1e-12
+    assert rel_err(F_block, g["F_simple"][:, :250]).max() <= 1e-12
