@@ -240,7 +240,11 @@ ForceConfig choose_config(nbr_ctx* c, int precision, double eps2, long long n_i,
     std::lock_guard<std::mutex> g(g_tune_mu);
     load_tune_locked();
     auto it = g_tune->find(tune_key(precision, n_i, ntiles, eps2 == 0.0));
-    cfg = it != g_tune->end() ? it->second : ForceConfig{4, 4, 0};
+    // Defaults from a configuration sweep on B200 (N = 32768 .. 262144):
+    // FP32C is FMA-pipe bound and gains from 4 receiver pairs per thread;
+    // FP64 has twice the registers per receiver and prefers 4 per thread.
+    const ForceConfig dflt = precision == kFP32C ? ForceConfig{8, 2, 0} : ForceConfig{4, 4, 0};
+    cfg = it != g_tune->end() ? it->second : dflt;
   }
   if (cfg.split <= 0) cfg.split = auto_split(precision, eps2, cfg, n_i, ntiles, c->sms);
   if (cfg.split > ntiles) cfg.split = std::max(1, ntiles);
