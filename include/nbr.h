@@ -120,6 +120,36 @@ int nbr_forces_device(nbr_ctx* ctx, int precision, double G, double eps2);
 /* Copies the accelerations left by nbr_forces_device / nbr_run to the host. */
 int nbr_forces_download(nbr_ctx* ctx, double* ax, double* ay, double* az);
 
+/* Largest particle count nbr_forces_noalloc accepts. */
+#define NBR_NOALLOC_MAX_N 32768
+
+/* Accelerations of n particles (FP64 or FP32C, as nbr_forces with
+ * want_force = 0) computed without allocating anything.  This entry point has
+ * no counterpart in the reference.  It exists for callers that cannot let a
+ * library allocate device memory: an application whose memory pool owns every
+ * device allocation, a process held to a fixed device-memory budget, or a
+ * latency-critical loop that cannot afford the synchronisation cudaMalloc and
+ * cudaFree may imply.  The caller provides the inputs and outputs; all
+ * scratch lives in one static device array inside libnbr.so (about 8.5 MB),
+ * which every GPU that loads the library holds until the process exits.
+ *  - x, y, z, m (n entries) and ax, ay, az (n entries) are device-accessible
+ *    pointers (device, managed or mapped pinned memory) owned by the caller;
+ *  - n <= NBR_NOALLOC_MAX_N, else NBR_ERR_INVALID_ARG and nothing runs;
+ *  - stream: a cudaStream_t (NULL for the default stream); the call returns
+ *    after the work on that stream has finished, so a bounded-wait timeout can
+ *    be reported (NBR_ERR_TIMEOUT);
+ *  - the first call on a device looks up the scratch array's device address
+ *    (cudaGetSymbolAddress, with that device current); make that first call
+ *    before any stream capture;
+ *  - all calls on a device share the scratch array, which keeps the last
+ *    call's contents (each call clears what must start at zero); calls that
+ *    overlap on the same GPU, from several streams or host threads, race on it
+ *    and must be serialised by the caller.
+ * Errors are reported through nbr_last_error_string(NULL). */
+int nbr_forces_noalloc(int precision, size_t n, const double* x, const double* y, const double* z,
+                       const double* m, double G, double eps2, double* ax, double* ay, double* az,
+                       void* stream);
+
 /* Accelerations or forces on n_i receivers from n_j sources (separate sets).
  * The block-pair call the reference's ring decomposition makes for a received
  * block (compute_forces_* with local_N, rank, comm_sz, recv_round,

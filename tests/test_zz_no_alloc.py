@@ -1,0 +1,67 @@
+"""The no-allocation force entry point (nbr_forces_noalloc), called through the
+C ABI with caller-owned device buffers, must give what the ordinary entry
+point nbr_forces gives.
+
+Some callers cannot let a library allocate device memory (their memory pool
+owns every allocation, or they run under a fixed device-memory budget, or a
+cudaMalloc's synchronisation is too costly in their loop); this entry point
+keeps all of its scratch in a static device array instead.  Two calls in a
+row, with different sizes, check that the shared scratch is cleared and
+reused correctly.  This file is collected last on purpose.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+FP64, FP32C = 0, 1
+# per-particle relative tolerance, as in the other parity tests
+TOL = {FP64: 1e-12, FP32C: 1e-6}
+
+
+def _entry(nbr):
+    lib = nbr.load()
+    f = lib.nbr_forces_noalloc
+    f.argtypes = [C.c_int, C.c_size_t] + [C.c_void_p] * 4 + [C.c_double, C.c_double] + \
+                 [C.c_void_p] * 3 + [C.c_void_p]
+    f.restype = C.c_int
+    return lib, f
+
+
+def _rel(a, b):
+    num = np.linalg.norm(a - b, axis=0)
+    den = np.linalg.norm(b, axis=0)
+    return num / np.where(den > 0, den, 1.0)
+
+
+@pytest.mark.parametrize("prec", [FP64, FP32C])
+def test_noalloc_matches_nbr_forces_two_calls(nbr, prec):
+    import torch
+    lib, f = _entry(nbr)
+    eps2 = 1e-6
+    with nbr.Context(0) as ctx:
+        for n, seed in ((20000, 31), (12345, 32)):
+            s = nbr.plummer(n, seed)
+            ctx.upload(s)
+            want = ctx.forces(prec, G=1.0, eps2=eps2)
+            dev = {k: torch.from_numpy(s[k]).cuda() for k in ("x", "y", "z", "m")}
+            out = torch.full((3, n), float("nan"), dtype=torch.float64, device="cuda")
+            stream = torch.cuda.current_stream().cuda_stream
+            torch.cuda.synchronize()
+            rc = f(prec, n, dev["x"].data_ptr(), dev["y"].data_ptr(), dev["z"].data_ptr(),
+                   dev["m"].data_ptr(), 1.0, eps2, out[0].data_ptr(), out[1].data_ptr(),
+                   out[2].data_ptr(), C.c_void_p(stream))
+            assert rc == 0, lib.nbr_last_error_string(None)
+            got = out.cpu().numpy()
+            assert np.all(np.isfinite(got))
+            assert _rel(got, want).max() <= TOL[prec], (n, _rel(got, want).max())
+
+
+def test_noalloc_rejects_sizes_above_the_limit(nbr):
+    lib, f = _entry(nbr)
+    n = 32769
+    rc = f(FP64, n, 1, 1, 1, 1, 1.0, 0.0, 1, 1, 1, None)  # rejected before any pointer is used
+    assert rc == 1
+    assert b"no-allocation limit" in lib.nbr_last_error_string(None)
