@@ -55,6 +55,7 @@ def parse():
     p.add_argument("--precision", choices=["fp32c", "fp64"], default="fp32c")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-accuracy", action="store_true")
+    p.add_argument("--no-batch", action="store_true")
     return p.parse_args()
 
 
@@ -334,6 +335,8 @@ def run_ours(a):
     fp64 = {"value": pairs / statistics.mean(k64) / 1e9, "unit": UNIT, "kernel_ms": 1e3 * statistics.mean(k64)}
     fp64["fp32c_over_fp64"] = achieved / fp64["value"]
 
+    batched = None if a.no_batch else measure_batch(ctx, ext, eps2, value)
+
     cpu = None
     if not a.no_cpu_baseline and rank == 0:
         try:
@@ -350,9 +353,36 @@ def run_ours(a):
                     "d2h_bytes_per_step": 6 * 8 * n, "scheme": "dkd order 2 (reduced_solver_omp_lf's)",
                     "ms_per_step": 1e3 * sum(e2e_s) / a.steps},
             "roofline": roofline, "fp64": fp64, "accuracy": acc, "clocks": clk,
-            "cpu_baseline": cpu}
+            "batched": batched, "cpu_baseline": cpu}
     print(json.dumps(line))
     ctx.close()
+
+
+def measure_batch(ctx, ext, eps2, single_value, steps=10, nsys=4096, seed=3):
+    """The batched workload: 4096 Plummer systems, sizes log-uniform in
+    [64, 4096] (seed 3, system s seeded by index), KDK dt = 1e-3, one persistent
+    work-queue launch per step, the step loop in one CUDA graph."""
+    import torch
+    import nbr
+    off, st = nbr.batch_plummer(nsys, seed)
+    ctx.batch_upload(off, st)
+    out = {"workload": f"{nsys} Plummer systems, N log-uniform in [64, 4096], seed {seed}, "
+                       f"eps 1e-3, KDK dt 1e-3", "systems": nsys, "particles": int(off[-1])}
+    for prec, name in ((nbr.FP32C, "fp32c"), (nbr.FP64, "fp64")):
+        ctx.batch_upload(off, st)
+        ctx.batch_run(prec, dt=1e-3, steps=2, eps2=eps2)  # warm-up (and FSAL)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        r = ctx.batch_run(prec, dt=1e-3, steps=steps, eps2=eps2)
+        e1.record(ext)
+        e1.synchronize()
+        t = e0.elapsed_time(e1) * 1e-3
+        out[name] = {"gpairs": r["pairs"] / t / 1e9, "systems_steps_per_s": nsys * steps / t,
+                     "ms_per_step": 1e3 * t / steps, "force_evals": r["force_evals"],
+                     "kernels": r["kernels"]}
+    out["fp32c"]["frac_of_single_system"] = out["fp32c"]["gpairs"] / single_value
+    return out
 
 
 def run_sharded(a, rank, world, local):

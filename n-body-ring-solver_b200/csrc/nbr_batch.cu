@@ -1,8 +1,507 @@
-// nbr_batch.cu -- batched independent systems (nbr_batch_*).
+// nbr_batch.cu -- thousands of independent systems in one persistent launch.
+//
+// Layout: the systems are stored back to back, each padded to whole
+// 128-particle tiles (padding: zero mass at the origin), so a tile never mixes
+// systems.  A force evaluation is one launch of k_batch_force: a persistent
+// grid whose warps pull work items (system, 128-receiver tile) from a device
+// queue with atomicAdd.  Items are ordered by cost (receivers x system size,
+// largest first) so the tail of the queue holds the cheapest items.  Each warp
+// streams its system's source tiles through its own 3-stage shared-memory ring
+// (1-D bulk copies, one mbarrier per stage, lane 0 produces).
+//
+// Small items: when an item has R <= 64 real receivers (a system of <= 64
+// particles, or the last tile of a system), the warp splits into F = 2, 4 or
+// 8 lane groups that take every F-th source; the partial sums are combined
+// with warp shuffles (xor over the group bits).  Padded sources of a system's
+// last tile are skipped (the loop stops at the tile's real count rounded up to
+// 4), so padding costs ~1 % of the pair work on the log-uniform workload.
+//
+// Pair arithmetic and accumulation are those of the single-system kernels
+// (nbr_kernels.cu): FP32C f32x2 pairs with TwoSum-compensated tile sums, or
+// FP64.  The epilogue applies the KDK kick/drift and packs the FP32C records of
+// the item's tile for the next evaluation.
 #include "nbr.h"
 #include "nbr_ctx.h"
+#include "nbr_device.cuh"
+#include "nbr_kernels.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <vector>
 
 using namespace nbr;
+
+namespace {
+
+constexpr int kBWarps = 4;                    // warps per CTA
+constexpr int kBStages = 3;                   // tile stages per warp
+constexpr int kRec32 = kTile * 48;            // FP32C records of one tile
+constexpr int kStageB32 = kRec32 + 32;        // + origin
+constexpr int kStageB64 = 4 * kTile * 8;      // FP64 x, y, z, m
+constexpr int kBHead = 128;                   // barriers: kBWarps * kBStages * 8 <= 128
+
+struct BatchParams {
+  const double* x; const double* y; const double* z; const double* m;  // current buffer
+  const float4* rec; const double4* org;
+  const long long* poff;     // padded offset of each system (multiple of kTile)
+  const int* nreal;          // real size of each system
+  const int2* items;         // (system, global tile index of the receivers)
+  int n_items;
+  unsigned* head;            // queue head, zero at launch
+  int mode;                  // 0: write a; 1: leapfrog kick + drift
+  double G, kick, drift;
+  double* ax; double* ay; double* az;
+  double* vx; double* vy; double* vz;
+  double* xn; double* yn; double* zn;
+  float4* rec_next; double4* org_next;
+  int* err;
+  unsigned long long wait_ns;
+  int skip_tile;
+};
+
+template <int P>
+struct Stage;
+template <>
+struct Stage<kFP32C> {
+  static constexpr int bytes = kStageB32;
+};
+template <>
+struct Stage<kFP64> {
+  static constexpr int bytes = kStageB64;
+};
+
+// One source tile of FP32C records against the lane's 2 receiver pairs.
+// Sources j = j0, j0 + step, ... < jend.
+template <bool EXCL, bool FULL>
+__device__ __forceinline__ void tile_f32c(const unsigned char* base, int j0, int step, int jend,
+                                          const double* xi, const double* yi, const double* zi,
+                                          u64 EPS2, u64* hx, u64* hy, u64* hz, u64* lx, u64* ly,
+                                          u64* lz) {
+  const double4 o = *reinterpret_cast<const double4*>(base + kRec32);
+  u64 XI[2], YI[2], ZI[2], AX[2], AY[2], AZ[2];
+#pragma unroll
+  for (int p = 0; p < 2; ++p) {
+    XI[p] = pack2(__double2float_rn(xi[2 * p] - o.x), __double2float_rn(xi[2 * p + 1] - o.x));
+    YI[p] = pack2(__double2float_rn(yi[2 * p] - o.y), __double2float_rn(yi[2 * p + 1] - o.y));
+    ZI[p] = pack2(__double2float_rn(zi[2 * p] - o.z), __double2float_rn(zi[2 * p + 1] - o.z));
+    AX[p] = AY[p] = AZ[p] = 0ull;
+  }
+  const ulonglong2* R = reinterpret_cast<const ulonglong2*>(base);
+  auto pair = [&](int j) {
+    const ulonglong2 q0 = R[3 * j];
+    const ulonglong2 q1 = R[3 * j + 1];
+    const u64 bj = R[3 * j + 2].x;
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+      const u64 dx = sub2(q0.x, XI[p]);
+      const u64 dy = sub2(q0.y, YI[p]);
+      const u64 dz = sub2(q1.x, ZI[p]);
+      u64 r2 = fma2(dx, dx, EPS2);
+      r2 = fma2(dy, dy, r2);
+      r2 = fma2(dz, dz, r2);
+      u64 y;
+      if (EXCL) {
+        float rl, rh;
+        unpack2(r2, rl, rh);
+        y = pack2(rl > 0.f ? rsqrt_mufu(rl) : 0.f, rh > 0.f ? rsqrt_mufu(rh) : 0.f);
+      } else {
+        y = rsqrt2(r2);
+      }
+      const u64 y2 = mul2(y, y);
+      const u64 pr = mul2(r2, y2);
+      const u64 mg = fma2(q1.y, pr, bj);
+      const u64 y3 = mul2(y2, y);
+      const u64 s = mul2(y3, mg);
+      AX[p] = fma2(s, dx, AX[p]);
+      AY[p] = fma2(s, dy, AY[p]);
+      AZ[p] = fma2(s, dz, AZ[p]);
+    }
+  };
+  if (FULL) {
+#pragma unroll 4
+    for (int j = 0; j < kTile; ++j) pair(j);
+  } else {
+#pragma unroll 4
+    for (int j = j0; j < jend; j += step) pair(j);
+  }
+#pragma unroll
+  for (int p = 0; p < 2; ++p) {
+    two_sum2(hx[p], lx[p], AX[p]);
+    two_sum2(hy[p], ly[p], AY[p]);
+    two_sum2(hz[p], lz[p], AZ[p]);
+  }
+}
+
+template <bool EXCL, bool FULL>
+__device__ __forceinline__ void tile_f64(const unsigned char* base, int j0, int step, int jend,
+                                         const double* xi, const double* yi, const double* zi,
+                                         double eps2, double* ax, double* ay, double* az) {
+  const double* sx = reinterpret_cast<const double*>(base);
+  const double* sy = sx + kTile;
+  const double* sz = sy + kTile;
+  const double* sm = sz + kTile;
+  auto pair = [&](int j) {
+    const double xj = sx[j], yj = sy[j], zj = sz[j], mj = sm[j];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const double dx = xj - xi[k], dy = yj - yi[k], dz = zj - zi[k];
+      double r2 = fma(dx, dx, eps2);
+      r2 = fma(dy, dy, r2);
+      r2 = fma(dz, dz, r2);
+      double yv = rsqrt(r2);
+      if (EXCL) yv = r2 > 0.0 ? yv : 0.0;
+      const double s = mj * (yv * yv * yv);
+      ax[k] = fma(s, dx, ax[k]);
+      ay[k] = fma(s, dy, ay[k]);
+      az[k] = fma(s, dz, az[k]);
+    }
+  };
+  if (FULL) {
+#pragma unroll 2
+    for (int j = 0; j < kTile; ++j) pair(j);
+  } else {
+#pragma unroll 2
+    for (int j = j0; j < jend; j += step) pair(j);
+  }
+}
+
+template <int PREC, bool EXCL>
+__global__ void __launch_bounds__(kBWarps * 32) k_batch_force(const BatchParams p, const double eps2) {
+  constexpr int SB = Stage<PREC>::bytes;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem) + warp * kBStages;
+  unsigned char* stages = smem + kBHead + (size_t)warp * kBStages * SB;
+  if (lane == 0) {
+    for (int st = 0; st < kBStages; ++st) mbar_init(smem_u32(&bars[st]), 1);
+    mbar_fence_init();
+  }
+  __syncwarp();
+  const float e2f = (float)eps2;
+  const u64 EPS2 = pack2(e2f, e2f);
+  unsigned tcount = 0;  // tiles this warp has consumed (ring position)
+
+  while (true) {
+    int item = 0;
+    if (lane == 0) item = (int)atomicAdd(p.head, 1u);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    if (item >= p.n_items) break;
+    const int2 it = p.items[item];
+    const int s = it.x;
+    const long long poff = p.poff[s];
+    const int ns = p.nreal[s];
+    const long long rbase = (long long)it.y * kTile;          // first receiver (padded index)
+    const int rfirst = (int)(rbase - poff);                      // its index inside the system
+    const int R = min(kTile, ns - rfirst);                       // real receivers in this item
+    const int F = R > 64 ? 1 : R > 32 ? 2 : R > 16 ? 4 : 8;      // lane groups
+    const int G = 32 / F;
+    const int gl = lane % G, phase = lane / G;
+    const int t_first = (int)(poff / kTile);
+    const int ntl = (ns + kTile - 1) / kTile;
+    const int last_cnt = ((ns - (ntl - 1) * kTile) + 3) & ~3;  // real sources of the last tile, to 4
+
+    double xi[4], yi[4], zi[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const long long i = rbase + gl + G * k;  // inside the item's tile for every F
+      xi[k] = p.x[i]; yi[k] = p.y[i]; zi[k] = p.z[i];
+    }
+    u64 hx[2] = {0, 0}, hy[2] = {0, 0}, hz[2] = {0, 0}, lx[2] = {0, 0}, ly[2] = {0, 0}, lz[2] = {0, 0};
+    double ax[4] = {0, 0, 0, 0}, ay[4] = {0, 0, 0, 0}, az[4] = {0, 0, 0, 0};
+
+    uint32_t pending = 0;
+    auto issue = [&](int t) {  // lane 0 only
+      if (t == p.skip_tile) return;
+      const unsigned pos = tcount + t;
+      const int st = pos % kBStages;
+      unsigned char* dst = stages + st * SB;
+      const uint32_t bar = smem_u32(&bars[st]);
+      const size_t tile = (size_t)(t_first + t);
+      if (PREC == kFP32C) {
+        mbar_expect_tx(bar, kStageB32);
+        bulk_g2s(dst, p.rec + tile * kTile * 3, kRec32, bar);
+        bulk_g2s(dst + kRec32, p.org + tile, 32, bar);
+      } else {
+        mbar_expect_tx(bar, kStageB64);
+        const size_t off = tile * kTile;
+        bulk_g2s(dst, p.x + off, kTile * 8, bar);
+        bulk_g2s(dst + kTile * 8, p.y + off, kTile * 8, bar);
+        bulk_g2s(dst + 2 * kTile * 8, p.z + off, kTile * 8, bar);
+        bulk_g2s(dst + 3 * kTile * 8, p.m + off, kTile * 8, bar);
+      }
+      pending |= 1u << st;
+    };
+    if (lane == 0)
+      for (int t = 0; t < kBStages && t < ntl; ++t) issue(t);
+    bool aborted = false;
+    int t = 0;
+    for (; t < ntl; ++t) {
+      const unsigned pos = tcount + t;
+      const int st = pos % kBStages;
+      const bool ok = mbar_wait_bounded(smem_u32(&bars[st]), (pos / kBStages) & 1u, p.wait_ns);
+      const unsigned char* base = stages + st * SB;
+      const int jend = (t == ntl - 1) ? last_cnt : kTile;
+      const bool full = (F == 1) && (jend == kTile);
+      if (PREC == kFP32C) {
+        if (full) tile_f32c<EXCL, true>(base, 0, 1, kTile, xi, yi, zi, EPS2, hx, hy, hz, lx, ly, lz);
+        else tile_f32c<EXCL, false>(base, phase, F, jend, xi, yi, zi, EPS2, hx, hy, hz, lx, ly, lz);
+      } else {
+        if (full) tile_f64<EXCL, true>(base, 0, 1, kTile, xi, yi, zi, eps2, ax, ay, az);
+        else tile_f64<EXCL, false>(base, phase, F, jend, xi, yi, zi, eps2, ax, ay, az);
+      }
+      __syncwarp();
+      if (__any_sync(0xffffffffu, !ok)) {
+        aborted = true;
+        break;
+      }
+      if (lane == 0) {
+        pending &= ~(1u << st);
+        if (t + kBStages < ntl) issue(t + kBStages);
+      }
+    }
+    if (aborted) {
+      if (lane == 0) {
+        record_error(p.err, kErrTileWait);
+        for (int u = t; u < ntl && u < t + kBStages; ++u) {
+          const unsigned pos = tcount + u;
+          const int st = pos % kBStages;
+          if (!(pending & (1u << st))) continue;
+          if (!mbar_wait_bounded(smem_u32(&bars[st]), (pos / kBStages) & 1u, p.wait_ns)) {
+            record_error(p.err, kErrDrainWait);
+            break;
+          }
+        }
+      }
+      return;  // this warp takes no more items; the host reports the error
+    }
+    tcount += ntl;
+
+    if (PREC == kFP32C) {
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        float h0, h1, l0, l1;
+        unpack2(hx[q], h0, h1); unpack2(lx[q], l0, l1);
+        ax[2 * q] = (double)h0 + (double)l0; ax[2 * q + 1] = (double)h1 + (double)l1;
+        unpack2(hy[q], h0, h1); unpack2(ly[q], l0, l1);
+        ay[2 * q] = (double)h0 + (double)l0; ay[2 * q + 1] = (double)h1 + (double)l1;
+        unpack2(hz[q], h0, h1); unpack2(lz[q], l0, l1);
+        az[2 * q] = (double)h0 + (double)l0; az[2 * q + 1] = (double)h1 + (double)l1;
+      }
+    }
+    // Combine the lane groups' partial sums (fixed xor order: deterministic).
+    for (int off = G; off < 32; off <<= 1) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        ax[k] += __shfl_xor_sync(0xffffffffu, ax[k], off);
+        ay[k] += __shfl_xor_sync(0xffffffffu, ay[k], off);
+        az[k] += __shfl_xor_sync(0xffffffffu, az[k], off);
+      }
+    }
+    // Epilogue: lane group 0 owns receivers gl + G k of the item.
+    if (phase == 0) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int loc = gl + G * k;
+        if (loc >= R) continue;
+        const long long i = rbase + loc;
+        const double gx = p.G * ax[k], gy = p.G * ay[k], gz = p.G * az[k];
+        p.ax[i] = gx; p.ay[i] = gy; p.az[i] = gz;
+        if (p.mode == 1) {
+          const double vx = p.vx[i] + p.kick * gx;
+          const double vy = p.vy[i] + p.kick * gy;
+          const double vz = p.vz[i] + p.kick * gz;
+          p.vx[i] = vx; p.vy[i] = vy; p.vz[i] = vz;
+          p.xn[i] = xi[k] + p.drift * vx;
+          p.yn[i] = yi[k] + p.drift * vy;
+          p.zn[i] = zi[k] + p.drift * vz;
+        }
+      }
+    }
+    if (p.mode == 1 && p.rec_next) {
+      // Pack the item's tile of the new positions (natural layout lane + 32k).
+      __syncwarp();
+      double px[4], py[4], pz[4];
+      double sx = 0.0, sy = 0.0, sz = 0.0, cnt = 0.0;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int loc = lane + 32 * k;
+        const long long i = rbase + loc;
+        px[k] = py[k] = pz[k] = 0.0;
+        if (loc < R) {
+          px[k] = p.xn[i]; py[k] = p.yn[i]; pz[k] = p.zn[i];
+          sx += px[k]; sy += py[k]; sz += pz[k]; cnt += 1.0;
+        }
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        sx += __shfl_xor_sync(0xffffffffu, sx, off);
+        sy += __shfl_xor_sync(0xffffffffu, sy, off);
+        sz += __shfl_xor_sync(0xffffffffu, sz, off);
+        cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
+      }
+      const double ox = sx / cnt, oy = sy / cnt, oz = sz / cnt;  // R >= 1
+      if (lane == 0) p.org_next[it.y] = make_double4(ox, oy, oz, 0.0);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int loc = lane + 32 * k;
+        const long long i = rbase + loc;
+        float fx = 0.f, fy = 0.f, fz = 0.f, fa = 0.f, fb = 0.f;
+        if (loc < R) {
+          fx = __double2float_rn(px[k] - ox);
+          fy = __double2float_rn(py[k] - oy);
+          fz = __double2float_rn(pz[k] - oz);
+          fa = __double2float_rn(-1.5 * p.m[i]);
+          fb = __double2float_rn(2.5 * p.m[i]);
+        }
+        p.rec_next[3 * i + 0] = make_float4(fx, fx, fy, fy);
+        p.rec_next[3 * i + 1] = make_float4(fz, fz, fa, fa);
+        p.rec_next[3 * i + 2] = make_float4(fb, fb, 0.f, 0.f);
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// Per-system diagnostics: one CTA per system.  out[s * 9 + c] =
+// T, Px, Py, Pz, Lx, Ly, Lz, M, U (softened, FP64, fixed-order reductions).
+__global__ void __launch_bounds__(256)
+    k_batch_diag(const double* __restrict__ x, const double* __restrict__ y,
+                 const double* __restrict__ z, const double* __restrict__ vx,
+                 const double* __restrict__ vy, const double* __restrict__ vz,
+                 const double* __restrict__ m, const long long* __restrict__ poff,
+                 const int* __restrict__ nreal, double G, double eps2, double* __restrict__ out) {
+  __shared__ double red[9][256];
+  __shared__ double sx[256], sy[256], sz[256], sm[256];
+  const int s = blockIdx.x;
+  const long long o = poff[s];
+  const int n = nreal[s];
+  double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int i0 = 0; i0 < n; i0 += 256) {
+    const int i = i0 + threadIdx.x;
+    const bool valid = i < n;
+    const double xi = valid ? x[o + i] : 0.0, yi = valid ? y[o + i] : 0.0, zi = valid ? z[o + i] : 0.0;
+    const double mi = valid ? m[o + i] : 0.0;
+    if (valid) {
+      const double ux = vx[o + i], uy = vy[o + i], uz = vz[o + i];
+      v[0] += 0.5 * mi * (ux * ux + uy * uy + uz * uz);
+      v[1] += mi * ux; v[2] += mi * uy; v[3] += mi * uz;
+      v[4] += mi * (yi * uz - zi * uy);
+      v[5] += mi * (zi * ux - xi * uz);
+      v[6] += mi * (xi * uy - yi * ux);
+      v[7] += mi;
+    }
+    double phi = 0.0;
+    for (int j0 = 0; j0 < n; j0 += 256) {
+      const int jl = j0 + threadIdx.x;
+      __syncthreads();
+      sx[threadIdx.x] = jl < n ? x[o + jl] : 0.0;
+      sy[threadIdx.x] = jl < n ? y[o + jl] : 0.0;
+      sz[threadIdx.x] = jl < n ? z[o + jl] : 0.0;
+      sm[threadIdx.x] = jl < n ? m[o + jl] : 0.0;
+      __syncthreads();
+      const int cnt = min(256, n - j0);
+      for (int jj = 0; jj < cnt; ++jj) {
+        if (j0 + jj == i) continue;
+        const double dx = sx[jj] - xi, dy = sy[jj] - yi, dz = sz[jj] - zi;
+        phi += sm[jj] / sqrt(dx * dx + dy * dy + dz * dz + eps2);
+      }
+    }
+    if (valid) v[8] += -0.5 * G * mi * phi;
+  }
+#pragma unroll
+  for (int c = 0; c < 9; ++c) red[c][threadIdx.x] = v[c];
+  __syncthreads();
+  for (int h = 128; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h)
+      for (int c = 0; c < 9; ++c) red[c][threadIdx.x] += red[c][threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int c = 0; c < 9; ++c) out[(size_t)s * 9 + c] = red[c][0];
+}
+
+template <int PREC, bool EXCL>
+cudaError_t launch_batch_t(const BatchParams& p, double eps2, int grid, cudaStream_t st) {
+  const size_t smem = kBHead + (size_t)kBWarps * kBStages * Stage<PREC>::bytes;
+  k_batch_force<PREC, EXCL><<<grid, kBWarps * 32, smem, st>>>(p, eps2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch(int prec, const BatchParams& p, double eps2, int grid, cudaStream_t st) {
+  const bool ex = eps2 == 0.0;
+  if (prec == kFP32C)
+    return ex ? launch_batch_t<kFP32C, true>(p, eps2, grid, st) : launch_batch_t<kFP32C, false>(p, eps2, grid, st);
+  return ex ? launch_batch_t<kFP64, true>(p, eps2, grid, st) : launch_batch_t<kFP64, false>(p, eps2, grid, st);
+}
+
+// Sets the kernel's shared-memory attribute and returns the persistent grid
+// (resident CTAs per SM x SMs).  Called outside stream capture; cached.
+int batch_grid(nbr_ctx* c, int prec, double eps2) {
+  int& cached = c->bat.grid[prec == kFP32C ? 1 : 0][eps2 == 0.0 ? 1 : 0];
+  if (cached > 0) return cached;
+  const int sms = c->sms;
+  const size_t smem = kBHead + (size_t)kBWarps * kBStages * (prec == kFP32C ? kStageB32 : kStageB64);
+  const void* fn = prec == kFP32C ? (eps2 == 0.0 ? (const void*)k_batch_force<kFP32C, true>
+                                                 : (const void*)k_batch_force<kFP32C, false>)
+                                  : (eps2 == 0.0 ? (const void*)k_batch_force<kFP64, true>
+                                                 : (const void*)k_batch_force<kFP64, false>);
+  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int per = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, kBWarps * 32, smem) != cudaSuccess ||
+      per < 1)
+    per = 1;
+  cached = per * sms;
+  return cached;
+}
+
+// One batched force evaluation (mode 0: a only; 1: leapfrog step into the
+// other buffer).
+int batch_eval(nbr_ctx* c, int prec, double G, double eps2, int mode, double kick, double drift,
+               int* kernels) {
+  BatchState& b = c->bat;
+  SysState& s = b.s;
+  const int a = s.cur, o = 1 - s.cur;
+  cudaError_t e = cudaSuccess;
+  if (prec == kFP32C && !s.rec_ok[a]) {
+    e = launch_kick_drift((long long)s.n, (long long)s.n_pad, s.pos[a][0], s.pos[a][1], s.pos[a][2],
+                          s.mass, nullptr, nullptr, nullptr, 0.0, 0.0, nullptr, nullptr, nullptr,
+                          nullptr, nullptr, nullptr, s.rec[a], s.org[a], c->stream);
+    if (kernels) ++*kernels;
+    if (e != cudaSuccess) return cuda_fail(c, e, "batch pack");
+    s.rec_ok[a] = true;
+  }
+  e = cudaMemsetAsync(b.d_head, 0, sizeof(unsigned), c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "batch queue reset");
+  BatchParams p{};
+  p.x = s.pos[a][0]; p.y = s.pos[a][1]; p.z = s.pos[a][2]; p.m = s.mass;
+  p.rec = s.rec[a]; p.org = s.org[a];
+  p.poff = b.d_poff; p.nreal = b.d_nreal; p.items = b.d_items; p.n_items = b.n_items;
+  p.head = b.d_head;
+  p.mode = mode; p.G = G; p.kick = kick; p.drift = drift;
+  p.ax = s.acc[0]; p.ay = s.acc[1]; p.az = s.acc[2];
+  p.vx = s.vel[0]; p.vy = s.vel[1]; p.vz = s.vel[2];
+  p.xn = s.pos[o][0]; p.yn = s.pos[o][1]; p.zn = s.pos[o][2];
+  p.rec_next = (mode == 1 && prec == kFP32C) ? s.rec[o] : nullptr;
+  p.org_next = s.org[o];
+  p.err = c->d_err;
+  JStream js{};
+  pipeline_params(js);
+  p.wait_ns = js.wait_ns;
+  p.skip_tile = js.skip_tile;
+  e = launch_batch(prec, p, eps2, batch_grid(c, prec, eps2), c->stream);
+  if (kernels) ++*kernels;
+  if (e != cudaSuccess) return cuda_fail(c, e, "batch force launch");
+  if (mode == 1) {
+    s.cur = o;
+    s.rec_ok[o] = (prec == kFP32C);
+    s.rec_ok[a] = false;
+  }
+  return NBR_OK;
+}
+
+}  // namespace
 
 void nbr::BatchState::release() {
   s.release();
@@ -16,20 +515,279 @@ void nbr::BatchState::release() {
 }
 
 extern "C" {
-int nbr_batch_upload(nbr_ctx* c, size_t, const size_t*, const double*, const double*,
-                     const double*, const double*, const double*, const double*, const double*) {
-  return fail(c, NBR_ERR_UNSUPPORTED, "batched systems not built yet");
+
+int nbr_batch_upload(nbr_ctx* c, size_t nsys, const size_t* offsets, const double* x,
+                     const double* y, const double* z, const double* vx, const double* vy,
+                     const double* vz, const double* m) {
+  if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
+  if (nsys == 0 || !offsets || !x || !y || !z || !m)
+    return fail(c, NBR_ERR_INVALID_ARG, "empty batch or NULL array");
+  if ((vx || vy || vz) && !(vx && vy && vz))
+    return fail(c, NBR_ERR_INVALID_ARG, "velocities must be all given or all NULL");
+  if (offsets[0] != 0) return fail(c, NBR_ERR_INVALID_ARG, "offsets[0] must be 0");
+  for (size_t s = 0; s < nsys; ++s) {
+    if (offsets[s + 1] <= offsets[s]) return fail(c, NBR_ERR_INVALID_ARG, "every system needs >= 1 particle");
+    if (offsets[s + 1] - offsets[s] > (size_t)1 << 30) return fail(c, NBR_ERR_INVALID_ARG, "system too large");
+  }
+  const size_t n = offsets[nsys];
+  if (!finite_array(x, n) || !finite_array(y, n) || !finite_array(z, n) || !finite_array(m, n) ||
+      (vx && (!finite_array(vx, n) || !finite_array(vy, n) || !finite_array(vz, n))))
+    return fail(c, NBR_ERR_NONFINITE, "input contains NaN or Inf");
+  for (size_t i = 0; i < n; ++i)
+    if (m[i] < 0.0) return fail(c, NBR_ERR_INVALID_ARG, "negative mass");
+  cudaSetDevice(c->device);
+  BatchState& b = c->bat;
+  b.release();
+  b.nsys = nsys;
+  b.n_real = n;
+  b.off.assign(offsets, offsets + nsys + 1);
+  b.poff.assign(nsys + 1, 0);
+  double pairs = 0.0;
+  for (size_t s = 0; s < nsys; ++s) {
+    const long long ns = (long long)(offsets[s + 1] - offsets[s]);
+    b.poff[s + 1] = b.poff[s] + ((ns + kTile - 1) / kTile) * kTile;
+    pairs += double(ns) * double(ns - 1);
+  }
+  b.pairs_per_eval = pairs;
+  const size_t np = (size_t)b.poff[nsys];
+  cudaError_t e = b.s.reserve(np);
+  if (e != cudaSuccess) return cuda_fail(c, e, "batch allocation");
+  // Host staging in the padded layout.
+  std::vector<double> h(b.s.n_pad, 0.0);
+  auto put = [&](double* d, const double* src) {
+    if (e != cudaSuccess) return;
+    std::fill(h.begin(), h.end(), 0.0);
+    if (src)
+      for (size_t s = 0; s < nsys; ++s)
+        std::memcpy(&h[b.poff[s]], src + offsets[s], (offsets[s + 1] - offsets[s]) * sizeof(double));
+    e = cudaMemcpy(d, h.data(), b.s.n_pad * sizeof(double), cudaMemcpyHostToDevice);
+  };
+  put(b.s.pos[0][0], x); put(b.s.pos[0][1], y); put(b.s.pos[0][2], z);
+  put(b.s.vel[0], vx); put(b.s.vel[1], vy); put(b.s.vel[2], vz);
+  put(b.s.mass, m);
+  for (int d = 0; d < 3 && e == cudaSuccess; ++d) {
+    e = cudaMemset(b.s.pos[1][d], 0, b.s.n_pad * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemset(b.s.acc[d], 0, b.s.n_pad * sizeof(double));
+  }
+  if (e != cudaSuccess) return cuda_fail(c, e, "batch upload");
+  // Work items ordered by cost (receivers x system size), largest first.
+  std::vector<int2> items;
+  std::vector<double> cost;
+  for (size_t s = 0; s < nsys; ++s) {
+    const long long ns = (long long)(offsets[s + 1] - offsets[s]);
+    const long long nt = (ns + kTile - 1) / kTile;
+    for (long long t = 0; t < nt; ++t) {
+      const long long r = std::min<long long>(kTile, ns - t * kTile);
+      items.push_back(make_int2((int)s, (int)(b.poff[s] / kTile + t)));
+      cost.push_back(double(r > 64 ? kTile : r > 32 ? 64 : r > 16 ? 32 : 16) * double(ns));
+    }
+  }
+  std::vector<int> order(items.size());
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int bb) { return cost[a] > cost[bb]; });
+  std::vector<int2> sorted(items.size());
+  for (size_t k = 0; k < order.size(); ++k) sorted[k] = items[order[k]];
+  b.n_items = (int)sorted.size();
+  std::vector<int> nreal(nsys);
+  for (size_t s = 0; s < nsys; ++s) nreal[s] = (int)(offsets[s + 1] - offsets[s]);
+  e = dalloc((void**)&b.d_poff, (nsys + 1) * sizeof(long long));
+  if (e == cudaSuccess) e = dalloc((void**)&b.d_nreal, nsys * sizeof(int));
+  if (e == cudaSuccess) e = dalloc((void**)&b.d_items, sorted.size() * sizeof(int2));
+  if (e == cudaSuccess) e = dalloc((void**)&b.d_head, 256);
+  if (e == cudaSuccess) e = dalloc((void**)&b.d_red, nsys * 9 * sizeof(double));
+  if (e == cudaSuccess)
+    e = cudaMemcpy(b.d_poff, b.poff.data(), (nsys + 1) * sizeof(long long), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b.d_nreal, nreal.data(), nsys * sizeof(int), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(b.d_items, sorted.data(), sorted.size() * sizeof(int2), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    b.release();
+    return cuda_fail(c, e, "batch tables");
+  }
+  b.s.cur = 0;
+  b.s.rec_ok[0] = b.s.rec_ok[1] = false;
+  b.acc_ok = false;
+  return NBR_OK;
 }
-int nbr_batch_download(nbr_ctx* c, double*, double*, double*, double*, double*, double*) {
-  return fail(c, NBR_ERR_UNSUPPORTED, "batched systems not built yet");
+
+int nbr_batch_download(nbr_ctx* c, double* x, double* y, double* z, double* vx, double* vy,
+                       double* vz) {
+  if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
+  BatchState& b = c->bat;
+  if (b.nsys == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no batch uploaded");
+  cudaSetDevice(c->device);
+  std::vector<double> h(b.s.n_pad);
+  cudaError_t e = cudaSuccess;
+  auto get = [&](double* dst, const double* d) {
+    if (!dst || e != cudaSuccess) return;
+    e = cudaMemcpy(h.data(), d, b.s.n_pad * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return;
+    for (size_t s = 0; s < b.nsys; ++s)
+      std::memcpy(dst + b.off[s], &h[b.poff[s]], (b.off[s + 1] - b.off[s]) * sizeof(double));
+  };
+  const int a = b.s.cur;
+  get(x, b.s.pos[a][0]); get(y, b.s.pos[a][1]); get(z, b.s.pos[a][2]);
+  get(vx, b.s.vel[0]); get(vy, b.s.vel[1]); get(vz, b.s.vel[2]);
+  return e == cudaSuccess ? NBR_OK : cuda_fail(c, e, "batch download");
 }
-int nbr_batch_forces(nbr_ctx* c, int, double, double, int, double*, double*, double*) {
-  return fail(c, NBR_ERR_UNSUPPORTED, "batched systems not built yet");
+
+int nbr_batch_forces(nbr_ctx* c, int precision, double G, double eps2, int want_force, double* ax,
+                     double* ay, double* az) {
+  if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
+  if (precision != NBR_FP64 && precision != NBR_FP32C)
+    return fail(c, NBR_ERR_INVALID_ARG, "unknown precision");
+  if (!(eps2 >= 0.0) || !std::isfinite(eps2) || !std::isfinite(G))
+    return fail(c, NBR_ERR_INVALID_ARG, "eps2 must be finite and >= 0, G finite");
+  BatchState& b = c->bat;
+  if (b.nsys == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no batch uploaded");
+  cudaSetDevice(c->device);
+  int rc = batch_eval(c, precision, G, eps2, 0, 0.0, 0.0, nullptr);
+  if (rc) return rc;
+  rc = check_device_error(c);
+  if (rc) return rc;
+  b.acc_ok = true;
+  b.acc_prec = precision;
+  b.acc_G = G;
+  b.acc_eps2 = eps2;
+  std::vector<double> h(b.s.n_pad), mh;
+  cudaError_t e = cudaSuccess;
+  if (want_force) {
+    mh.resize(b.s.n_pad);
+    e = cudaMemcpy(mh.data(), b.s.mass, b.s.n_pad * sizeof(double), cudaMemcpyDeviceToHost);
+  }
+  auto get = [&](double* dst, const double* d) {
+    if (!dst || e != cudaSuccess) return;
+    e = cudaMemcpy(h.data(), d, b.s.n_pad * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return;
+    for (size_t s = 0; s < b.nsys; ++s)
+      for (size_t k = 0; k < b.off[s + 1] - b.off[s]; ++k) {
+        const size_t i = (size_t)b.poff[s] + k;
+        dst[b.off[s] + k] = want_force ? h[i] * mh[i] : h[i];
+      }
+  };
+  get(ax, b.s.acc[0]); get(ay, b.s.acc[1]); get(az, b.s.acc[2]);
+  return e == cudaSuccess ? NBR_OK : cuda_fail(c, e, "batch forces download");
 }
-int nbr_batch_run(nbr_ctx* c, int, double, size_t, double, double, nbr_run_stats*) {
-  return fail(c, NBR_ERR_UNSUPPORTED, "batched systems not built yet");
+
+int nbr_batch_run(nbr_ctx* c, int precision, double dt, size_t steps, double G, double eps2,
+                  nbr_run_stats* stats) {
+  if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
+  if (precision != NBR_FP64 && precision != NBR_FP32C)
+    return fail(c, NBR_ERR_INVALID_ARG, "unknown precision");
+  if (!std::isfinite(dt) || !(eps2 >= 0.0) || !std::isfinite(eps2) || !std::isfinite(G))
+    return fail(c, NBR_ERR_INVALID_ARG, "dt, G must be finite, eps2 finite and >= 0");
+  BatchState& b = c->bat;
+  if (b.nsys == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no batch uploaded");
+  cudaSetDevice(c->device);
+  nbr_run_stats st{};
+  if (steps > 0) {
+    // Configure the kernel (shared-memory attribute, grid) before capture.
+    batch_grid(c, precision, eps2);
+    const bool fsal = b.acc_ok && b.acc_prec == precision && b.acc_G == G && b.acc_eps2 == eps2;
+    SysState& s = b.s;
+    const int cur0 = s.cur;
+    const bool r0 = s.rec_ok[0], r1 = s.rec_ok[1];
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_fail(c, e, "begin capture");
+    int kernels = 0, rc = NBR_OK;
+    double evals = 0;
+    const bool fp32 = precision == kFP32C;
+    if (fsal) {
+      const int a = s.cur, o = 1 - s.cur;
+      e = launch_kick_drift((long long)s.n, (long long)s.n_pad, s.pos[a][0], s.pos[a][1],
+                            s.pos[a][2], s.mass, s.acc[0], s.acc[1], s.acc[2], 0.5 * dt, dt,
+                            s.vel[0], s.vel[1], s.vel[2], s.pos[o][0], s.pos[o][1], s.pos[o][2],
+                            fp32 ? s.rec[o] : nullptr, fp32 ? s.org[o] : nullptr, c->stream);
+      ++kernels;
+      if (e != cudaSuccess) rc = cuda_fail(c, e, "batch kick-drift");
+      s.cur = o;
+      s.rec_ok[o] = fp32;
+      s.rec_ok[a] = false;
+    } else {
+      rc = batch_eval(c, precision, G, eps2, 1, 0.5 * dt, dt, &kernels);
+      evals += 1;
+    }
+    for (size_t k = 1; k < steps && rc == NBR_OK; ++k) {
+      rc = batch_eval(c, precision, G, eps2, 1, dt, dt, &kernels);
+      evals += 1;
+    }
+    if (rc == NBR_OK) {
+      rc = batch_eval(c, precision, G, eps2, 1, 0.5 * dt, 0.0, &kernels);
+      evals += 1;
+    }
+    cudaError_t ee = cudaStreamEndCapture(c->stream, &graph);
+    if (rc != NBR_OK || ee != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      s.cur = cur0;
+      s.rec_ok[0] = r0;
+      s.rec_ok[1] = r1;
+      return rc != NBR_OK ? rc : cuda_fail(c, ee, "end capture");
+    }
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      s.cur = cur0;
+      s.rec_ok[0] = r0;
+      s.rec_ok[1] = r1;
+      return cuda_fail(c, e, "graph instantiate");
+    }
+    e = cudaEventRecord(c->ev0, c->stream);
+    if (e == cudaSuccess) e = cudaGraphLaunch(exec, c->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(c->ev1, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaGraphExecDestroy(exec);
+    if (e != cudaSuccess) {
+      b.acc_ok = false;
+      return cuda_fail(c, e, "graph launch");
+    }
+    rc = check_device_error(c);
+    if (rc) {
+      b.acc_ok = false;
+      return rc;
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    st.gpu_ms = ms;
+    st.kernels = kernels;
+    st.force_evals = evals;
+    st.pairs = evals * b.pairs_per_eval;
+    b.acc_ok = true;
+    b.acc_prec = precision;
+    b.acc_G = G;
+    b.acc_eps2 = eps2;
+  }
+  if (stats) *stats = st;
+  return NBR_OK;
 }
-int nbr_batch_diagnostics(nbr_ctx* c, double, double, nbr_diag*) {
-  return fail(c, NBR_ERR_UNSUPPORTED, "batched systems not built yet");
+
+int nbr_batch_diagnostics(nbr_ctx* c, double G, double eps2, nbr_diag* out) {
+  if (!c || !out) return fail(c, NBR_ERR_INVALID_ARG, "NULL argument");
+  if (!(eps2 >= 0.0) || !std::isfinite(eps2)) return fail(c, NBR_ERR_INVALID_ARG, "bad eps2");
+  BatchState& b = c->bat;
+  if (b.nsys == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no batch uploaded");
+  cudaSetDevice(c->device);
+  const int a = b.s.cur;
+  k_batch_diag<<<(unsigned)b.nsys, 256, 0, c->stream>>>(
+      b.s.pos[a][0], b.s.pos[a][1], b.s.pos[a][2], b.s.vel[0], b.s.vel[1], b.s.vel[2], b.s.mass,
+      b.d_poff, b.d_nreal, G, eps2, b.d_red);
+  cudaError_t e = cudaGetLastError();
+  std::vector<double> h(b.nsys * 9);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(h.data(), b.d_red, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "batch diagnostics");
+  for (size_t s = 0; s < b.nsys; ++s) {
+    const double* r = &h[s * 9];
+    out[s].T = r[0];
+    out[s].P[0] = r[1]; out[s].P[1] = r[2]; out[s].P[2] = r[3];
+    out[s].L[0] = r[4]; out[s].L[1] = r[5]; out[s].L[2] = r[6];
+    out[s].M = r[7];
+    out[s].U = r[8];
+    out[s].E = r[0] + r[8];
+  }
+  return NBR_OK;
 }
-}
+
+}  // extern "C"

@@ -66,6 +66,7 @@ struct BatchState {
   int acc_prec = 0;
   double acc_G = 0.0, acc_eps2 = 0.0;
   double pairs_per_eval = 0.0;
+  int grid[2][2] = {{0, 0}, {0, 0}};  // persistent grid per (precision, eps == 0)
 
   void release();
 };
@@ -76,6 +77,8 @@ cudaError_t dalloc(void** p, size_t bytes);
 void dfree(void* p);
 bool finite_array(const double* a, size_t n);
 int check_device_error(nbr_ctx* c);
+// Bounded-wait limit and tile-skip test hook from the environment.
+void pipeline_params(JStream& js);
 
 }  // namespace nbr
 
