@@ -560,14 +560,15 @@ int nbr_batch_upload(nbr_ctx* c, size_t nsys, const size_t* offsets, const doubl
     if (src)
       for (size_t s = 0; s < nsys; ++s)
         std::memcpy(&h[b.poff[s]], src + offsets[s], (offsets[s + 1] - offsets[s]) * sizeof(double));
-    e = cudaMemcpy(d, h.data(), b.s.n_pad * sizeof(double), cudaMemcpyHostToDevice);
+    e = cudaMemcpyAsync(d, h.data(), b.s.n_pad * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);  // h is reused
   };
   put(b.s.pos[0][0], x); put(b.s.pos[0][1], y); put(b.s.pos[0][2], z);
   put(b.s.vel[0], vx); put(b.s.vel[1], vy); put(b.s.vel[2], vz);
   put(b.s.mass, m);
   for (int d = 0; d < 3 && e == cudaSuccess; ++d) {
-    e = cudaMemset(b.s.pos[1][d], 0, b.s.n_pad * sizeof(double));
-    if (e == cudaSuccess) e = cudaMemset(b.s.acc[d], 0, b.s.n_pad * sizeof(double));
+    e = cudaMemsetAsync(b.s.pos[1][d], 0, b.s.n_pad * sizeof(double), c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b.s.acc[d], 0, b.s.n_pad * sizeof(double), c->stream);
   }
   if (e != cudaSuccess) return cuda_fail(c, e, "batch upload");
   // Work items ordered by cost (receivers x system size), largest first.
@@ -596,10 +597,14 @@ int nbr_batch_upload(nbr_ctx* c, size_t nsys, const size_t* offsets, const doubl
   if (e == cudaSuccess) e = dalloc((void**)&b.d_head, 256);
   if (e == cudaSuccess) e = dalloc((void**)&b.d_red, nsys * 9 * sizeof(double));
   if (e == cudaSuccess)
-    e = cudaMemcpy(b.d_poff, b.poff.data(), (nsys + 1) * sizeof(long long), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(b.d_nreal, nreal.data(), nsys * sizeof(int), cudaMemcpyHostToDevice);
+    e = cudaMemcpyAsync(b.d_poff, b.poff.data(), (nsys + 1) * sizeof(long long),
+                        cudaMemcpyHostToDevice, c->stream);
   if (e == cudaSuccess)
-    e = cudaMemcpy(b.d_items, sorted.data(), sorted.size() * sizeof(int2), cudaMemcpyHostToDevice);
+    e = cudaMemcpyAsync(b.d_nreal, nreal.data(), nsys * sizeof(int), cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b.d_items, sorted.data(), sorted.size() * sizeof(int2),
+                        cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) {
     b.release();
     return cuda_fail(c, e, "batch tables");
@@ -620,7 +625,8 @@ int nbr_batch_download(nbr_ctx* c, double* x, double* y, double* z, double* vx, 
   cudaError_t e = cudaSuccess;
   auto get = [&](double* dst, const double* d) {
     if (!dst || e != cudaSuccess) return;
-    e = cudaMemcpy(h.data(), d, b.s.n_pad * sizeof(double), cudaMemcpyDeviceToHost);
+    e = cudaMemcpyAsync(h.data(), d, b.s.n_pad * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return;
     for (size_t s = 0; s < b.nsys; ++s)
       std::memcpy(dst + b.off[s], &h[b.poff[s]], (b.off[s + 1] - b.off[s]) * sizeof(double));
@@ -653,11 +659,14 @@ int nbr_batch_forces(nbr_ctx* c, int precision, double G, double eps2, int want_
   cudaError_t e = cudaSuccess;
   if (want_force) {
     mh.resize(b.s.n_pad);
-    e = cudaMemcpy(mh.data(), b.s.mass, b.s.n_pad * sizeof(double), cudaMemcpyDeviceToHost);
+    e = cudaMemcpyAsync(mh.data(), b.s.mass, b.s.n_pad * sizeof(double), cudaMemcpyDeviceToHost,
+                        c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   }
   auto get = [&](double* dst, const double* d) {
     if (!dst || e != cudaSuccess) return;
-    e = cudaMemcpy(h.data(), d, b.s.n_pad * sizeof(double), cudaMemcpyDeviceToHost);
+    e = cudaMemcpyAsync(h.data(), d, b.s.n_pad * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return;
     for (size_t s = 0; s < b.nsys; ++s)
       for (size_t k = 0; k < b.off[s + 1] - b.off[s]; ++k) {

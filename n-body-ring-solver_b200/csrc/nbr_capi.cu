@@ -43,12 +43,19 @@ void dfree(void* p) {
   if (p) cudaFree(p);
 }
 
+// Allocates and zeroes device memory.  cudaMemset runs on the legacy default
+// stream, which does not order with the contexts' non-blocking streams, so the
+// zeroing is completed here before any kernel can see the memory (a counter
+// array zeroed late once left split-arrival counters non-zero).  Allocation is
+// rare (buffers only grow), so the device-wide wait costs nothing in a step.
 cudaError_t dalloc(void** p, size_t bytes) {
   *p = nullptr;
   if (bytes == 0) bytes = 256;
   cudaError_t e = cudaMalloc(p, bytes);
   if (e != cudaSuccess) return e;
-  return cudaMemset(*p, 0, bytes);
+  e = cudaMemset(*p, 0, bytes);
+  if (e != cudaSuccess) return e;
+  return cudaDeviceSynchronize();
 }
 
 bool finite_array(const double* a, size_t n) {
@@ -219,8 +226,10 @@ void save_tune_locked() {
 
 }  // namespace
 
-// Heuristic split: enough (chunk, split) units for ~8 waves of resident CTAs,
-// each split range at least 8 tiles.
+// Heuristic split.  Finer (chunk, split) units balance the SMs better; a B200
+// sweep (N = 32768 .. 1048576) found throughput rising with the split up to
+// 8 tiles (1024 sources) per split range and at most 64 splits.  Small systems
+// get at least ~4 waves of resident CTAs, down to 2 tiles per range.
 int auto_split(int precision, double eps2, const ForceConfig& c, long long n_i, int ntiles,
                int sms) {
   const long long chunk = 32LL * c.ni * c.warps;
@@ -228,9 +237,9 @@ int auto_split(int precision, double eps2, const ForceConfig& c, long long n_i, 
   int per_sm = force_blocks_per_sm(precision, eps2, c);
   if (per_sm < 1) per_sm = 1;
   const long long slots = (long long)sms * per_sm;
-  long long s = (8 * slots + chunks - 1) / chunks;
-  const long long smax = std::max<long long>(1, ntiles / 8);
-  s = std::max<long long>(1, std::min(s, smax));
+  const long long waves4 = (4 * slots + chunks - 1) / chunks;
+  long long s = std::max<long long>(ntiles / 8, std::min<long long>(ntiles / 2, waves4));
+  s = std::max<long long>(1, std::min<long long>(s, 64));
   return (int)s;
 }
 

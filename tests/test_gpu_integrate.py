@@ -219,3 +219,32 @@ int main(int argc, char** argv) {
     from conftest import rel_err
     assert rel_err(F_full, g["F_simple"]).max() <= 1e-12
     assert rel_err(F_block, g["F_simple"][:, :250]).max() <= 1e-12
+
+
+@pytest.mark.parametrize("prec", [FP32C, FP64])
+def test_fresh_buffers_are_zero_before_first_launch(nbr, prec):
+    """Regression: buffers allocated just before a launch (split partial sums and
+    arrival counters) must be zeroed before any kernel sees them.  When the
+    zeroing ran on the legacy stream it raced the context stream's first force
+    launch and left arrival counters non-zero, corrupting later steps.  The
+    sequence below (forces-only launches that allocate the split scratch,
+    re-upload, diagnostics, KDK steps) must give the same bits as a plain run."""
+    s = nbr.plummer(262144, 2)
+    eps2, dt = 1e-6, 5e-4
+    with nbr.Context(0) as c:
+        c.upload(s)
+        for _ in range(3):
+            c.forces_device(prec, eps2=eps2)
+        c.synchronize()
+        c.upload(s)
+        c.diagnostics(eps2=eps2)
+        for _ in range(3):
+            c.run(prec, KDK, 2, dt, 1, eps2=eps2)
+        got = c.download()
+    with nbr.Context(0) as c:
+        c.upload(s)
+        for _ in range(3):
+            c.run(prec, KDK, 2, dt, 1, eps2=eps2)
+        want = c.download()
+    for k in KEYS6:
+        np.testing.assert_array_equal(got[k], want[k])
