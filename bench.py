@@ -18,7 +18,8 @@ Output: ONE JSON line on stdout (rank 0).  Keys beyond the base contract:
 
 --impl reference times the reference's CPU implementation instead (rank 0).
 --gpus N (under torchrun) shards the receivers of the one system over N GPUs
-with an NCCL all-gather of positions per step.
+with an NCCL all-gather of positions per step (--shard takes that path on
+one GPU too).
 """
 import argparse
 import json
@@ -56,6 +57,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-accuracy", action="store_true")
     p.add_argument("--no-batch", action="store_true")
+    p.add_argument("--shard", action="store_true",
+                   help="use the multi-GPU i-partition path even on one GPU (process group of 1)")
     return p.parse_args()
 
 
@@ -221,7 +224,7 @@ def run_ours(a):
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
+    if world > 1 or a.shard:
         return run_sharded(a, rank, world, local)
     torch.cuda.set_device(local)
     prec = nbr.FP32C if a.precision == "fp32c" else nbr.FP64
@@ -328,6 +331,9 @@ def run_ours(a):
     peak = SMS * 128 * mhz * 1e6 / FMA_OPS_PER_PAIR / 1e9
     roofline = {"bound": "fp32_fma_pipe", "achieved": achieved, "peak": peak, "unit": UNIT,
                 "frac": achieved / peak, "traffic": profile_traffic(),
+                "algorithmic_bytes": 96 * n,
+                "traffic_note": "dram bytes per launch from profiles/force_fp32c_plummer262144.json; "
+                                "402 MB of it are the split partial sums (written and read once)",
                 "peak_source": "148 SMs x 128 FP32 lanes x median SM clock sampled in the timed region "
                                "/ 16 FMA-pipe ops per pair (MEASURED_PEAKS.json has no FP32-pipe figure)",
                 "frac_at_max_clock": achieved / (SMS * 128 * 1965e6 / FMA_OPS_PER_PAIR / 1e9),
@@ -386,7 +392,125 @@ def measure_batch(ctx, ext, eps2, single_value, steps=10, nsys=4096, seed=3):
 
 
 def run_sharded(a, rank, world, local):
-    raise SystemExit("multi-GPU sharding is not built yet")
+    """--gpus N under torchrun: the one system split by receivers over the N
+    GPUs (nbr_shard.ShardedSystem: owned slice against all sources, then an
+    NCCL all-gather of positions per step, as hybrid_full_solver does with
+    MPI_Allgather).  Strong scaling: N(N-1) pairs per step in total."""
+    import datetime
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import nbr
+    from nbr_shard import ShardedSystem
+
+    torch.cuda.set_device(local)
+    for k, v in (("MASTER_ADDR", "127.0.0.1"), ("MASTER_PORT", "29533"), ("RANK", str(rank)),
+                 ("WORLD_SIZE", str(world))):
+        os.environ.setdefault(k, v)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                            device_id=torch.device("cuda", local))
+    try:
+        prec = nbr.FP32C if a.precision == "fp32c" else nbr.FP64
+        eps2 = a.eps * a.eps
+        n = a.n
+        pairs = float(n) * float(n - 1)
+        s = nbr.plummer(n, a.seed)
+        ctx = nbr.Context(local)
+        sh = ShardedSystem(ctx)
+        sh.upload(s)
+        ext = torch.cuda.ExternalStream(ctx.stream)
+        flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")
+
+        def l2_flush():
+            with torch.cuda.stream(ext):
+                flush.zero_()
+
+        def timed(fn):
+            l2_flush()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(ext)
+            fn()
+            e1.record(ext)
+            e1.synchronize()
+            return e0.elapsed_time(e1) * 1e-3
+
+        def step():
+            sh.step(prec, nbr.KDK, a.dt, a.dt, 1.0, eps2)
+
+        def max_over_ranks(v):
+            t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+
+        # kernel-only: the owned slice's evaluation with kick = drift = 0
+        # (state unchanged), then an exchange to refill the other slices
+        k_s = []
+        for _ in range(3):
+            if sh.owned:
+                k_s.append(timed(lambda: ctx.step_range(prec, nbr.KDK, sh.i0, sh.owned, 0.0, 0.0,
+                                                        1.0, eps2)))
+            sh.exchange_positions()
+        for _ in range(a.warmup):
+            step()
+        ctx.synchronize()
+        clocks = ClockSampler(local) if rank == 0 else None
+        if clocks:
+            clocks.start()
+            time.sleep(0.5)
+        dist.barrier()
+        torch.cuda.synchronize()
+        step_s = [timed(step) for _ in range(a.steps)]
+        dist.barrier()
+        torch.cuda.synchronize()
+        clk = clocks.stop() if clocks else None
+        t_total = max_over_ranks(sum(step_s))
+        ctx.synchronize()  # surfaces a bounded-wait timeout of any step
+        value = a.steps * pairs / t_total / 1e9
+
+        # end to end: host state in (pinned), one sharded step, positions out
+        host = {k: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy() for k in nbr.KEYS}
+        for k in nbr.KEYS:
+            host[k][:] = s[k]
+        e2e_s = []
+        for i in range(a.warmup + a.steps):
+            def e2e_step():
+                ctx.upload_raw(n, *[host[k] for k in nbr.KEYS])
+                sh.step(prec, nbr.KDK, a.dt, a.dt, 1.0, eps2)
+                ctx.download_raw(host["x"], host["y"], host["z"], None, None, None)
+            t = timed(e2e_step)
+            if i >= a.warmup:
+                e2e_s.append(t)
+        e2e_total = max_over_ranks(sum(e2e_s))
+        k_t = statistics.mean(k_s) if k_s else 0.0
+        k_max = max_over_ranks(k_t)
+        if rank == 0:
+            mhz = (clk or {}).get("sm_mhz") or 1965.0
+            peak = world * SMS * 128 * mhz * 1e6 / FMA_OPS_PER_PAIR / 1e9
+            achieved = pairs / k_max / 1e9 if k_max > 0 else None
+            line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                    "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * t_total / a.steps,
+                    "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+                    "dtype": "f32" if prec == nbr.FP32C else "f64", "data": "synthetic",
+                    "config": workload_config(a, {"precision": a.precision,
+                                                  "parallelism": f"i-partition x{world}, NCCL "
+                                                                 "all-gather of positions per step",
+                                                  "shard": sh.count}),
+                    "gpu_launches": 2 * a.steps,
+                    "e2e": {"value": a.steps * pairs / e2e_total / 1e9, "unit": UNIT,
+                            "h2d_bytes_per_step": 7 * 8 * n, "d2h_bytes_per_step": 3 * 8 * n,
+                            "scheme": "kdk, whole state uploaded and positions downloaded per step"},
+                    "roofline": {"bound": "fp32_fma_pipe", "achieved": achieved, "peak": peak,
+                                 "unit": UNIT, "frac": achieved / peak if achieved else None,
+                                 "traffic": None,
+                                 "peak_source": f"{world} GPUs x 148 SMs x 128 FP32 lanes x rank-0 "
+                                                "median SM clock / 16 FMA-pipe ops per pair",
+                                 "kernel_ms_max_over_ranks": 1e3 * k_max},
+                    "clocks": clk, "cpu_baseline": None, "collectives_per_step": 1}
+            print(json.dumps(line))
+        ctx.synchronize()
+        ctx.close()
+    finally:
+        dist.destroy_process_group()
 
 
 def main():

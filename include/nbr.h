@@ -188,6 +188,42 @@ int nbr_run(nbr_ctx* ctx, int precision, int scheme, int order, double dt, size_
  * 2, 4, 6 or 8; returns lf_steps = 2w, or 0 for an unsupported order. */
 int nbr_yoshida_coefficients(int order, double* c, double* d);
 
+/* --------------------------------------------- multi-GPU i-partition ---- */
+/* One process (and one context) per GPU; every context holds the whole system
+ * and owns the receivers [i0, i0 + count).  A step is one force evaluation
+ * of the owned receivers against all n sources, their kick and drift, then an
+ * exchange that brings every context the new positions of all particles.
+ * This replaces hybrid_full_solver (CPU/hybrid_solver.cpp:226-336): each MPI
+ * rank owns local_N = N / comm_sz particles, computes their forces against
+ * all N (compute_forces_full_avx2, :288), updates them (:290-299) and
+ * MPI_Allgathers the positions (:310).  The exchange belongs to the caller
+ * (e.g. an NCCL all-gather on the arrays nbr_state_pointers returns, ordered
+ * after the step on nbr_ctx_stream); the library only computes. */
+
+/* One force evaluation of receivers [i0, i0 + count) (count is clipped to
+ * n - i0; i0 a multiple of 128) with the fused update, asynchronous on the
+ * context's stream:
+ *   scheme NBR_KDK or NBR_DKD: v += kick * a, then x' = x + drift * v;
+ *   scheme NBR_EULER:          x' = x + drift * v_old, v += kick * a;
+ * x' goes to the other position buffer, which becomes current.  Only the
+ * range's entries of that buffer are written: the positions of every other
+ * particle must be filled in (the exchange) before the next step, followed
+ * by nbr_state_changed.  A KDK run of k steps from x_0 is k + 1 calls with
+ * (kick, drift) = (dt/2, dt), then (dt, dt) k - 1 times, then (dt/2, 0).
+ * A bounded-wait timeout is reported by the next synchronising call
+ * (nbr_ctx_synchronize, a download). */
+int nbr_step_range(nbr_ctx* ctx, int precision, int scheme, size_t i0, size_t count, double kick,
+                   double drift, double G, double eps2);
+/* Device pointers of the current position and velocity arrays of the
+ * uploaded system (any pointer may be NULL) and their allocated length
+ * (*len >= n; entries >= n are zero-mass padding).  The position pointers
+ * change with every step (double buffering): query them after each step. */
+int nbr_state_pointers(nbr_ctx* ctx, double** x, double** y, double** z, double** vx, double** vy,
+                       double** vz, size_t* len);
+/* Declares that positions or velocities were written through
+ * nbr_state_pointers: FP32C source records are rebuilt from the positions at
+ * the next evaluation and stored accelerations are not reused. */
+int nbr_state_changed(nbr_ctx* ctx);
 /* ------------------------------------------------------------ tuning ---- */
 /* Forces a kernel configuration for the given precision (ni receivers per
  * thread: 4 or 8; warps per CTA: 2, 4 or 8; split >= 1 or 0 = automatic).

@@ -77,6 +77,11 @@ void SysState::release() {
 
 cudaError_t SysState::reserve(size_t n_) {
   const size_t np = ((n_ + 1023) / 1024) * 1024;
+  // Per-particle arrays carry kRangeSlack zeroed entries past n_pad: a force
+  // launch over a receiver range [i0, i0 + count) reads receivers in whole
+  // chunks (up to 1023 past the range end), and an all-gather of equal
+  // 128-aligned shards may write up to 8 x 127 entries past n.
+  const size_t na = np + kRangeSlack;
   if (np <= cap) {
     n = n_;
     n_pad = np;
@@ -89,15 +94,15 @@ cudaError_t SysState::reserve(size_t n_) {
     if (e == cudaSuccess) e = dalloc(p, bytes);
   };
   for (int b = 0; b < 2; ++b) {
-    for (int d = 0; d < 3; ++d) A((void**)&pos[b][d], np * sizeof(double));
+    for (int d = 0; d < 3; ++d) A((void**)&pos[b][d], na * sizeof(double));
     A((void**)&rec[b], np * 3 * sizeof(float4));
     A((void**)&org[b], (np / kTile) * sizeof(double4));
   }
   for (int d = 0; d < 3; ++d) {
-    A((void**)&vel[d], np * sizeof(double));
-    A((void**)&acc[d], np * sizeof(double));
+    A((void**)&vel[d], na * sizeof(double));
+    A((void**)&acc[d], na * sizeof(double));
   }
-  A((void**)&mass, np * sizeof(double));
+  A((void**)&mass, na * sizeof(double));
   if (e != cudaSuccess) {
     release();
     return e;
@@ -109,10 +114,11 @@ cudaError_t SysState::reserve(size_t n_) {
   return cudaSuccess;
 }
 
-// Zeroes the padding of every array (entries n .. n_pad-1), so padding
-// particles have zero mass and sit at the origin of both buffers.
+// Zeroes the padding of every per-particle array (entries n .. cap +
+// kRangeSlack - 1), so padding particles have zero mass and sit at the origin
+// of both buffers.
 cudaError_t SysState::clear_padding(cudaStream_t st) {
-  const size_t tail = n_pad - n;
+  const size_t tail = cap + kRangeSlack - n;
   cudaError_t e = cudaSuccess;
   auto Z = [&](double* p) {
     if (e == cudaSuccess && tail) e = cudaMemsetAsync(p + n, 0, tail * sizeof(double), st);
@@ -317,40 +323,49 @@ cudaError_t ensure_records(nbr_ctx* c, int b, int* kernels) {
 
 // One force evaluation of the uploaded system on its current buffer with the
 // given epilogue (mode 1 writes the next buffer, which becomes current).
+// Receivers are particles [r0, r0 + rn) (rn < 0: all n); sources are always
+// all n.  With a receiver range only the range's entries of the next buffer
+// are written, so no FP32C records are packed for it.
 int eval_system(nbr_ctx* c, int precision, double G, double eps2, int mode, double kick,
-                double drift, int want_force, int* kernels) {
+                double drift, int want_force, int* kernels, long long r0 = 0, long long rn = -1) {
   SysState& s = c->sys;
   const int a = s.cur, b = 1 - s.cur;
+  const bool ranged = rn >= 0;
+  if (!ranged) {
+    r0 = 0;
+    rn = (long long)s.n;
+  }
+  const long long np_i = ((rn + 1023) / 1024) * 1024;
   cudaError_t e = cudaSuccess;
   if (precision == kFP32C) e = ensure_records(c, a, kernels);
   if (e != cudaSuccess) return cuda_fail(c, e, "pack");
-  ForceConfig cfg = choose_config(c, precision, eps2, (long long)s.n, s.ntiles);
-  int rc = prepare_split(c, cfg, (long long)s.n_pad);
+  ForceConfig cfg = choose_config(c, precision, eps2, rn, s.ntiles);
+  int rc = prepare_split(c, cfg, np_i);
   if (rc) return rc;
-  IParticles ip{s.pos[a][0], s.pos[a][1], s.pos[a][2], s.mass, (long long)s.n};
+  IParticles ip{s.pos[a][0] + r0, s.pos[a][1] + r0, s.pos[a][2] + r0, s.mass + r0, rn};
   JStream js{s.pos[a][0], s.pos[a][1], s.pos[a][2], s.mass, s.rec[a], s.org[a], s.ntiles, 0, -1};
   pipeline_params(js);
   Epilogue ep{};
   ep.mode = mode;
   ep.G = G;
-  ep.ax = s.acc[0]; ep.ay = s.acc[1]; ep.az = s.acc[2];
+  ep.ax = s.acc[0] + r0; ep.ay = s.acc[1] + r0; ep.az = s.acc[2] + r0;
   ep.want_force = want_force;
   ep.kick = kick;
   ep.drift = drift;
-  ep.vx = s.vel[0]; ep.vy = s.vel[1]; ep.vz = s.vel[2];
-  ep.xn = s.pos[b][0]; ep.yn = s.pos[b][1]; ep.zn = s.pos[b][2];
-  ep.rec_next = (mode != 0 && precision == kFP32C) ? s.rec[b] : nullptr;
+  ep.vx = s.vel[0] + r0; ep.vy = s.vel[1] + r0; ep.vz = s.vel[2] + r0;
+  ep.xn = s.pos[b][0] + r0; ep.yn = s.pos[b][1] + r0; ep.zn = s.pos[b][2] + r0;
+  ep.rec_next = (mode != 0 && precision == kFP32C && !ranged) ? s.rec[b] : nullptr;
   ep.origin_next = s.org[b];
   ep.part = c->scr.part;
   ep.counters = c->scr.cnt;
-  ep.n_pad = (long long)s.n_pad;
+  ep.n_pad = np_i;
   ep.err = c->d_err;
   e = launch_force(precision, eps2, cfg, ip, js, ep, c->stream);
   if (kernels) ++*kernels;
   if (e != cudaSuccess) return cuda_fail(c, e, "force launch");
   if (mode != 0) {
     s.cur = b;
-    s.rec_ok[b] = (precision == kFP32C);
+    s.rec_ok[b] = (precision == kFP32C) && !ranged;
     s.rec_ok[a] = false;
   }
   return NBR_OK;
@@ -505,8 +520,11 @@ void* nbr_ctx_stream(nbr_ctx* c) { return c ? (void*)c->stream : nullptr; }
 
 int nbr_ctx_synchronize(nbr_ctx* c) {
   if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
+  cudaSetDevice(c->device);
   cudaError_t e = cudaStreamSynchronize(c->stream);
-  return e == cudaSuccess ? NBR_OK : cuda_fail(c, e, "synchronize");
+  if (e != cudaSuccess) return cuda_fail(c, e, "synchronize");
+  // A bounded wait that gave up in an asynchronous call surfaces here.
+  return check_device_error(c);
 }
 
 size_t nbr_system_size(const nbr_ctx* c) { return c ? c->sys.n : 0; }
@@ -624,6 +642,53 @@ int nbr_forces_download(nbr_ctx* c, double* ax, double* ay, double* az) {
   D(ax, s.acc[0]); D(ay, s.acc[1]); D(az, s.acc[2]);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   return e == cudaSuccess ? NBR_OK : cuda_fail(c, e, "forces download");
+}
+
+// ------------------------------------------------ multi-GPU i-partition ----
+
+int nbr_step_range(nbr_ctx* c, int precision, int scheme, size_t i0, size_t count, double kick,
+                   double drift, double G, double eps2) {
+  if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
+  if (precision != NBR_FP64 && precision != NBR_FP32C)
+    return fail(c, NBR_ERR_INVALID_ARG, "unknown precision");
+  if (scheme != NBR_KDK && scheme != NBR_DKD && scheme != NBR_EULER)
+    return fail(c, NBR_ERR_INVALID_ARG, "unknown scheme");
+  if (!std::isfinite(kick) || !std::isfinite(drift) || !(eps2 >= 0.0) || !std::isfinite(eps2) ||
+      !std::isfinite(G))
+    return fail(c, NBR_ERR_INVALID_ARG, "kick, drift, G must be finite, eps2 finite and >= 0");
+  SysState& s = c->sys;
+  if (s.n == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no system uploaded");
+  if (i0 % kTile != 0) return fail(c, NBR_ERR_INVALID_ARG, "i0 must be a multiple of 128");
+  if (count == 0 || i0 >= s.n) return fail(c, NBR_ERR_INVALID_ARG, "empty receiver range");
+  const size_t rn = std::min(count, s.n - i0);
+  cudaSetDevice(c->device);
+  const int rc = eval_system(c, precision, G, eps2, scheme == NBR_EULER ? 2 : 1, kick, drift, 0,
+                             nullptr, (long long)i0, (long long)rn);
+  c->acc_ok = false;
+  return rc;
+}
+
+int nbr_state_pointers(nbr_ctx* c, double** x, double** y, double** z, double** vx, double** vy,
+                       double** vz, size_t* len) {
+  if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
+  SysState& s = c->sys;
+  if (s.n == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no system uploaded");
+  if (x) *x = s.pos[s.cur][0];
+  if (y) *y = s.pos[s.cur][1];
+  if (z) *z = s.pos[s.cur][2];
+  if (vx) *vx = s.vel[0];
+  if (vy) *vy = s.vel[1];
+  if (vz) *vz = s.vel[2];
+  if (len) *len = s.n_pad + kRangeSlack;
+  return NBR_OK;
+}
+
+int nbr_state_changed(nbr_ctx* c) {
+  if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
+  SysState& s = c->sys;
+  s.rec_ok[0] = s.rec_ok[1] = false;
+  c->acc_ok = false;
+  return NBR_OK;
 }
 
 int nbr_accel_ij(nbr_ctx* c, int precision, size_t n_i, const double* xi, const double* yi,

@@ -13,7 +13,12 @@ namespace nbr {
 // Device state of one particle system (or of a batch of systems stored back to
 // back).  Positions are double-buffered: a force evaluation reads buffer
 // `cur` and its fused kick/drift epilogue writes buffer 1 - cur.  Every array
-// holds n_pad entries; entries >= n are zero-mass padding at the origin.
+// holds n_pad entries (per-particle arrays kRangeSlack more); entries >= n are
+// zero-mass padding at the origin.
+// Zeroed entries allocated past n_pad in every per-particle array (see
+// SysState::reserve).
+constexpr size_t kRangeSlack = 1024;
+
 struct SysState {
   size_t n = 0, n_pad = 0, cap = 0;
   int ntiles = 0;

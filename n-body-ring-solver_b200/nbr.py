@@ -100,6 +100,10 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "nbr_batch_run": ([C.c_void_p, C.c_int, C.c_double, _SZ, C.c_double, C.c_double,
                            C.POINTER(RunStats)], C.c_int),
         "nbr_batch_diagnostics": ([C.c_void_p, C.c_double, C.c_double, C.POINTER(Diag)], C.c_int),
+        "nbr_step_range": ([C.c_void_p, C.c_int, C.c_int, _SZ, _SZ, C.c_double, C.c_double, C.c_double,
+                            C.c_double], C.c_int),
+        "nbr_state_pointers": ([C.c_void_p] + [C.POINTER(C.c_void_p)] * 6 + [C.POINTER(_SZ)], C.c_int),
+        "nbr_state_changed": ([C.c_void_p], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -204,6 +208,15 @@ def batch_plummer(nsys: int, seed: int, nmin: int = 64, nmax: int = 4096):
     return off, st
 
 
+class _DeviceArray:
+    """A float64 device array the library owns, exposed through
+    __cuda_array_interface__ so torch can view it without a copy."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False),
+                                         "version": 2, "strides": None}
+
+
 # ------------------------------------------------------------------- context --
 class Context:
     """One GPU context (its own CUDA stream); see include/nbr.h."""
@@ -216,6 +229,7 @@ class Context:
         self.L = L
         self.h = h
         self.n = 0
+        self.device = device
 
     def close(self):
         if self.h:
@@ -319,6 +333,33 @@ class Context:
         if diag:
             out["diag"] = (d[0].as_dict(), d[1].as_dict())
         return out
+
+    # multi-GPU i-partition (see nbr_shard.py)
+    def step_range(self, precision, scheme, i0, count, kick, drift, G=1.0, eps2=0.0):
+        """One force evaluation of receivers [i0, i0 + count) with the fused
+        kick/drift, asynchronous on the context's stream."""
+        self._chk(self.L.nbr_step_range(self.h, precision, scheme, i0, count, kick, drift, G, eps2),
+                  "step_range")
+
+    def state_pointers(self):
+        """Device addresses of the current x, y, z, vx, vy, vz arrays and their length."""
+        ptrs = [C.c_void_p() for _ in range(6)]
+        ln = _SZ()
+        self._chk(self.L.nbr_state_pointers(self.h, *[C.byref(p) for p in ptrs], C.byref(ln)),
+                  "state_pointers")
+        return dict(zip(KEYS[:6], [int(p.value or 0) for p in ptrs])), int(ln.value)
+
+    def state_tensors(self):
+        """The current x, y, z, vx, vy, vz as float64 torch tensors viewing
+        the context's device memory (valid until the next upload; positions
+        until the next step)."""
+        import torch
+        ptrs, ln = self.state_pointers()
+        dev = torch.device("cuda", self.device)
+        return {k: torch.as_tensor(_DeviceArray(p, ln), device=dev) for k, p in ptrs.items()}
+
+    def state_changed(self):
+        self._chk(self.L.nbr_state_changed(self.h), "state_changed")
 
     def set_force_config(self, precision, ni=0, warps=0, split=0):
         self._chk(self.L.nbr_set_force_config(self.h, precision, ni, warps, split), "set_force_config")

@@ -1,0 +1,129 @@
+"""nbr_step_range / nbr_state_pointers / nbr_state_changed on one GPU.
+
+The i-partition is emulated with several contexts on the same GPU, one per
+rank, exchanging owned slices by device copies between steps (each launch
+finishes before the next begins: no kernel waits on another).  With the same
+kernel configuration forced everywhere, the per-receiver summation order is
+the same as in one whole-system run, so the emulated ranks must reproduce
+nbr_run bit for bit.  The process-group exchange itself is covered on CPU by
+test_shard.py.
+"""
+import numpy as np
+import pytest
+import torch
+
+import nbr_shard
+
+pytestmark = pytest.mark.gpu
+
+CFG = {0: (4, 4, 4), 1: (8, 2, 4)}  # precision -> (ni, warps, split) on every context
+
+
+def _contexts(nbr, k, s, precision):
+    out = []
+    for _ in range(k):
+        c = nbr.Context(0)
+        c.set_force_config(precision, *CFG[precision])
+        c.upload(s)
+        out.append(c)
+    return out
+
+
+def _exchange(ctxs, n):
+    """Every context receives every other context's owned position slice."""
+    world = len(ctxs)
+    for c in ctxs:
+        c.synchronize()
+    st = [c.state_tensors() for c in ctxs]
+    for r in range(world):
+        i0, _, owned = nbr_shard.shard_bounds(n, world, r)
+        for q in range(world):
+            if q != r and owned:
+                for k in ("x", "y", "z"):
+                    st[q][k][i0:i0 + owned].copy_(st[r][k][i0:i0 + owned])
+    torch.cuda.synchronize()
+    for c in ctxs:
+        c.state_changed()
+
+
+def _gather_velocities(ctxs, n):
+    world = len(ctxs)
+    st = [c.state_tensors() for c in ctxs]
+    for r in range(world):
+        i0, _, owned = nbr_shard.shard_bounds(n, world, r)
+        for k in ("vx", "vy", "vz"):
+            st[0][k][i0:i0 + owned].copy_(st[r][k][i0:i0 + owned])
+    torch.cuda.synchronize()
+    ctxs[0].state_changed()
+
+
+def _emulated_run(nbr, s, precision, scheme, dt, steps, world, eps2):
+    n = len(s["x"])
+    ctxs = _contexts(nbr, world, s, precision)
+    if scheme == nbr.KDK:
+        sched = [(0.5 * dt, dt)] + [(dt, dt)] * (steps - 1) + [(0.5 * dt, 0.0)]
+    else:
+        sched = [(dt, dt)] * steps
+    for kick, drift in sched:
+        for r, c in enumerate(ctxs):
+            i0, _, owned = nbr_shard.shard_bounds(n, world, r)
+            if owned:
+                c.step_range(precision, scheme, i0, owned, kick, drift, 1.0, eps2)
+        _exchange(ctxs, n)
+    _gather_velocities(ctxs, n)
+    out = ctxs[0].download()
+    for c in ctxs:
+        c.synchronize()
+        c.close()
+    return out
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "fp32c"])
+@pytest.mark.parametrize("scheme", [0, 2], ids=["kdk", "euler"])
+@pytest.mark.parametrize("n,world", [(8192, 2), (5000, 3)])
+def test_emulated_ranks_match_whole_run(nbr, precision, scheme, n, world):
+    s = nbr.plummer(n, 5)
+    eps2, dt, steps = 1e-6, 1e-3, 3
+    whole = nbr.Context(0)
+    whole.set_force_config(precision, *CFG[precision])
+    whole.upload(s)
+    whole.run(precision, scheme, 2, dt, steps, eps2=eps2)
+    ref = whole.download()
+    whole.close()
+    got = _emulated_run(nbr, s, precision, scheme, dt, steps, world, eps2)
+    for k in ("x", "y", "z", "vx", "vy", "vz"):
+        np.testing.assert_array_equal(got[k], ref[k], err_msg=k)
+
+
+def test_step_range_matches_oracle_forces(nbr, oracle):
+    """The owned slice's accelerations (FP64) against the oracle's, through
+    a step with kick 1 and drift 0 from zero velocities: v = a."""
+    n = 3000
+    s = nbr.plummer(n, 6)
+    s["vx"][:] = 0.0; s["vy"][:] = 0.0; s["vz"][:] = 0.0
+    c = nbr.Context(0)
+    c.upload(s)
+    c.step_range(nbr.FP64, nbr.KDK, 1024, 1500, 1.0, 0.0, 1.0, 1e-4)
+    c.synchronize()
+    st = c.state_tensors()
+    v = np.stack([st[k][:n].cpu().numpy() for k in ("vx", "vy", "vz")])
+    c.close()
+    a = oracle.accel(s["x"], s["y"], s["z"], s["m"], 1.0, 1e-4)
+    sl = slice(1024, 2524)
+    np.testing.assert_allclose(v[:, sl], a[:, sl], rtol=1e-12, atol=1e-12 * np.abs(a).max())
+    assert not v[:, :1024].any() and not v[:, 2524:].any()
+
+
+def test_step_range_argument_errors(nbr):
+    s = nbr.plummer(1000, 1)
+    c = nbr.Context(0)
+    c.upload(s)
+    for args in ((100, 10), (0, 0), (1024, 5)):
+        with pytest.raises(nbr.NbrError) as e:
+            c.step_range(nbr.FP64, nbr.KDK, args[0], args[1], 1.0, 1.0)
+        assert e.value.status == 1
+    with pytest.raises(nbr.NbrError):
+        c.step_range(7, nbr.KDK, 0, 128, 1.0, 1.0)
+    ptrs, ln = c.state_pointers()
+    assert ln >= 1024 + 1024 and all(p for p in ptrs.values())
+    c.close()
