@@ -86,13 +86,16 @@ int nbr_device_count(void);
 /* The context's CUDA stream (a cudaStream_t as an opaque pointer), for callers
  * that time or order their own work against the solver's. */
 void* nbr_ctx_stream(nbr_ctx* ctx);
-/* Waits for all work issued on the context's stream. */
+/* Waits for all work issued on the context's stream; reports a bounded-wait
+ * timeout (NBR_ERR_TIMEOUT) of asynchronous calls issued before it. */
 int nbr_ctx_synchronize(nbr_ctx* ctx);
 
 /* -------------------------------------------------------------- state ---- */
 /* Copies a system of n particles in (replaces NBody_system::alloc_particles +
  * the initialisers' stores, CPU/nbody_system.cpp:177-193).  vx/vy/vz may be
- * NULL (zero velocities).  Rejects NaN/Inf and negative masses. */
+ * NULL (zero velocities).  Rejects NaN/Inf (NBR_ERR_NONFINITE) and negative
+ * masses (NBR_ERR_INVALID_ARG); the check runs on the device copy, and a
+ * rejected upload leaves the context with no system. */
 int nbr_system_upload(nbr_ctx* ctx, size_t n, const double* x, const double* y, const double* z,
                       const double* vx, const double* vy, const double* vz, const double* m);
 /* Copies the current state out; any pointer may be NULL. */

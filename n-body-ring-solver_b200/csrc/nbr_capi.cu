@@ -536,11 +536,6 @@ int nbr_system_upload(nbr_ctx* c, size_t n, const double* x, const double* y, co
   if ((vx || vy || vz) && !(vx && vy && vz))
     return fail(c, NBR_ERR_INVALID_ARG, "velocities must be all given or all NULL");
   if (n > (size_t)1 << 31) return fail(c, NBR_ERR_INVALID_ARG, "n above 2^31");
-  if (!finite_array(x, n) || !finite_array(y, n) || !finite_array(z, n) || !finite_array(m, n) ||
-      (vx && (!finite_array(vx, n) || !finite_array(vy, n) || !finite_array(vz, n))))
-    return fail(c, NBR_ERR_NONFINITE, "input contains NaN or Inf");
-  for (size_t i = 0; i < n; ++i)
-    if (m[i] < 0.0) return fail(c, NBR_ERR_INVALID_ARG, "negative mass");
   cudaSetDevice(c->device);
   SysState& s = c->sys;
   cudaError_t e = s.reserve(n);
@@ -559,9 +554,24 @@ int nbr_system_upload(nbr_ctx* c, size_t n, const double* x, const double* y, co
     for (int d = 0; d < 3 && e == cudaSuccess; ++d)
       e = cudaMemsetAsync(s.vel[d], 0, B, c->stream);
   }
+  // NaN / Inf / negative-mass check on the device copy (one pass over the
+  // uploaded bytes at HBM speed instead of a host loop over them).
+  int* flags = c->d_err + 1;
+  int h_flags = 0;
+  if (e == cudaSuccess) e = cudaMemsetAsync(flags, 0, sizeof(int), c->stream);
+  if (e == cudaSuccess)
+    e = launch_validate((long long)n, s.pos[0][0], s.pos[0][1], s.pos[0][2], vx ? s.vel[0] : nullptr,
+                        s.vel[1], s.vel[2], s.mass, flags, c->sms, c->stream);
   if (e == cudaSuccess) e = s.clear_padding(c->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&h_flags, flags, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "upload");
+  if (h_flags) {
+    s.n = 0;  // the rejected system is not kept
+    return (h_flags & 1) ? fail(c, NBR_ERR_NONFINITE, "input contains NaN or Inf")
+                         : fail(c, NBR_ERR_INVALID_ARG, "negative mass");
+  }
   return NBR_OK;
 }
 

@@ -37,6 +37,7 @@
 #include "nbr_device.cuh"
 #include "nbr_kernels.cuh"
 
+#include <algorithm>
 #include <cstdio>
 
 namespace nbr {
@@ -526,6 +527,28 @@ __global__ void __launch_bounds__(256) k_rowsum(const double* __restrict__ part,
   }
 }
 
+// Input validation of an uploaded system, on the device after the copy:
+// sets bit 0 of *flags if a coordinate, velocity or mass is NaN or Inf and
+// bit 1 if a mass is negative.  Velocities may be null.
+__global__ void __launch_bounds__(256) k_validate(long long n, const double* __restrict__ x,
+                                                  const double* __restrict__ y,
+                                                  const double* __restrict__ z,
+                                                  const double* __restrict__ vx,
+                                                  const double* __restrict__ vy,
+                                                  const double* __restrict__ vz,
+                                                  const double* __restrict__ m, int* flags) {
+  int f = 0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const double mm = m[i];
+    bool bad = !isfinite(x[i]) || !isfinite(y[i]) || !isfinite(z[i]) || !isfinite(mm);
+    if (vx) bad = bad || !isfinite(vx[i]) || !isfinite(vy[i]) || !isfinite(vz[i]);
+    f |= (bad ? 1 : 0) | (mm < 0.0 ? 2 : 0);
+  }
+  f = __reduce_or_sync(0xffffffffu, f);
+  if ((threadIdx.x & 31) == 0 && f) atomicOr(flags, f);
+}
+
 // -------------------------------------------------------------- dispatch ----
 template <int NI, int W, bool EX>
 cudaError_t launch_f32c_t(float eps2f, int split, const IParticles& ip, const JStream& js,
@@ -643,6 +666,16 @@ cudaError_t launch_moments(long long n, long long n_pad, const double* x, const 
 cudaError_t launch_rowsum(const double* part, int nblocks, int width, double* out,
                           cudaStream_t st) {
   k_rowsum<<<1, 256, 0, st>>>(part, nblocks, width, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_validate(long long n, const double* x, const double* y, const double* z,
+                            const double* vx, const double* vy, const double* vz,
+                            const double* m, int* flags, int sms, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  const long long want = (n + 255) / 256;
+  const unsigned blocks = (unsigned)std::min<long long>(want, 8LL * (sms > 0 ? sms : 148));
+  k_validate<<<blocks, 256, 0, st>>>(n, x, y, z, vx, vy, vz, m, flags);
   return cudaGetLastError();
 }
 

@@ -82,6 +82,11 @@ cudaError_t launch_moments(long long n, long long n_pad, const double* x, const 
 // Sums nblocks rows of `width` doubles in block order (deterministic).
 cudaError_t launch_rowsum(const double* part, int nblocks, int width, double* out,
                           cudaStream_t stream);
+// Sets bit 0 of *flags if any x, y, z, (vx, vy, vz,) m entry is NaN or Inf,
+// bit 1 if a mass is negative (vx may be null: no velocities).
+cudaError_t launch_validate(long long n, const double* x, const double* y, const double* z,
+                            const double* vx, const double* vy, const double* vz,
+                            const double* m, int* flags, int sms, cudaStream_t stream);
 size_t force_smem_bytes(int precision, const ForceConfig& cfg);
 // Resident CTAs per SM of the force kernel for this configuration (0 on error).
 int force_blocks_per_sm(int precision, double eps2, const ForceConfig& cfg);

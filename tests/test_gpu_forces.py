@@ -174,6 +174,16 @@ def test_invalid_inputs_are_rejected(ctx, nbr):
     with pytest.raises(nbr.NbrError) as ei:
         ctx.upload(neg)
     assert ei.value.status == 1
+    # a rejected upload leaves no system behind
+    with pytest.raises(nbr.NbrError) as ei:
+        ctx.forces(FP64, eps2=0.0)
+    assert ei.value.status == 5
+    inf_v = dict(s)
+    inf_v["vz"] = s["vz"].copy()
+    inf_v["vz"][99] = np.inf
+    with pytest.raises(nbr.NbrError) as ei:
+        ctx.upload(inf_v)
+    assert ei.value.status == 7
     upload(ctx, s)
     with pytest.raises(nbr.NbrError):
         ctx.forces(FP64, eps2=-1.0)
