@@ -58,6 +58,23 @@ cudaError_t dalloc(void** p, size_t bytes) {
   return cudaDeviceSynchronize();
 }
 
+bool RunKey::operator==(const RunKey& o) const {
+  if (precision != o.precision || scheme != o.scheme || order != o.order || dt != o.dt ||
+      G != o.G || eps2 != o.eps2 || steps != o.steps || n != o.n || cap != o.cap ||
+      fsal != o.fsal || cur != o.cur || rec_ok[0] != o.rec_ok[0] || rec_ok[1] != o.rec_ok[1] ||
+      cfg.ni != o.cfg.ni || cfg.warps != o.cfg.warps || cfg.split != o.cfg.split ||
+      wait_ns != o.wait_ns || skip_tile != o.skip_tile)
+    return false;
+  for (int i = 0; i < 6; ++i)
+    if (ptr[i] != o.ptr[i]) return false;
+  return true;
+}
+
+void RunGraph::release() {
+  if (exec) cudaGraphExecDestroy(exec);
+  *this = RunGraph();
+}
+
 bool finite_array(const double* a, size_t n) {
   bool ok = true;
   for (size_t i = 0; i < n; ++i) ok &= std::isfinite(a[i]);
@@ -504,6 +521,7 @@ int nbr_ctx_destroy(nbr_ctx* c) {
   if (!c) return NBR_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  c->run_graph.release();
   c->sys.release();
   c->bat.release();
   c->scr.release();
@@ -843,70 +861,104 @@ int nbr_run(nbr_ctx* c, int precision, int scheme, int order, double dt, size_t 
     if (rc) return rc;
     const bool fsal = (scheme == NBR_KDK) && c->acc_ok && c->acc_prec == precision &&
                       c->acc_G == G && c->acc_eps2 == eps2;
-    cudaGraph_t graph = nullptr;
-    cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
-    if (e != cudaSuccess) return cuda_fail(c, e, "begin capture");
+    // A repeated call (same arguments, starting state and buffers) replays the
+    // graph captured last time instead of capturing and instantiating again.
+    RunKey key;
+    key.precision = precision; key.scheme = scheme; key.order = order;
+    key.dt = dt; key.G = G; key.eps2 = eps2; key.steps = steps;
+    key.n = s.n; key.cap = s.cap; key.fsal = fsal; key.cur = s.cur;
+    key.rec_ok[0] = s.rec_ok[0]; key.rec_ok[1] = s.rec_ok[1];
+    key.cfg = cfg;
+    {
+      JStream probe{};
+      pipeline_params(probe);
+      key.wait_ns = probe.wait_ns;
+      key.skip_tile = probe.skip_tile;
+    }
+    key.ptr[0] = s.pos[0][0]; key.ptr[1] = s.rec[0]; key.ptr[2] = s.vel[0];
+    key.ptr[3] = c->scr.part; key.ptr[4] = c->scr.cnt; key.ptr[5] = c->d_err;
+    RunGraph& rg = c->run_graph;
     int kernels = 0;
     double evals = 0;
-    const int cur0 = s.cur;
-    const bool rec0 = s.rec_ok[0], rec1 = s.rec_ok[1];
-    rc = NBR_OK;
-    const bool fp32 = precision == kFP32C;
-    if (scheme == NBR_KDK) {
-      if (fsal) {
-        rc = kick_drift_system(c, fp32, 0.5 * dt, dt, true, &kernels);
-      } else {
-        rc = eval_system(c, precision, G, eps2, 1, 0.5 * dt, dt, 0, &kernels);
-        evals += 1;
-      }
-      for (size_t k = 1; k < steps && rc == NBR_OK; ++k) {
-        rc = eval_system(c, precision, G, eps2, 1, dt, dt, 0, &kernels);
-        evals += 1;
-      }
-      if (rc == NBR_OK) {
-        rc = eval_system(c, precision, G, eps2, 1, 0.5 * dt, 0.0, 0, &kernels);
-        evals += 1;
-      }
-    } else if (scheme == NBR_EULER) {
-      for (size_t k = 0; k < steps && rc == NBR_OK; ++k) {
-        rc = eval_system(c, precision, G, eps2, 2, dt, dt, 0, &kernels);
-        evals += 1;
-      }
+    cudaError_t e = cudaSuccess;
+    if (rg.exec && rg.key == key) {
+      s.cur = rg.cur_after;
+      s.rec_ok[0] = rg.rec_after[0];
+      s.rec_ok[1] = rg.rec_after[1];
+      kernels = rg.kernels;
+      evals = rg.evals;
     } else {
-      rc = kick_drift_system(c, fp32, 0.0, cc[0] * dt, false, &kernels);
-      for (size_t k = 0; k < steps && rc == NBR_OK; ++k) {
-        for (int sub = 0; sub < lf - 1 && rc == NBR_OK; ++sub) {
-          double drift;
-          if (sub < lf - 2) drift = cc[sub + 1];
-          else drift = (k + 1 < steps) ? cc[lf - 1] + cc[0] : cc[lf - 1];
-          rc = eval_system(c, precision, G, eps2, 1, dd[sub] * dt, drift * dt, 0, &kernels);
+      rg.release();
+      cudaGraph_t graph = nullptr;
+      e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+      if (e != cudaSuccess) return cuda_fail(c, e, "begin capture");
+      const int cur0 = s.cur;
+      const bool rec0 = s.rec_ok[0], rec1 = s.rec_ok[1];
+      rc = NBR_OK;
+      const bool fp32 = precision == kFP32C;
+      if (scheme == NBR_KDK) {
+        if (fsal) {
+          rc = kick_drift_system(c, fp32, 0.5 * dt, dt, true, &kernels);
+        } else {
+          rc = eval_system(c, precision, G, eps2, 1, 0.5 * dt, dt, 0, &kernels);
           evals += 1;
         }
+        for (size_t k = 1; k < steps && rc == NBR_OK; ++k) {
+          rc = eval_system(c, precision, G, eps2, 1, dt, dt, 0, &kernels);
+          evals += 1;
+        }
+        if (rc == NBR_OK) {
+          rc = eval_system(c, precision, G, eps2, 1, 0.5 * dt, 0.0, 0, &kernels);
+          evals += 1;
+        }
+      } else if (scheme == NBR_EULER) {
+        for (size_t k = 0; k < steps && rc == NBR_OK; ++k) {
+          rc = eval_system(c, precision, G, eps2, 2, dt, dt, 0, &kernels);
+          evals += 1;
+        }
+      } else {
+        rc = kick_drift_system(c, fp32, 0.0, cc[0] * dt, false, &kernels);
+        for (size_t k = 0; k < steps && rc == NBR_OK; ++k) {
+          for (int sub = 0; sub < lf - 1 && rc == NBR_OK; ++sub) {
+            double drift;
+            if (sub < lf - 2) drift = cc[sub + 1];
+            else drift = (k + 1 < steps) ? cc[lf - 1] + cc[0] : cc[lf - 1];
+            rc = eval_system(c, precision, G, eps2, 1, dd[sub] * dt, drift * dt, 0, &kernels);
+            evals += 1;
+          }
+        }
       }
-    }
-    cudaError_t ee = cudaStreamEndCapture(c->stream, &graph);
-    if (rc != NBR_OK || ee != cudaSuccess) {
-      if (graph) cudaGraphDestroy(graph);
-      s.cur = cur0;
-      s.rec_ok[0] = rec0;
-      s.rec_ok[1] = rec1;
-      return rc != NBR_OK ? rc : cuda_fail(c, ee, "end capture");
-    }
-    cudaGraphExec_t exec = nullptr;
-    e = cudaGraphInstantiate(&exec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (e != cudaSuccess) {
-      s.cur = cur0;
-      s.rec_ok[0] = rec0;
-      s.rec_ok[1] = rec1;
-      return cuda_fail(c, e, "graph instantiate");
+      cudaError_t ee = cudaStreamEndCapture(c->stream, &graph);
+      if (rc != NBR_OK || ee != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        s.cur = cur0;
+        s.rec_ok[0] = rec0;
+        s.rec_ok[1] = rec1;
+        return rc != NBR_OK ? rc : cuda_fail(c, ee, "end capture");
+      }
+      cudaGraphExec_t exec = nullptr;
+      e = cudaGraphInstantiate(&exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess) {
+        s.cur = cur0;
+        s.rec_ok[0] = rec0;
+        s.rec_ok[1] = rec1;
+        return cuda_fail(c, e, "graph instantiate");
+      }
+      rg.exec = exec;
+      rg.key = key;
+      rg.cur_after = s.cur;
+      rg.rec_after[0] = s.rec_ok[0];
+      rg.rec_after[1] = s.rec_ok[1];
+      rg.kernels = kernels;
+      rg.evals = evals;
     }
     e = cudaEventRecord(c->ev0, c->stream);
-    if (e == cudaSuccess) e = cudaGraphLaunch(exec, c->stream);
+    if (e == cudaSuccess) e = cudaGraphLaunch(rg.exec, c->stream);
     if (e == cudaSuccess) e = cudaEventRecord(c->ev1, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-    cudaGraphExecDestroy(exec);
     if (e != cudaSuccess) {
+      rg.release();
       c->acc_ok = false;
       return cuda_fail(c, e, "graph launch");
     }

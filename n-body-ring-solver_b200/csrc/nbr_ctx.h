@@ -87,6 +87,34 @@ void pipeline_params(JStream& js);
 
 }  // namespace nbr
 
+namespace nbr {
+// Identity of a captured nbr_run launch sequence: the call's arguments, the
+// host-side state it starts from and every device address it bakes in.
+struct RunKey {
+  int precision = -1, scheme = -1, order = 0;
+  double dt = 0.0, G = 0.0, eps2 = 0.0;
+  size_t steps = 0, n = 0, cap = 0;
+  bool fsal = false;
+  int cur = 0;
+  bool rec_ok[2] = {false, false};
+  ForceConfig cfg{0, 0, 0};
+  unsigned long long wait_ns = 0;
+  int skip_tile = -1;
+  const void* ptr[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  bool operator==(const RunKey& o) const;
+};
+// The last nbr_run graph, replayed while the key matches.
+struct RunGraph {
+  cudaGraphExec_t exec = nullptr;
+  RunKey key;
+  int cur_after = 0;
+  bool rec_after[2] = {false, false};
+  int kernels = 0;
+  double evals = 0.0;
+  void release();
+};
+}  // namespace nbr
+
 struct nbr_ctx {
   int device = 0;
   int sms = 148;
@@ -104,4 +132,5 @@ struct nbr_ctx {
   int acc_prec = 0;
   double acc_G = 0.0, acc_eps2 = 0.0;
   nbr::ForceConfig override_cfg[2] = {{0, 0, 0}, {0, 0, 0}};
+  nbr::RunGraph run_graph;
 };

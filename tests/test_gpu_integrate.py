@@ -91,6 +91,30 @@ def test_kdk_first_same_as_last(ctx, nbr):
         np.testing.assert_allclose(two[k], one[k], rtol=0, atol=1e-13 * max(1.0, np.abs(one[k]).max()))
 
 
+def test_replayed_run_graphs(ctx, nbr, oracle):
+    """nbr_run replays its last graph when a call repeats (same arguments,
+    starting state and buffers).  A sequence of repeated and alternating
+    one-step calls must follow the oracle's sequence of the same steps."""
+    s = nbr.plummer(2048, 3)
+    eps2, dt = 1e-6, 1e-3
+    ctx.upload(s)
+    want = {k: v.copy() for k, v in s.items()}
+    plan = [(KDK, 2, 4), (DKD, 4, 3), (KDK, 2, 3), (EULER, 2, 2), (DKD, 2, 2), (KDK, 2, 2)]
+    for scheme, order, calls in plan:
+        for _ in range(calls):
+            st = ctx.run(FP64, scheme, order, dt, 1, eps2=eps2)
+            assert st["force_evals"] >= 1 and st["kernels"] >= 1
+        if scheme == KDK:
+            want = oracle.kdk(want, dt, calls, eps2=eps2)
+        elif scheme == DKD:
+            for _ in range(calls):
+                want = oracle.dkd(want, dt, 1, order=order, eps2=eps2)
+        else:
+            want = oracle.euler(want, dt, calls, eps2=eps2)
+    got = ctx.download()
+    assert_state_close(got, want, 1e-11)
+
+
 def test_ring_rotation_known_answer(ctx, nbr):
     """The reference's ring experiment: after one revolution (dt = 1/1000,
     1000 DKD steps) every ring particle is back near its start
