@@ -35,7 +35,8 @@ typedef enum nbr_status {
   NBR_ERR_TIMEOUT = 4,      /* a bounded device wait gave up (kernel aborted cleanly) */
   NBR_ERR_NO_SYSTEM = 5,    /* no particles uploaded yet */
   NBR_ERR_UNSUPPORTED = 6,  /* no CUDA device / unsupported configuration */
-  NBR_ERR_NONFINITE = 7     /* an input contains NaN or Inf */
+  NBR_ERR_NONFINITE = 7,    /* an input contains NaN or Inf */
+  NBR_ERR_IO = 8            /* a snapshot file could not be opened, read or written */
 } nbr_status;
 
 /* Arithmetic of the pair interaction. */
@@ -227,6 +228,36 @@ int nbr_state_pointers(nbr_ctx* ctx, double** x, double** y, double** z, double*
  * nbr_state_pointers: FP32C source records are rebuilt from the positions at
  * the next evaluation and stored accelerations are not reused. */
 int nbr_state_changed(nbr_ctx* ctx);
+/* ---------------------------------------------------------- snapshots ---- */
+/* Checkpoints in the reference's binary snapshot format,
+ * NBody_system::save_particles (CPU/nbody_system.cpp:133-152): per record the
+ * time time_step * delta_t, then n masses, positions x, y, z, velocities
+ * x, y, z and forces x, y, z, all native-endian doubles (8 + 80 n bytes).  The
+ * reference names the file "NBody_<n>.dat"; here the caller names it.
+ * time_step == 0 truncates the file, any other value appends a record. */
+
+/* One record from host arrays (m, x, y, z required; velocities and forces may
+ * be NULL: written as zeros).  No context and no GPU needed. */
+int nbr_snapshot_write_arrays(const char* path, size_t n, size_t time_step, double delta_t,
+                              const double* m, const double* x, const double* y, const double* z,
+                              const double* vx, const double* vy, const double* vz,
+                              const double* fx, const double* fy, const double* fz);
+/* One record of the context's current state.  Forces are m_i a_i of the
+ * current positions when the context holds those accelerations (after
+ * nbr_forces with want_force = 0, nbr_forces_device or a KDK nbr_run), zeros
+ * otherwise. */
+int nbr_snapshot_save(nbr_ctx* ctx, const char* path, size_t time_step, double delta_t);
+/* Number of whole n-particle records in the file (NBR_ERR_INVALID_ARG when the
+ * size is not a whole number of records: wrong n or a truncated file). */
+int nbr_snapshot_records(const char* path, size_t n, size_t* records);
+/* Record `record` (0-based) into host arrays; any output may be NULL. */
+int nbr_snapshot_read_arrays(const char* path, size_t n, size_t record, double* time, double* m,
+                             double* x, double* y, double* z, double* vx, double* vy, double* vz,
+                             double* fx, double* fy, double* fz);
+/* Resume: uploads record `record` (masses, positions, velocities) as the
+ * context's system; *time (may be NULL) receives its time. */
+int nbr_snapshot_load(nbr_ctx* ctx, const char* path, size_t n, size_t record, double* time);
+
 /* ------------------------------------------------------------ tuning ---- */
 /* Forces a kernel configuration for the given precision (ni receivers per
  * thread: 4 or 8; warps per CTA: 2, 4 or 8; split >= 1 or 0 = automatic).

@@ -12,8 +12,11 @@
 //   -t gpu-batch     many independent systems in one persistent launch.
 // Added flags: -eps (softening length), -dt (overrides T/s), -ic
 // ring|plummer|ball|twocomp|random, -seed, -scheme dkd|kdk, -G, -nsys, -nmin,
-// -nmax, -autotune.  -p accepts dp|sp (reference names) and fp64|fp32c;
-// sp selects the FP32-compensated kernel.
+// -nmax, -autotune, -save K (a record of the reference's snapshot format,
+// NBody_<N>.dat as save_particles names it, at step 0 and every K steps) and
+// -resume PATH (start from the last record of a snapshot file of N particles).
+// -p accepts dp|sp (reference names) and fp64|fp32c; sp selects the
+// FP32-compensated kernel.
 #include <unistd.h>
 
 #include <algorithm>
@@ -54,6 +57,8 @@ struct Args {
   size_t nsys = 4096, nmin = 64, nmax = 4096;
   bool autotune = false;
   int device = 0;
+  size_t save_every = 0;  // -save K: snapshot every K steps (NBody_<N>.dat)
+  std::string resume;     // -resume PATH: start from the file's last record
 };
 
 bool parse(int argc, char** argv, Args& a) {
@@ -109,6 +114,8 @@ bool parse(int argc, char** argv, Args& a) {
     else if (is("-nmin")) a.nmin = std::strtoull(argv[++i], nullptr, 10);
     else if (is("-nmax")) a.nmax = std::strtoull(argv[++i], nullptr, 10);
     else if (is("-device")) a.device = std::atoi(argv[++i]);
+    else if (is("-save")) a.save_every = std::strtoull(argv[++i], nullptr, 10);
+    else if (is("-resume")) a.resume = argv[++i];
   }
   // Validation and resets of CPU/main.cpp:271-288.
   if (a.N >= 100000000 || a.start_N >= 100000000 ||
@@ -195,36 +202,77 @@ bool file_exists(const std::string& p) { return access(p.c_str(), F_OK) != -1; }
 
 int run_gpu(nbr_ctx* ctx, const Args& a, bool bench) {
   State s;
-  if (make_ic(a, a.N, a.ratio, s) != NBR_OK) return 1;
-  State ref = s;
   const double dt = a.dt > 0.0 ? a.dt : a.T / double(a.time_steps);
   const double eps2 = a.eps * a.eps;
+  size_t step0 = 0;
   std::printf("N = %zu, s = %zu\n", a.N, a.time_steps);
-  if (nbr_system_upload(ctx, s.n, s.x.data(), s.y.data(), s.z.data(), s.vx.data(), s.vy.data(),
-                        s.vz.data(), s.m.data()) != NBR_OK) {
-    std::printf("upload failed: %s\n", nbr_last_error_string(ctx));
-    return 1;
+  if (!a.resume.empty()) {
+    size_t records = 0;
+    double t = 0.0;
+    if (nbr_snapshot_records(a.resume.c_str(), a.N, &records) != NBR_OK || records == 0 ||
+        nbr_snapshot_load(ctx, a.resume.c_str(), a.N, records - 1, &t) != NBR_OK) {
+      std::printf("resume failed: %s\n", nbr_last_error_string(ctx));
+      return 1;
+    }
+    step0 = dt > 0.0 ? (size_t)std::llround(t / dt) : 0;
+    std::printf("Resumed from %s, record %zu (t = %f, step %zu)\n", a.resume.c_str(), records - 1, t,
+                step0);
+    s.resize(a.N);
+    nbr_system_download(ctx, s.x.data(), s.y.data(), s.z.data(), s.vx.data(), s.vy.data(),
+                        s.vz.data());
+  } else {
+    if (make_ic(a, a.N, a.ratio, s) != NBR_OK) return 1;
+    if (nbr_system_upload(ctx, s.n, s.x.data(), s.y.data(), s.z.data(), s.vx.data(), s.vy.data(),
+                          s.vz.data(), s.m.data()) != NBR_OK) {
+      std::printf("upload failed: %s\n", nbr_last_error_string(ctx));
+      return 1;
+    }
   }
+  State ref = s;
   if (a.autotune) nbr_autotune(ctx, a.precision, eps2);
   nbr_diag d[2];
   nbr_run_stats st{};
-  int rc;
+  int rc = NBR_OK;
   double evals_per_step = 1.0;
-  auto t0 = std::chrono::steady_clock::now();
+  int scheme = NBR_EULER, use_order = 1;
   if (a.integ == "lf") {
     const int order = a.order < 2 ? 2 : a.order;
     double c[16], dd[16];
     const int lf = nbr_yoshida_coefficients(order, c, dd);
-    const int use_order = lf ? order : 2;
+    use_order = lf ? order : 2;
     if (!lf) std::printf("Order %d not supported! Defaulting to 2nd order\n", order);
     if (a.scheme == NBR_KDK && use_order != 2) {
       std::printf("KDK is second order; using DKD for order %d\n", use_order);
     }
-    const int scheme = use_order == 2 ? a.scheme : NBR_DKD;
+    scheme = use_order == 2 ? a.scheme : NBR_DKD;
     evals_per_step = scheme == NBR_DKD ? double((lf ? lf : 2) - 1) : 1.0;
+  }
+  auto t0 = std::chrono::steady_clock::now();
+  if (a.save_every == 0) {
     rc = nbr_run(ctx, a.precision, scheme, use_order, dt, a.time_steps, a.G, eps2, d, &st);
   } else {
-    rc = nbr_run(ctx, a.precision, NBR_EULER, 1, dt, a.time_steps, a.G, eps2, d, &st);
+    // Chunks of save_every steps and a snapshot record after each.  A fresh
+    // run first writes the initial state as record 0 (truncating the file); a
+    // resumed run appends, its starting state being the record it came from.
+    const std::string snap = "NBody_" + std::to_string(a.N) + ".dat";
+    if (a.resume.empty()) rc = nbr_snapshot_save(ctx, snap.c_str(), 0, dt);
+    size_t done = 0;
+    while (rc == NBR_OK && done < a.time_steps) {
+      const size_t k = std::min(a.save_every, a.time_steps - done);
+      nbr_diag dk[2];
+      nbr_run_stats sk{};
+      rc = nbr_run(ctx, a.precision, scheme, use_order, dt, k, a.G, eps2, dk, &sk);
+      if (rc != NBR_OK) break;
+      if (done == 0) d[0] = dk[0];
+      d[1] = dk[1];
+      st.gpu_ms += sk.gpu_ms;
+      st.force_evals += sk.force_evals;
+      st.pairs += sk.pairs;
+      st.kernels += sk.kernels;
+      done += k;
+      rc = nbr_snapshot_save(ctx, snap.c_str(), step0 + done, dt);
+    }
+    if (rc == NBR_OK) std::printf("Snapshots written to %s\n", snap.c_str());
   }
   auto t1 = std::chrono::steady_clock::now();
   if (rc != NBR_OK) {

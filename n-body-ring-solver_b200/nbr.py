@@ -22,7 +22,7 @@ LIB_PATH = os.path.join(HERE, "libnbr.so")
 NBR_OK = 0
 STATUS = {0: "NBR_OK", 1: "NBR_ERR_INVALID_ARG", 2: "NBR_ERR_CUDA", 3: "NBR_ERR_NO_MEMORY",
           4: "NBR_ERR_TIMEOUT", 5: "NBR_ERR_NO_SYSTEM", 6: "NBR_ERR_UNSUPPORTED",
-          7: "NBR_ERR_NONFINITE"}
+          7: "NBR_ERR_NONFINITE", 8: "NBR_ERR_IO"}
 FP64, FP32C = 0, 1
 KDK, DKD, EULER = 0, 1, 2
 KEYS = ("x", "y", "z", "vx", "vy", "vz", "m")
@@ -104,6 +104,11 @@ def load(path: str = LIB_PATH) -> C.CDLL:
                             C.c_double], C.c_int),
         "nbr_state_pointers": ([C.c_void_p] + [C.POINTER(C.c_void_p)] * 6 + [C.POINTER(_SZ)], C.c_int),
         "nbr_state_changed": ([C.c_void_p], C.c_int),
+        "nbr_snapshot_write_arrays": ([C.c_char_p, _SZ, _SZ, C.c_double] + [_D] * 10, C.c_int),
+        "nbr_snapshot_save": ([C.c_void_p, C.c_char_p, _SZ, C.c_double], C.c_int),
+        "nbr_snapshot_records": ([C.c_char_p, _SZ, C.POINTER(_SZ)], C.c_int),
+        "nbr_snapshot_read_arrays": ([C.c_char_p, _SZ, _SZ, _D] + [_D] * 10, C.c_int),
+        "nbr_snapshot_load": ([C.c_void_p, C.c_char_p, _SZ, _SZ, _D], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -135,6 +140,39 @@ def yoshida(order: int):
     if k == 0:
         raise ValueError(f"order {order} unsupported")
     return c[:k].copy(), d[:k - 1].copy()
+
+
+# ----------------------------------------------------------------- snapshots --
+SNAP_FIELDS = ("m", "x", "y", "z", "vx", "vy", "vz", "fx", "fy", "fz")
+
+
+def snapshot_write(path: str, s: Dict[str, np.ndarray], time_step: int, delta_t: float,
+                   forces: Optional[np.ndarray] = None):
+    """One record in the reference's save_particles format (host arrays)."""
+    n = len(s["x"])
+    arr = {k: _f64(s[k]) for k in ("m", "x", "y", "z")}
+    for k in ("vx", "vy", "vz"):
+        arr[k] = _f64(s[k]) if s.get(k) is not None else None
+    for d, k in enumerate(("fx", "fy", "fz")):
+        arr[k] = _f64(forces[d]) if forces is not None else None
+    _check(load().nbr_snapshot_write_arrays(str(path).encode(), n, time_step, delta_t,
+                                            *[_p(arr[k]) for k in SNAP_FIELDS]), "snapshot_write")
+
+
+def snapshot_records(path: str, n: int) -> int:
+    out = _SZ()
+    _check(load().nbr_snapshot_records(str(path).encode(), n, C.byref(out)), "snapshot_records")
+    return int(out.value)
+
+
+def snapshot_read(path: str, n: int, record: int) -> Dict[str, np.ndarray]:
+    """Record `record` as a dict with t and the ten fields."""
+    out = {k: np.zeros(n) for k in SNAP_FIELDS}
+    t = C.c_double()
+    _check(load().nbr_snapshot_read_arrays(str(path).encode(), n, record, C.byref(t),
+                                           *[_p(out[k]) for k in SNAP_FIELDS]), "snapshot_read")
+    out["t"] = t.value
+    return out
 
 
 # ------------------------------------------------------------------ samplers --
@@ -360,6 +398,17 @@ class Context:
 
     def state_changed(self):
         self._chk(self.L.nbr_state_changed(self.h), "state_changed")
+
+    def snapshot_save(self, path, time_step, delta_t):
+        self._chk(self.L.nbr_snapshot_save(self.h, str(path).encode(), time_step, delta_t),
+                  "snapshot_save")
+
+    def snapshot_load(self, path, n, record):
+        t = C.c_double()
+        self._chk(self.L.nbr_snapshot_load(self.h, str(path).encode(), n, record, C.byref(t)),
+                  "snapshot_load")
+        self.n = n
+        return t.value
 
     def set_force_config(self, precision, ni=0, warps=0, split=0):
         self._chk(self.L.nbr_set_force_config(self.h, precision, ni, warps, split), "set_force_config")

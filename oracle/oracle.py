@@ -168,6 +168,8 @@ class Reference:
         L.ref_ring_predict.restype = C.c_int
         L.ref_yoshida.argtypes = [C.c_int, _D, _D]
         L.ref_yoshida.restype = C.c_int
+        L.ref_save_snapshot.argtypes = [C.c_char_p, _SZ] + [_D] * 10 + [_SZ, C.c_double]
+        L.ref_save_snapshot.restype = C.c_int
 
     @property
     def has_avx512(self) -> bool:
@@ -224,6 +226,17 @@ class Reference:
         arrs = [np.zeros(n) for _ in range(6)]
         self.lib.ref_ring_predict(n, R, omega, step, steps_per_rev, *[_p(a) for a in arrs])
         return dict(zip(("x", "y", "z", "vx", "vy", "vz"), arrs))
+
+    def save_snapshot(self, directory, s, f, records, delta_t):
+        """Writes `records` records of state s (forces f, (3, n)) with the
+        reference's save_particles into directory/NBody_<n>.dat; returns the path."""
+        n = len(s["x"])
+        arr = [np.ascontiguousarray(a, dtype=np.float64) for a in
+               (s["m"], s["x"], s["y"], s["z"], s["vx"], s["vy"], s["vz"], f[0], f[1], f[2])]
+        rc = self.lib.ref_save_snapshot(str(directory).encode(), n, *[_p(a) for a in arr], records, delta_t)
+        if rc != 0:
+            raise OSError(f"ref_save_snapshot failed in {directory}")
+        return os.path.join(str(directory), f"NBody_{n}.dat")
 
     def yoshida(self, order):
         c = np.zeros(16); d = np.zeros(16)

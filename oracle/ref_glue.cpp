@@ -296,4 +296,25 @@ int ref_ring_predict(size_t n, double R, double omega, size_t step, size_t steps
 
 int ref_yoshida(int order, double* c, double* d) { return int(yoshida(order, c, d)); }
 
+// `records` snapshot records of one state through NBody_system::save_particles
+// (CPU/nbody_system.cpp:133-152), time steps 0 .. records-1: the reference
+// writes "NBody_<n>.dat" in the working directory, so the call runs with
+// `dir` as the working directory.  Returns 0, or -1 if dir is unusable.
+int ref_save_snapshot(const char* dir, size_t n, const double* m, const double* x, const double* y,
+                      const double* z, const double* vx, const double* vy, const double* vz,
+                      const double* fx, const double* fy, const double* fz, size_t records,
+                      double delta_t) {
+  char old[4096];
+  if (!getcwd(old, sizeof(old)) || chdir(dir) != 0) return -1;
+  {
+    NBody_system s;
+    load(s, n, x, y, z, vx, vy, vz, m);
+    for (size_t i = 0; i < n; ++i) {
+      s.force[X][i] = fx[i]; s.force[Y][i] = fy[i]; s.force[Z][i] = fz[i];
+    }
+    for (size_t t = 0; t < records; ++t) s.save_particles(t, delta_t);
+  }  // the destructor closes (flushes) the file
+  return chdir(old) == 0 ? 0 : -1;
+}
+
 }  // extern "C"
