@@ -319,6 +319,19 @@ int nbr_batch_forces(nbr_ctx* ctx, int precision, double G, double eps2, int wan
  * step loop captured in one CUDA graph. */
 int nbr_batch_run(nbr_ctx* ctx, int precision, double dt, size_t steps, double G, double eps2,
                   nbr_run_stats* stats);
+/* Forces the batched kernel's configuration for a precision: wide = 1 pairs a
+ * system's receiver tiles into two-tile work items (8 receivers per lane),
+ * wide = 0 keeps one-tile items (4 per lane); ctas_per_sm = resident CTAs per
+ * SM of the persistent grid (0: the occupancy limit).  wide = -1 restores the
+ * autotune cache or the default (occupancy limit; two-tile items for FP32C,
+ * one-tile items for FP64).  Applies to
+ * the uploaded batch; an upload starts from the autotune cache again. */
+int nbr_batch_set_config(nbr_ctx* ctx, int precision, int wide, int ctas_per_sm);
+/* Times every (item width, CTAs per SM) on the uploaded batch and stores the
+ * fastest in the autotune cache under the batch's (precision, log2 system
+ * count, log2 largest system, eps == 0) bucket; later uploads of a batch in
+ * the same bucket use it. */
+int nbr_batch_autotune(nbr_ctx* ctx, int precision, double eps2);
 /* Per-system diagnostics (out has nsys entries). */
 int nbr_batch_diagnostics(nbr_ctx* ctx, double G, double eps2, nbr_diag* out);
 

@@ -9,6 +9,11 @@
 // streams its system's source tiles through its own 3-stage shared-memory ring
 // (1-D bulk copies, one mbarrier per stage, lane 0 produces).
 //
+// Wide items: a system's receiver tiles can be paired into two-tile items
+// (256 receivers, 8 per lane): every source read from shared memory then
+// feeds 8 receivers and each lane runs four independent f32x2 chains.  A
+// system's odd last tile stays a one-tile item.
+//
 // Small items: when an item has R <= 64 real receivers (a system of <= 64
 // particles, or the last tile of a system), the warp splits into F = 2, 4 or
 // 8 lane groups that take every F-th source; the partial sums are combined
@@ -41,6 +46,7 @@ constexpr int kRec32 = kTile * 48;            // FP32C records of one tile
 constexpr int kStageB32 = kRec32 + 32;        // + origin
 constexpr int kStageB64 = 4 * kTile * 8;      // FP64 x, y, z, m
 constexpr int kBHead = 128;                   // barriers: kBWarps * kBStages * 8 <= 128
+constexpr int kWideItem = 1 << 30;            // item flag: two receiver tiles
 
 struct BatchParams {
   const double* x; const double* y; const double* z; const double* m;  // current buffer
@@ -72,17 +78,17 @@ struct Stage<kFP64> {
   static constexpr int bytes = kStageB64;
 };
 
-// One source tile of FP32C records against the lane's 2 receiver pairs.
+// One source tile of FP32C records against the lane's NP receiver pairs.
 // Sources j = j0, j0 + step, ... < jend.
-template <bool EXCL, bool FULL>
+template <bool EXCL, bool FULL, int NP>
 __device__ __forceinline__ void tile_f32c(const unsigned char* base, int j0, int step, int jend,
                                           const double* xi, const double* yi, const double* zi,
                                           u64 EPS2, u64* hx, u64* hy, u64* hz, u64* lx, u64* ly,
                                           u64* lz) {
   const double4 o = *reinterpret_cast<const double4*>(base + kRec32);
-  u64 XI[2], YI[2], ZI[2], AX[2], AY[2], AZ[2];
+  u64 XI[NP], YI[NP], ZI[NP], AX[NP], AY[NP], AZ[NP];
 #pragma unroll
-  for (int p = 0; p < 2; ++p) {
+  for (int p = 0; p < NP; ++p) {
     XI[p] = pack2(__double2float_rn(xi[2 * p] - o.x), __double2float_rn(xi[2 * p + 1] - o.x));
     YI[p] = pack2(__double2float_rn(yi[2 * p] - o.y), __double2float_rn(yi[2 * p + 1] - o.y));
     ZI[p] = pack2(__double2float_rn(zi[2 * p] - o.z), __double2float_rn(zi[2 * p + 1] - o.z));
@@ -94,7 +100,7 @@ __device__ __forceinline__ void tile_f32c(const unsigned char* base, int j0, int
     const ulonglong2 q1 = R[3 * j + 1];
     const u64 bj = R[3 * j + 2].x;
 #pragma unroll
-    for (int p = 0; p < 2; ++p) {
+    for (int p = 0; p < NP; ++p) {
       const u64 dx = sub2(q0.x, XI[p]);
       const u64 dy = sub2(q0.y, YI[p]);
       const u64 dz = sub2(q1.x, ZI[p]);
@@ -127,14 +133,15 @@ __device__ __forceinline__ void tile_f32c(const unsigned char* base, int j0, int
     for (int j = j0; j < jend; j += step) pair(j);
   }
 #pragma unroll
-  for (int p = 0; p < 2; ++p) {
+  for (int p = 0; p < NP; ++p) {
     two_sum2(hx[p], lx[p], AX[p]);
     two_sum2(hy[p], ly[p], AY[p]);
     two_sum2(hz[p], lz[p], AZ[p]);
   }
 }
 
-template <bool EXCL, bool FULL>
+// One FP64 source tile against the lane's NR receivers.
+template <bool EXCL, bool FULL, int NR>
 __device__ __forceinline__ void tile_f64(const unsigned char* base, int j0, int step, int jend,
                                          const double* xi, const double* yi, const double* zi,
                                          double eps2, double* ax, double* ay, double* az) {
@@ -145,7 +152,7 @@ __device__ __forceinline__ void tile_f64(const unsigned char* base, int j0, int 
   auto pair = [&](int j) {
     const double xj = sx[j], yj = sy[j], zj = sz[j], mj = sm[j];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < NR; ++k) {
       const double dx = xj - xi[k], dy = yj - yi[k], dz = zj - zi[k];
       double r2 = fma(dx, dx, eps2);
       r2 = fma(dy, dy, r2);
@@ -167,166 +174,166 @@ __device__ __forceinline__ void tile_f64(const unsigned char* base, int j0, int 
   }
 }
 
-template <int PREC, bool EXCL>
-__global__ void __launch_bounds__(kBWarps * 32) k_batch_force(const BatchParams p, const double eps2) {
+// The per-warp state that persists across items: the tile ring.
+struct Ring {
+  uint64_t* bars;
+  unsigned char* stages;
+  unsigned tcount;  // tiles this warp has consumed (ring position)
+};
+
+// One work item: NR / 4 receiver tiles (4 receivers per lane per tile)
+// starting at global tile `tile0` of system `s`, against all of the system's
+// source tiles.  Narrow items (NR = 4) split the warp into lane groups when
+// they hold <= 64 real receivers.  Returns false if a tile wait gave up.
+template <int PREC, bool EXCL, int NR>
+__device__ __forceinline__ bool run_item(const BatchParams& p, double eps2, u64 EPS2, Ring& ring,
+                                         int lane, int s, int tile0) {
   constexpr int SB = Stage<PREC>::bytes;
-  extern __shared__ __align__(128) unsigned char smem[];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem) + warp * kBStages;
-  unsigned char* stages = smem + kBHead + (size_t)warp * kBStages * SB;
-  if (lane == 0) {
-    for (int st = 0; st < kBStages; ++st) mbar_init(smem_u32(&bars[st]), 1);
-    mbar_fence_init();
+  constexpr int NP = NR / 2;
+  const long long poff = p.poff[s];
+  const int ns = p.nreal[s];
+  const long long rbase = (long long)tile0 * kTile;             // first receiver (padded index)
+  const int rfirst = (int)(rbase - poff);                       // its index inside the system
+  const int R = min(32 * NR, ns - rfirst);                      // real receivers in this item
+  const int F = NR > 4 ? 1 : R > 64 ? 1 : R > 32 ? 2 : R > 16 ? 4 : 8;  // lane groups
+  const int G = 32 / F;
+  const int gl = lane % G, phase = lane / G;
+  const int t_first = (int)(poff / kTile);
+  const int ntl = (ns + kTile - 1) / kTile;
+  const int last_cnt = ((ns - (ntl - 1) * kTile) + 3) & ~3;  // real sources of the last tile, to 4
+
+  double xi[NR], yi[NR], zi[NR];
+#pragma unroll
+  for (int k = 0; k < NR; ++k) {
+    const long long i = rbase + gl + G * k;  // inside the item's tiles for every F
+    xi[k] = p.x[i]; yi[k] = p.y[i]; zi[k] = p.z[i];
   }
-  __syncwarp();
-  const float e2f = (float)eps2;
-  const u64 EPS2 = pack2(e2f, e2f);
-  unsigned tcount = 0;  // tiles this warp has consumed (ring position)
-
-  while (true) {
-    int item = 0;
-    if (lane == 0) item = (int)atomicAdd(p.head, 1u);
-    item = __shfl_sync(0xffffffffu, item, 0);
-    if (item >= p.n_items) break;
-    const int2 it = p.items[item];
-    const int s = it.x;
-    const long long poff = p.poff[s];
-    const int ns = p.nreal[s];
-    const long long rbase = (long long)it.y * kTile;          // first receiver (padded index)
-    const int rfirst = (int)(rbase - poff);                      // its index inside the system
-    const int R = min(kTile, ns - rfirst);                       // real receivers in this item
-    const int F = R > 64 ? 1 : R > 32 ? 2 : R > 16 ? 4 : 8;      // lane groups
-    const int G = 32 / F;
-    const int gl = lane % G, phase = lane / G;
-    const int t_first = (int)(poff / kTile);
-    const int ntl = (ns + kTile - 1) / kTile;
-    const int last_cnt = ((ns - (ntl - 1) * kTile) + 3) & ~3;  // real sources of the last tile, to 4
-
-    double xi[4], yi[4], zi[4];
+  u64 hx[NP], hy[NP], hz[NP], lx[NP], ly[NP], lz[NP];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const long long i = rbase + gl + G * k;  // inside the item's tile for every F
-      xi[k] = p.x[i]; yi[k] = p.y[i]; zi[k] = p.z[i];
-    }
-    u64 hx[2] = {0, 0}, hy[2] = {0, 0}, hz[2] = {0, 0}, lx[2] = {0, 0}, ly[2] = {0, 0}, lz[2] = {0, 0};
-    double ax[4] = {0, 0, 0, 0}, ay[4] = {0, 0, 0, 0}, az[4] = {0, 0, 0, 0};
+  for (int q = 0; q < NP; ++q) hx[q] = hy[q] = hz[q] = lx[q] = ly[q] = lz[q] = 0ull;
+  double ax[NR], ay[NR], az[NR];
+#pragma unroll
+  for (int k = 0; k < NR; ++k) ax[k] = ay[k] = az[k] = 0.0;
 
-    uint32_t pending = 0;
-    auto issue = [&](int t) {  // lane 0 only
-      if (t == p.skip_tile) return;
-      const unsigned pos = tcount + t;
-      const int st = pos % kBStages;
-      unsigned char* dst = stages + st * SB;
-      const uint32_t bar = smem_u32(&bars[st]);
-      const size_t tile = (size_t)(t_first + t);
-      if (PREC == kFP32C) {
-        mbar_expect_tx(bar, kStageB32);
-        bulk_g2s(dst, p.rec + tile * kTile * 3, kRec32, bar);
-        bulk_g2s(dst + kRec32, p.org + tile, 32, bar);
-      } else {
-        mbar_expect_tx(bar, kStageB64);
-        const size_t off = tile * kTile;
-        bulk_g2s(dst, p.x + off, kTile * 8, bar);
-        bulk_g2s(dst + kTile * 8, p.y + off, kTile * 8, bar);
-        bulk_g2s(dst + 2 * kTile * 8, p.z + off, kTile * 8, bar);
-        bulk_g2s(dst + 3 * kTile * 8, p.m + off, kTile * 8, bar);
-      }
-      pending |= 1u << st;
-    };
-    if (lane == 0)
-      for (int t = 0; t < kBStages && t < ntl; ++t) issue(t);
-    bool aborted = false;
-    int t = 0;
-    for (; t < ntl; ++t) {
-      const unsigned pos = tcount + t;
-      const int st = pos % kBStages;
-      const bool ok = mbar_wait_bounded(smem_u32(&bars[st]), (pos / kBStages) & 1u, p.wait_ns);
-      const unsigned char* base = stages + st * SB;
-      const int jend = (t == ntl - 1) ? last_cnt : kTile;
-      const bool full = (F == 1) && (jend == kTile);
-      if (PREC == kFP32C) {
-        if (full) tile_f32c<EXCL, true>(base, 0, 1, kTile, xi, yi, zi, EPS2, hx, hy, hz, lx, ly, lz);
-        else tile_f32c<EXCL, false>(base, phase, F, jend, xi, yi, zi, EPS2, hx, hy, hz, lx, ly, lz);
-      } else {
-        if (full) tile_f64<EXCL, true>(base, 0, 1, kTile, xi, yi, zi, eps2, ax, ay, az);
-        else tile_f64<EXCL, false>(base, phase, F, jend, xi, yi, zi, eps2, ax, ay, az);
-      }
-      __syncwarp();
-      if (__any_sync(0xffffffffu, !ok)) {
-        aborted = true;
-        break;
-      }
-      if (lane == 0) {
-        pending &= ~(1u << st);
-        if (t + kBStages < ntl) issue(t + kBStages);
-      }
-    }
-    if (aborted) {
-      if (lane == 0) {
-        record_error(p.err, kErrTileWait);
-        for (int u = t; u < ntl && u < t + kBStages; ++u) {
-          const unsigned pos = tcount + u;
-          const int st = pos % kBStages;
-          if (!(pending & (1u << st))) continue;
-          if (!mbar_wait_bounded(smem_u32(&bars[st]), (pos / kBStages) & 1u, p.wait_ns)) {
-            record_error(p.err, kErrDrainWait);
-            break;
-          }
-        }
-      }
-      return;  // this warp takes no more items; the host reports the error
-    }
-    tcount += ntl;
-
+  uint32_t pending = 0;
+  auto issue = [&](int t) {  // lane 0 only
+    if (t == p.skip_tile) return;
+    const unsigned pos = ring.tcount + t;
+    const int st = pos % kBStages;
+    unsigned char* dst = ring.stages + st * SB;
+    const uint32_t bar = smem_u32(&ring.bars[st]);
+    const size_t tile = (size_t)(t_first + t);
     if (PREC == kFP32C) {
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        float h0, h1, l0, l1;
-        unpack2(hx[q], h0, h1); unpack2(lx[q], l0, l1);
-        ax[2 * q] = (double)h0 + (double)l0; ax[2 * q + 1] = (double)h1 + (double)l1;
-        unpack2(hy[q], h0, h1); unpack2(ly[q], l0, l1);
-        ay[2 * q] = (double)h0 + (double)l0; ay[2 * q + 1] = (double)h1 + (double)l1;
-        unpack2(hz[q], h0, h1); unpack2(lz[q], l0, l1);
-        az[2 * q] = (double)h0 + (double)l0; az[2 * q + 1] = (double)h1 + (double)l1;
-      }
+      mbar_expect_tx(bar, kStageB32);
+      bulk_g2s(dst, p.rec + tile * kTile * 3, kRec32, bar);
+      bulk_g2s(dst + kRec32, p.org + tile, 32, bar);
+    } else {
+      mbar_expect_tx(bar, kStageB64);
+      const size_t off = tile * kTile;
+      bulk_g2s(dst, p.x + off, kTile * 8, bar);
+      bulk_g2s(dst + kTile * 8, p.y + off, kTile * 8, bar);
+      bulk_g2s(dst + 2 * kTile * 8, p.z + off, kTile * 8, bar);
+      bulk_g2s(dst + 3 * kTile * 8, p.m + off, kTile * 8, bar);
     }
-    // Combine the lane groups' partial sums (fixed xor order: deterministic).
-    for (int off = G; off < 32; off <<= 1) {
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        ax[k] += __shfl_xor_sync(0xffffffffu, ax[k], off);
-        ay[k] += __shfl_xor_sync(0xffffffffu, ay[k], off);
-        az[k] += __shfl_xor_sync(0xffffffffu, az[k], off);
-      }
+    pending |= 1u << st;
+  };
+  if (lane == 0)
+    for (int t = 0; t < kBStages && t < ntl; ++t) issue(t);
+  bool aborted = false;
+  int t = 0;
+  for (; t < ntl; ++t) {
+    const unsigned pos = ring.tcount + t;
+    const int st = pos % kBStages;
+    const bool ok = mbar_wait_bounded(smem_u32(&ring.bars[st]), (pos / kBStages) & 1u, p.wait_ns);
+    const unsigned char* base = ring.stages + st * SB;
+    const int jend = (t == ntl - 1) ? last_cnt : kTile;
+    const bool full = (F == 1) && (jend == kTile);
+    if (PREC == kFP32C) {
+      if (full) tile_f32c<EXCL, true, NP>(base, 0, 1, kTile, xi, yi, zi, EPS2, hx, hy, hz, lx, ly, lz);
+      else tile_f32c<EXCL, false, NP>(base, phase, F, jend, xi, yi, zi, EPS2, hx, hy, hz, lx, ly, lz);
+    } else {
+      if (full) tile_f64<EXCL, true, NR>(base, 0, 1, kTile, xi, yi, zi, eps2, ax, ay, az);
+      else tile_f64<EXCL, false, NR>(base, phase, F, jend, xi, yi, zi, eps2, ax, ay, az);
     }
-    // Epilogue: lane group 0 owns receivers gl + G k of the item.
-    if (phase == 0) {
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const int loc = gl + G * k;
-        if (loc >= R) continue;
-        const long long i = rbase + loc;
-        const double gx = p.G * ax[k], gy = p.G * ay[k], gz = p.G * az[k];
-        p.ax[i] = gx; p.ay[i] = gy; p.az[i] = gz;
-        if (p.mode == 1) {
-          const double vx = p.vx[i] + p.kick * gx;
-          const double vy = p.vy[i] + p.kick * gy;
-          const double vz = p.vz[i] + p.kick * gz;
-          p.vx[i] = vx; p.vy[i] = vy; p.vz[i] = vz;
-          p.xn[i] = xi[k] + p.drift * vx;
-          p.yn[i] = yi[k] + p.drift * vy;
-          p.zn[i] = zi[k] + p.drift * vz;
+    __syncwarp();
+    if (__any_sync(0xffffffffu, !ok)) {
+      aborted = true;
+      break;
+    }
+    if (lane == 0) {
+      pending &= ~(1u << st);
+      if (t + kBStages < ntl) issue(t + kBStages);
+    }
+  }
+  if (aborted) {
+    if (lane == 0) {
+      record_error(p.err, kErrTileWait);
+      for (int u = t; u < ntl && u < t + kBStages; ++u) {
+        const unsigned pos = ring.tcount + u;
+        const int st = pos % kBStages;
+        if (!(pending & (1u << st))) continue;
+        if (!mbar_wait_bounded(smem_u32(&ring.bars[st]), (pos / kBStages) & 1u, p.wait_ns)) {
+          record_error(p.err, kErrDrainWait);
+          break;
         }
       }
     }
-    if (p.mode == 1 && p.rec_next) {
-      // Pack the item's tile of the new positions (natural layout lane + 32k).
-      __syncwarp();
+    return false;  // this warp takes no more items; the host reports the error
+  }
+  ring.tcount += ntl;
+
+  if (PREC == kFP32C) {
+#pragma unroll
+    for (int q = 0; q < NP; ++q) {
+      float h0, h1, l0, l1;
+      unpack2(hx[q], h0, h1); unpack2(lx[q], l0, l1);
+      ax[2 * q] = (double)h0 + (double)l0; ax[2 * q + 1] = (double)h1 + (double)l1;
+      unpack2(hy[q], h0, h1); unpack2(ly[q], l0, l1);
+      ay[2 * q] = (double)h0 + (double)l0; ay[2 * q + 1] = (double)h1 + (double)l1;
+      unpack2(hz[q], h0, h1); unpack2(lz[q], l0, l1);
+      az[2 * q] = (double)h0 + (double)l0; az[2 * q + 1] = (double)h1 + (double)l1;
+    }
+  }
+  // Combine the lane groups' partial sums (fixed xor order: deterministic).
+  for (int off = G; off < 32; off <<= 1) {
+#pragma unroll
+    for (int k = 0; k < NR; ++k) {
+      ax[k] += __shfl_xor_sync(0xffffffffu, ax[k], off);
+      ay[k] += __shfl_xor_sync(0xffffffffu, ay[k], off);
+      az[k] += __shfl_xor_sync(0xffffffffu, az[k], off);
+    }
+  }
+  // Epilogue: lane group 0 owns receivers gl + G k of the item.
+  if (phase == 0) {
+#pragma unroll
+    for (int k = 0; k < NR; ++k) {
+      const int loc = gl + G * k;
+      if (loc >= R) continue;
+      const long long i = rbase + loc;
+      const double gx = p.G * ax[k], gy = p.G * ay[k], gz = p.G * az[k];
+      p.ax[i] = gx; p.ay[i] = gy; p.az[i] = gz;
+      if (p.mode == 1) {
+        const double vx = p.vx[i] + p.kick * gx;
+        const double vy = p.vy[i] + p.kick * gy;
+        const double vz = p.vz[i] + p.kick * gz;
+        p.vx[i] = vx; p.vy[i] = vy; p.vz[i] = vz;
+        p.xn[i] = xi[k] + p.drift * vx;
+        p.yn[i] = yi[k] + p.drift * vy;
+        p.zn[i] = zi[k] + p.drift * vz;
+      }
+    }
+  }
+  if (p.mode == 1 && p.rec_next) {
+    // Pack each of the item's tiles of the new positions (layout lane + 32k);
+    // every tile of an item holds at least one real receiver.
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < NR / 4; ++q) {
       double px[4], py[4], pz[4];
       double sx = 0.0, sy = 0.0, sz = 0.0, cnt = 0.0;
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        const int loc = lane + 32 * k;
+        const int loc = kTile * q + lane + 32 * k;
         const long long i = rbase + loc;
         px[k] = py[k] = pz[k] = 0.0;
         if (loc < R) {
@@ -341,11 +348,11 @@ __global__ void __launch_bounds__(kBWarps * 32) k_batch_force(const BatchParams 
         sz += __shfl_xor_sync(0xffffffffu, sz, off);
         cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
       }
-      const double ox = sx / cnt, oy = sy / cnt, oz = sz / cnt;  // R >= 1
-      if (lane == 0) p.org_next[it.y] = make_double4(ox, oy, oz, 0.0);
+      const double ox = sx / cnt, oy = sy / cnt, oz = sz / cnt;  // cnt >= 1
+      if (lane == 0) p.org_next[tile0 + q] = make_double4(ox, oy, oz, 0.0);
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        const int loc = lane + 32 * k;
+        const int loc = kTile * q + lane + 32 * k;
         const long long i = rbase + loc;
         float fx = 0.f, fy = 0.f, fz = 0.f, fa = 0.f, fb = 0.f;
         if (loc < R) {
@@ -360,7 +367,41 @@ __global__ void __launch_bounds__(kBWarps * 32) k_batch_force(const BatchParams 
         p.rec_next[3 * i + 2] = make_float4(fb, fb, 0.f, 0.f);
       }
     }
-    __syncwarp();
+  }
+  __syncwarp();
+  return true;
+}
+
+// The persistent kernel.  WIDE = false: every item is narrow (4 receivers per
+// lane); WIDE = true: items flagged kWideItem cover two tiles (8 receivers per
+// lane: twice the pair work per source read, four independent f32x2 chains).
+template <int PREC, bool EXCL, bool WIDE>
+__global__ void __launch_bounds__(kBWarps * 32) k_batch_force(const BatchParams p, const double eps2) {
+  constexpr int SB = Stage<PREC>::bytes;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  Ring ring;
+  ring.bars = reinterpret_cast<uint64_t*>(smem) + warp * kBStages;
+  ring.stages = smem + kBHead + (size_t)warp * kBStages * SB;
+  ring.tcount = 0;
+  if (lane == 0) {
+    for (int st = 0; st < kBStages; ++st) mbar_init(smem_u32(&ring.bars[st]), 1);
+    mbar_fence_init();
+  }
+  __syncwarp();
+  const float e2f = (float)eps2;
+  const u64 EPS2 = pack2(e2f, e2f);
+  while (true) {
+    int item = 0;
+    if (lane == 0) item = (int)atomicAdd(p.head, 1u);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    if (item >= p.n_items) break;
+    const int2 it = p.items[item];
+    const int s = it.x & ~kWideItem;
+    bool ok;
+    if (WIDE && (it.x & kWideItem)) ok = run_item<PREC, EXCL, 8>(p, eps2, EPS2, ring, lane, s, it.y);
+    else ok = run_item<PREC, EXCL, 4>(p, eps2, EPS2, ring, lane, s, it.y);
+    if (!ok) return;
   }
 }
 
@@ -422,38 +463,83 @@ __global__ void __launch_bounds__(256)
     for (int c = 0; c < 9; ++c) out[(size_t)s * 9 + c] = red[c][0];
 }
 
-template <int PREC, bool EXCL>
-cudaError_t launch_batch_t(const BatchParams& p, double eps2, int grid, cudaStream_t st) {
-  const size_t smem = kBHead + (size_t)kBWarps * kBStages * Stage<PREC>::bytes;
-  k_batch_force<PREC, EXCL><<<grid, kBWarps * 32, smem, st>>>(p, eps2);
-  return cudaGetLastError();
+template <int PREC, bool EXCL, bool WIDE>
+const void* batch_fn() {
+  return (const void*)k_batch_force<PREC, EXCL, WIDE>;
 }
 
-cudaError_t launch_batch(int prec, const BatchParams& p, double eps2, int grid, cudaStream_t st) {
-  const bool ex = eps2 == 0.0;
-  if (prec == kFP32C)
-    return ex ? launch_batch_t<kFP32C, true>(p, eps2, grid, st) : launch_batch_t<kFP32C, false>(p, eps2, grid, st);
-  return ex ? launch_batch_t<kFP64, true>(p, eps2, grid, st) : launch_batch_t<kFP64, false>(p, eps2, grid, st);
+const void* batch_kernel(int prec, bool excl, bool wide) {
+  if (prec == kFP32C) {
+    if (excl) return wide ? batch_fn<kFP32C, true, true>() : batch_fn<kFP32C, true, false>();
+    return wide ? batch_fn<kFP32C, false, true>() : batch_fn<kFP32C, false, false>();
+  }
+  if (excl) return wide ? batch_fn<kFP64, true, true>() : batch_fn<kFP64, true, false>();
+  return wide ? batch_fn<kFP64, false, true>() : batch_fn<kFP64, false, false>();
 }
 
-// Sets the kernel's shared-memory attribute and returns the persistent grid
-// (resident CTAs per SM x SMs).  Called outside stream capture; cached.
+size_t batch_smem(int prec) {
+  return kBHead + (size_t)kBWarps * kBStages * (prec == kFP32C ? kStageB32 : kStageB64);
+}
+
+cudaError_t launch_batch(int prec, bool wide, const BatchParams& p, double eps2, int grid,
+                         cudaStream_t st) {
+  const void* fn = batch_kernel(prec, eps2 == 0.0, wide);
+  const size_t smem = batch_smem(prec);
+  void* args[] = {(void*)&p, (void*)&eps2};
+  return cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(kBWarps * 32), args, smem, st);
+}
+
+// Autotune-cache key of a batch: precision, log2 of the system count and of
+// the largest system, eps == 0.
+std::string batch_key(int prec, size_t nsys, int max_ns, bool excl) {
+  int sb = 0, nb = 0;
+  while (((size_t)1 << (sb + 1)) <= nsys) ++sb;
+  while ((1 << (nb + 1)) <= max_ns) ++nb;
+  return std::string("batch:") + (prec == kFP32C ? "fp32c" : "fp64") + ":s" + std::to_string(sb) +
+         ":n" + std::to_string(nb) + (excl ? ":e0" : "");
+}
+
+// The kernel configuration of the batch for a precision: from the autotune
+// cache when it holds this batch's key, else the default (occupancy-limited
+// grid; two-tile items for FP32C, one-tile items for FP64).
+void batch_config(nbr_ctx* c, int prec, double eps2) {
+  BatchState& b = c->bat;
+  const int pi = prec == kFP32C ? 1 : 0;
+  if (b.cfg_ok[pi]) return;
+  ForceConfig t{0, 0, 0};
+  if (tune_get(batch_key(prec, b.nsys, b.max_ns, eps2 == 0.0), &t) && (t.ni == 4 || t.ni == 8)) {
+    b.wide[pi] = t.ni == 8 ? 1 : 0;
+    b.per_sm[pi] = t.split;
+  } else {
+    // Defaults from the 4096-system workload on B200: two-tile items lift
+    // FP32C from 1868 to 2029 GPairs/s; FP64 (twice the registers per
+    // receiver) is faster with one-tile items (834 vs 784).
+    b.wide[pi] = prec == kFP32C ? 1 : 0;
+    b.per_sm[pi] = 0;
+  }
+  b.cfg_ok[pi] = true;
+}
+
+// Sets the kernel's shared-memory attribute (once per kernel variant) and
+// returns the persistent grid: resident CTAs per SM (the configured count,
+// at most the occupancy limit) x SMs.  Called before any stream capture.
 int batch_grid(nbr_ctx* c, int prec, double eps2) {
-  int& cached = c->bat.grid[prec == kFP32C ? 1 : 0][eps2 == 0.0 ? 1 : 0];
-  if (cached > 0) return cached;
-  const int sms = c->sms;
-  const size_t smem = kBHead + (size_t)kBWarps * kBStages * (prec == kFP32C ? kStageB32 : kStageB64);
-  const void* fn = prec == kFP32C ? (eps2 == 0.0 ? (const void*)k_batch_force<kFP32C, true>
-                                                 : (const void*)k_batch_force<kFP32C, false>)
-                                  : (eps2 == 0.0 ? (const void*)k_batch_force<kFP64, true>
-                                                 : (const void*)k_batch_force<kFP64, false>);
-  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  int per = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, kBWarps * 32, smem) != cudaSuccess ||
-      per < 1)
-    per = 1;
-  cached = per * sms;
-  return cached;
+  BatchState& b = c->bat;
+  batch_config(c, prec, eps2);
+  const int pi = prec == kFP32C ? 1 : 0, ei = eps2 == 0.0 ? 1 : 0, wi = b.wide[pi];
+  int& occ = b.occ[pi][ei][wi];
+  if (occ == 0) {
+    const void* fn = batch_kernel(prec, eps2 == 0.0, wi == 1);
+    const size_t smem = batch_smem(prec);
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, kBWarps * 32, smem) != cudaSuccess ||
+        per < 1)
+      per = 1;
+    occ = per;
+  }
+  const int per = b.per_sm[pi] > 0 ? std::min(b.per_sm[pi], occ) : occ;
+  return per * c->sms;
 }
 
 // One batched force evaluation (mode 0: a only; 1: leapfrog step into the
@@ -477,7 +563,9 @@ int batch_eval(nbr_ctx* c, int prec, double G, double eps2, int mode, double kic
   BatchParams p{};
   p.x = s.pos[a][0]; p.y = s.pos[a][1]; p.z = s.pos[a][2]; p.m = s.mass;
   p.rec = s.rec[a]; p.org = s.org[a];
-  p.poff = b.d_poff; p.nreal = b.d_nreal; p.items = b.d_items; p.n_items = b.n_items;
+  const int grid = batch_grid(c, prec, eps2);  // also settles the configuration
+  const int wi = b.wide[prec == kFP32C ? 1 : 0];
+  p.poff = b.d_poff; p.nreal = b.d_nreal; p.items = b.d_items[wi]; p.n_items = b.n_items[wi];
   p.head = b.d_head;
   p.mode = mode; p.G = G; p.kick = kick; p.drift = drift;
   p.ax = s.acc[0]; p.ay = s.acc[1]; p.az = s.acc[2];
@@ -490,7 +578,7 @@ int batch_eval(nbr_ctx* c, int prec, double G, double eps2, int mode, double kic
   pipeline_params(js);
   p.wait_ns = js.wait_ns;
   p.skip_tile = js.skip_tile;
-  e = launch_batch(prec, p, eps2, batch_grid(c, prec, eps2), c->stream);
+  e = launch_batch(prec, wi == 1, p, eps2, grid, c->stream);
   if (kernels) ++*kernels;
   if (e != cudaSuccess) return cuda_fail(c, e, "batch force launch");
   if (mode == 1) {
@@ -508,7 +596,8 @@ void nbr::BatchState::release() {
   dfree(d_poff);
   dfree(d_nreal);
   dfree(d_sys_of_tile);
-  dfree(d_items);
+  dfree(d_items[0]);
+  dfree(d_items[1]);
   dfree(d_head);
   dfree(d_red);
   *this = BatchState();
@@ -525,6 +614,7 @@ int nbr_batch_upload(nbr_ctx* c, size_t nsys, const size_t* offsets, const doubl
   if ((vx || vy || vz) && !(vx && vy && vz))
     return fail(c, NBR_ERR_INVALID_ARG, "velocities must be all given or all NULL");
   if (offsets[0] != 0) return fail(c, NBR_ERR_INVALID_ARG, "offsets[0] must be 0");
+  if (nsys >= (size_t)kWideItem) return fail(c, NBR_ERR_INVALID_ARG, "too many systems");
   for (size_t s = 0; s < nsys; ++s) {
     if (offsets[s + 1] <= offsets[s]) return fail(c, NBR_ERR_INVALID_ARG, "every system needs >= 1 particle");
     if (offsets[s + 1] - offsets[s] > (size_t)1 << 30) return fail(c, NBR_ERR_INVALID_ARG, "system too large");
@@ -571,29 +661,47 @@ int nbr_batch_upload(nbr_ctx* c, size_t nsys, const size_t* offsets, const doubl
     if (e == cudaSuccess) e = cudaMemsetAsync(b.s.acc[d], 0, b.s.n_pad * sizeof(double), c->stream);
   }
   if (e != cudaSuccess) return cuda_fail(c, e, "batch upload");
-  // Work items ordered by cost (receivers x system size), largest first.
-  std::vector<int2> items;
-  std::vector<double> cost;
-  for (size_t s = 0; s < nsys; ++s) {
-    const long long ns = (long long)(offsets[s + 1] - offsets[s]);
-    const long long nt = (ns + kTile - 1) / kTile;
-    for (long long t = 0; t < nt; ++t) {
-      const long long r = std::min<long long>(kTile, ns - t * kTile);
-      items.push_back(make_int2((int)s, (int)(b.poff[s] / kTile + t)));
-      cost.push_back(double(r > 64 ? kTile : r > 32 ? 64 : r > 16 ? 32 : 16) * double(ns));
+  // Work items ordered by cost (receiver slots x system size), largest first:
+  // list 0 with one-tile items only, list 1 pairing a system's tiles into
+  // two-tile items (a system's odd last tile stays a one-tile item).
+  std::vector<int2> lists[2];
+  for (int wl = 0; wl < 2; ++wl) {
+    std::vector<int2> items;
+    std::vector<double> cost;
+    for (size_t s = 0; s < nsys; ++s) {
+      const long long ns = (long long)(offsets[s + 1] - offsets[s]);
+      const long long nt = (ns + kTile - 1) / kTile;
+      for (long long t = 0; t < nt;) {
+        const int tile = (int)(b.poff[s] / kTile + t);
+        if (wl == 1 && t + 1 < nt) {
+          items.push_back(make_int2((int)s | kWideItem, tile));
+          cost.push_back(2.0 * kTile * double(ns));
+          t += 2;
+        } else {
+          const long long r = std::min<long long>(kTile, ns - t * kTile);
+          items.push_back(make_int2((int)s, tile));
+          cost.push_back(double(r > 64 ? kTile : r > 32 ? 64 : r > 16 ? 32 : 16) * double(ns));
+          t += 1;
+        }
+      }
     }
+    std::vector<int> order(items.size());
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int bb) { return cost[a] > cost[bb]; });
+    lists[wl].resize(items.size());
+    for (size_t k = 0; k < order.size(); ++k) lists[wl][k] = items[order[k]];
+    b.n_items[wl] = (int)lists[wl].size();
   }
-  std::vector<int> order(items.size());
-  std::iota(order.begin(), order.end(), 0);
-  std::stable_sort(order.begin(), order.end(), [&](int a, int bb) { return cost[a] > cost[bb]; });
-  std::vector<int2> sorted(items.size());
-  for (size_t k = 0; k < order.size(); ++k) sorted[k] = items[order[k]];
-  b.n_items = (int)sorted.size();
   std::vector<int> nreal(nsys);
-  for (size_t s = 0; s < nsys; ++s) nreal[s] = (int)(offsets[s + 1] - offsets[s]);
+  b.max_ns = 0;
+  for (size_t s = 0; s < nsys; ++s) {
+    nreal[s] = (int)(offsets[s + 1] - offsets[s]);
+    b.max_ns = std::max(b.max_ns, nreal[s]);
+  }
   e = dalloc((void**)&b.d_poff, (nsys + 1) * sizeof(long long));
   if (e == cudaSuccess) e = dalloc((void**)&b.d_nreal, nsys * sizeof(int));
-  if (e == cudaSuccess) e = dalloc((void**)&b.d_items, sorted.size() * sizeof(int2));
+  for (int wl = 0; wl < 2 && e == cudaSuccess; ++wl)
+    e = dalloc((void**)&b.d_items[wl], lists[wl].size() * sizeof(int2));
   if (e == cudaSuccess) e = dalloc((void**)&b.d_head, 256);
   if (e == cudaSuccess) e = dalloc((void**)&b.d_red, nsys * 9 * sizeof(double));
   if (e == cudaSuccess)
@@ -601,8 +709,8 @@ int nbr_batch_upload(nbr_ctx* c, size_t nsys, const size_t* offsets, const doubl
                         cudaMemcpyHostToDevice, c->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(b.d_nreal, nreal.data(), nsys * sizeof(int), cudaMemcpyHostToDevice, c->stream);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(b.d_items, sorted.data(), sorted.size() * sizeof(int2),
+  for (int wl = 0; wl < 2 && e == cudaSuccess; ++wl)
+    e = cudaMemcpyAsync(b.d_items[wl], lists[wl].data(), lists[wl].size() * sizeof(int2),
                         cudaMemcpyHostToDevice, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) {
@@ -768,6 +876,74 @@ int nbr_batch_run(nbr_ctx* c, int precision, double dt, size_t steps, double G, 
     b.acc_eps2 = eps2;
   }
   if (stats) *stats = st;
+  return NBR_OK;
+}
+
+int nbr_batch_set_config(nbr_ctx* c, int precision, int wide, int ctas_per_sm) {
+  if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
+  if (precision != NBR_FP64 && precision != NBR_FP32C)
+    return fail(c, NBR_ERR_INVALID_ARG, "unknown precision");
+  if (wide < -1 || wide > 1 || ctas_per_sm < 0)
+    return fail(c, NBR_ERR_INVALID_ARG, "wide must be -1, 0 or 1 and ctas_per_sm >= 0");
+  BatchState& b = c->bat;
+  const int pi = precision == kFP32C ? 1 : 0;
+  if (wide < 0) {
+    b.cfg_ok[pi] = false;  // back to the autotune cache or the default
+    return NBR_OK;
+  }
+  b.wide[pi] = wide;
+  b.per_sm[pi] = ctas_per_sm;
+  b.cfg_ok[pi] = true;
+  return NBR_OK;
+}
+
+int nbr_batch_autotune(nbr_ctx* c, int precision, double eps2) {
+  if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
+  if (precision != NBR_FP64 && precision != NBR_FP32C)
+    return fail(c, NBR_ERR_INVALID_ARG, "unknown precision");
+  if (!(eps2 >= 0.0) || !std::isfinite(eps2)) return fail(c, NBR_ERR_INVALID_ARG, "bad eps2");
+  BatchState& b = c->bat;
+  if (b.nsys == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no batch uploaded");
+  cudaSetDevice(c->device);
+  const int pi = precision == kFP32C ? 1 : 0;
+  int best_w = -1, best_p = 0;
+  float best_ms = 1e30f;
+  for (int w = 0; w < 2; ++w) {
+    b.wide[pi] = w;
+    b.per_sm[pi] = 0;
+    b.cfg_ok[pi] = true;
+    batch_grid(c, precision, eps2);
+    const int occ = b.occ[pi][eps2 == 0.0 ? 1 : 0][w];
+    for (int per = 1; per <= occ; ++per) {
+      b.per_sm[pi] = per;
+      float tot = 0.f;
+      bool ok = true;
+      for (int rep = 0; rep < 3 && ok; ++rep) {
+        cudaEventRecord(c->ev0, c->stream);
+        ok = batch_eval(c, precision, 1.0, eps2, 0, 0.0, 0.0, nullptr) == NBR_OK;
+        cudaEventRecord(c->ev1, c->stream);
+        ok = ok && check_device_error(c) == NBR_OK;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        if (rep > 0) tot += ms;  // the first repetition warms up
+      }
+      if (ok && tot < best_ms) {
+        best_ms = tot;
+        best_w = w;
+        best_p = per;
+      }
+    }
+  }
+  b.acc_ok = false;
+  if (best_w < 0) {
+    b.cfg_ok[pi] = false;
+    return fail(c, NBR_ERR_CUDA, "no batch configuration ran");
+  }
+  b.wide[pi] = best_w;
+  b.per_sm[pi] = best_p;
+  b.cfg_ok[pi] = true;
+  tune_put(batch_key(precision, b.nsys, b.max_ns, eps2 == 0.0),
+           ForceConfig{best_w ? 8 : 4, kBWarps, best_p});
   return NBR_OK;
 }
 

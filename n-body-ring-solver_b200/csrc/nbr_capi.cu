@@ -249,6 +249,22 @@ void save_tune_locked() {
 
 }  // namespace
 
+bool tune_get(const std::string& key, ForceConfig* out) {
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  load_tune_locked();
+  auto it = g_tune->find(key);
+  if (it == g_tune->end()) return false;
+  *out = it->second;
+  return true;
+}
+
+void tune_put(const std::string& key, const ForceConfig& cfg) {
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  load_tune_locked();
+  (*g_tune)[key] = cfg;
+  save_tune_locked();
+}
+
 // Heuristic split.  Finer (chunk, split) units balance the SMs better; a B200
 // sweep (N = 32768 .. 1048576) found throughput rising with the split up to
 // 8 tiles (1024 sources) per split range and at most 64 splits.  Small systems

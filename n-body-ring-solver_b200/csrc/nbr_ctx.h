@@ -63,18 +63,32 @@ struct BatchState {
   long long* d_poff = nullptr;       // padded offsets (device), nsys + 1
   int* d_nreal = nullptr;            // real size of each system (device)
   int* d_sys_of_tile = nullptr;      // system index of every padded tile
-  int2* d_items = nullptr;           // work queue: (system, first receiver tile)
-  int n_items = 0;
+  // Work queues of (system | kWideItem flag, first receiver tile), cost
+  // ordered: [0] one-tile items only, [1] two-tile items where a system has
+  // two tiles left.
+  int2* d_items[2] = {nullptr, nullptr};
+  int n_items[2] = {0, 0};
+  int max_ns = 0;                    // largest system
   unsigned* d_head = nullptr;        // work-queue heads
   double* d_red = nullptr;           // per-system diagnostic sums
   bool acc_ok = false;
   int acc_prec = 0;
   double acc_G = 0.0, acc_eps2 = 0.0;
   double pairs_per_eval = 0.0;
-  int grid[2][2] = {{0, 0}, {0, 0}};  // persistent grid per (precision, eps == 0)
+  // Kernel configuration per precision: wide items, resident CTAs per SM
+  // (0: the occupancy limit); chosen from the autotune cache or the default
+  // at first use.
+  bool cfg_ok[2] = {false, false};
+  int wide[2] = {1, 1};
+  int per_sm[2] = {0, 0};
+  int occ[2][2][2] = {};              // occupancy limit per (precision, eps == 0, wide)
 
   void release();
 };
+
+// Autotune cache (a JSON file shared by the processes on a host).
+bool tune_get(const std::string& key, ForceConfig* out);
+void tune_put(const std::string& key, const ForceConfig& cfg);
 
 int fail(nbr_ctx* c, int code, const std::string& msg);
 int cuda_fail(nbr_ctx* c, cudaError_t e, const char* where);

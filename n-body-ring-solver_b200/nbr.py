@@ -100,6 +100,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "nbr_batch_run": ([C.c_void_p, C.c_int, C.c_double, _SZ, C.c_double, C.c_double,
                            C.POINTER(RunStats)], C.c_int),
         "nbr_batch_diagnostics": ([C.c_void_p, C.c_double, C.c_double, C.POINTER(Diag)], C.c_int),
+        "nbr_batch_set_config": ([C.c_void_p, C.c_int, C.c_int, C.c_int], C.c_int),
+        "nbr_batch_autotune": ([C.c_void_p, C.c_int, C.c_double], C.c_int),
         "nbr_step_range": ([C.c_void_p, C.c_int, C.c_int, _SZ, _SZ, C.c_double, C.c_double, C.c_double,
                             C.c_double], C.c_int),
         "nbr_state_pointers": ([C.c_void_p] + [C.POINTER(C.c_void_p)] * 6 + [C.POINTER(_SZ)], C.c_int),
@@ -442,6 +444,12 @@ class Context:
         self._chk(self.L.nbr_batch_run(self.h, precision, dt, steps, G, eps2, C.byref(st)), "batch_run")
         return {"force_evals": st.force_evals, "pairs": st.pairs, "gpu_ms": st.gpu_ms,
                 "kernels": st.kernels}
+
+    def batch_set_config(self, precision, wide=-1, ctas_per_sm=0):
+        self._chk(self.L.nbr_batch_set_config(self.h, precision, wide, ctas_per_sm), "batch_set_config")
+
+    def batch_autotune(self, precision, eps2=0.0):
+        self._chk(self.L.nbr_batch_autotune(self.h, precision, eps2), "batch_autotune")
 
     def batch_diagnostics(self, G=1.0, eps2=0.0):
         d = (Diag * self.nsys)()

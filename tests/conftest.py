@@ -9,6 +9,7 @@
 import os
 import subprocess
 import sys
+import tempfile
 
 import numpy as np
 import pytest
@@ -20,6 +21,9 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 for p in (PKG, ORACLE_DIR):
     if p not in sys.path:
         sys.path.insert(0, p)
+# Autotune results of a test run go to a scratch file, not next to libnbr.so.
+os.environ.setdefault("NBR_TUNE_CACHE",
+                      os.path.join(tempfile.mkdtemp(prefix="nbr_tune_"), "nbr_tune_cache.json"))
 
 
 def pytest_configure(config):

@@ -33,10 +33,12 @@ def system(st, off, s):
     return {k: st[k][off[s]:off[s + 1]] for k in st}
 
 
+@pytest.mark.parametrize("wide", [0, 1], ids=["one-tile", "two-tile"])
 @pytest.mark.parametrize("prec", [FP64, FP32C])
-def test_batch_forces_match_oracle(ctx, nbr, oracle, prec):
+def test_batch_forces_match_oracle(ctx, nbr, oracle, prec, wide):
     off, st = make_batch(nbr, SIZES)
     ctx.batch_upload(off, st)
+    ctx.batch_set_config(prec, wide, 0)
     eps2 = 1e-6
     a = ctx.batch_forces(prec, eps2=eps2)
     errs = []
@@ -69,11 +71,13 @@ def test_batch_systems_do_not_interact(ctx, nbr):
     assert rel_err(a[:, :300], single).max() <= 1e-13
 
 
+@pytest.mark.parametrize("wide", [0, 1], ids=["one-tile", "two-tile"])
 @pytest.mark.parametrize("prec", [FP64, FP32C])
-def test_batch_kdk_matches_oracle(ctx, nbr, oracle, prec):
+def test_batch_kdk_matches_oracle(ctx, nbr, oracle, prec, wide):
     sizes = [64, 130, 513, 1000]
     off, st = make_batch(nbr, sizes, seed=9)
     ctx.batch_upload(off, st)
+    ctx.batch_set_config(prec, wide, 1 if wide else 0)
     eps2 = 1e-6
     stats = ctx.batch_run(prec, dt=1e-3, steps=20, eps2=eps2)
     assert stats["force_evals"] == 21
