@@ -196,7 +196,7 @@ def run_reference(a):
     kernel = "AVX512-RSQRT-4I" if ref.has_avx512 else "AVX2-blocked"
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * total / a.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": workload_config(a, {"reference_kernel": kernel,
                                                                "comm_sz": comm}),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": ref.threads(), "kind": "reference",
