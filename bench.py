@@ -57,6 +57,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-accuracy", action="store_true")
     p.add_argument("--no-batch", action="store_true")
+    p.add_argument("--no-config-accuracy", action="store_true",
+                   help="skip the cold-collapse and two-component accuracy runs")
     p.add_argument("--shard", action="store_true",
                    help="use the multi-GPU i-partition path even on one GPU (process group of 1)")
     return p.parse_args()
@@ -342,6 +344,7 @@ def run_ours(a):
     fp64["fp32c_over_fp64"] = achieved / fp64["value"]
 
     batched = None if a.no_batch else measure_batch(ctx, ext, eps2, value)
+    config_acc = None if a.no_config_accuracy else measure_config_accuracy(ctx)
 
     cpu = None
     if not a.no_cpu_baseline and rank == 0:
@@ -359,7 +362,7 @@ def run_ours(a):
                     "d2h_bytes_per_step": 6 * 8 * n, "scheme": "dkd order 2 (reduced_solver_omp_lf's)",
                     "ms_per_step": 1e3 * sum(e2e_s) / a.steps},
             "roofline": roofline, "fp64": fp64, "accuracy": acc, "clocks": clk,
-            "batched": batched, "cpu_baseline": cpu}
+            "batched": batched, "config_accuracy": config_acc, "cpu_baseline": cpu}
     print(json.dumps(line))
     ctx.close()
 
@@ -388,6 +391,69 @@ def measure_batch(ctx, ext, eps2, single_value, steps=10, nsys=4096, seed=3):
                      "ms_per_step": 1e3 * t / steps, "force_evals": r["force_evals"],
                      "kernels": r["kernels"]}
     out["fp32c"]["frac_of_single_system"] = out["fp32c"]["gpairs"] / single_value
+    return out
+
+
+def _rel(a, b):
+    import numpy as np
+    num = np.linalg.norm(a - b, axis=0)
+    den = np.linalg.norm(b, axis=0)
+    return num / np.where(den > 0, den, 1.0)
+
+
+def _drift(ctx, prec, s, dt, steps, eps2):
+    ctx.upload(s)
+    st = ctx.run(prec, 0, 2, dt, steps, eps2=eps2, diag=True)
+    e0, e1 = st["diag"]
+    return abs(e1["E"] - e0["E"]) / abs(e0["E"])
+
+
+def measure_config_accuracy(ctx):
+    """The two accuracy workloads beside the throughput one, FP32C against
+    the FP64 kernel on identical inputs:
+      * cold collapse: uniform ball N = 32768 (seed 1), zero velocities,
+        eps = 1e-2, KDK dt = 1e-4 for 200 steps;
+      * two-component stress test: N = 131072 Plummer (seed 4), 1 % heavy
+        particles 1000x heavier, eps = 1e-3, KDK dt = 2e-4 for 500 steps, with
+        the force error stratified by receiver and source mass class (each
+        class of sources evaluated separately through nbr_accel_ij)."""
+    import numpy as np
+    import nbr
+    out = {}
+    s = nbr.uniform_ball(32768, 1)
+    eps2 = 1e-4
+    ctx.upload(s)
+    a32 = ctx.forces(nbr.FP32C, eps2=eps2)
+    a64 = ctx.forces(nbr.FP64, eps2=eps2)
+    e = _rel(a32, a64)
+    out["uniform_ball_n32768"] = {
+        "force_median_rel_err": float(np.median(e)), "force_max_rel_err": float(e.max()),
+        "energy_drift_fp32c": _drift(ctx, nbr.FP32C, s, 1e-4, 200, eps2),
+        "energy_drift_fp64": _drift(ctx, nbr.FP64, s, 1e-4, 200, eps2), "steps": 200}
+    n, nh = 131072, 1311
+    s = nbr.two_component(n, nh, 1000.0, 4)
+    eps2 = 1e-6
+    heavy = np.zeros(n, dtype=bool)
+    heavy[:nh] = True
+    strat = {}
+    for src_name, src in (("heavy", heavy), ("light", ~heavy)):
+        res = {}
+        for prec in (nbr.FP32C, nbr.FP64):
+            res[prec] = ctx.accel_ij(s["x"], s["y"], s["z"], s["x"][src], s["y"][src], s["z"][src],
+                                     s["m"][src], precision=prec, eps2=eps2)
+        e = _rel(res[nbr.FP32C], res[nbr.FP64])
+        for rcv_name, rcv in (("heavy", heavy), ("light", ~heavy)):
+            strat[f"{rcv_name}<-{src_name}"] = {"median_rel_err": float(np.median(e[rcv])),
+                                                "max_rel_err": float(e[rcv].max())}
+    ctx.upload(s)
+    a32 = ctx.forces(nbr.FP32C, eps2=eps2)
+    a64 = ctx.forces(nbr.FP64, eps2=eps2)
+    e = _rel(a32, a64)
+    out["two_component_n131072"] = {
+        "stratified_receiver<-source": strat,
+        "force_median_rel_err": float(np.median(e)), "force_max_rel_err": float(e.max()),
+        "energy_drift_fp32c": _drift(ctx, nbr.FP32C, s, 2e-4, 500, eps2),
+        "energy_drift_fp64": _drift(ctx, nbr.FP64, s, 2e-4, 500, eps2), "steps": 500}
     return out
 
 

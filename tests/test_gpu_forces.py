@@ -259,3 +259,29 @@ def test_full_size_plummer_sampled(ctx, nbr, oracle, n, seed):
     for a in (a64, a32):
         net = np.abs((a * s["m"]).sum(axis=1)).max()
         assert net <= 1e-6 * (np.linalg.norm(a, axis=0) * s["m"]).sum()
+
+
+@pytest.mark.parametrize("prec", [FP64, FP32C])
+def test_two_component_error_by_mass_class(ctx, nbr, oracle, prec):
+    """The mass-ratio stress test's error, stratified by receiver and source
+    mass class: each source class through nbr_accel_ij against the
+    extended-precision oracle on sampled receivers of both classes."""
+    n, nh, eps2 = 32768, 328, 1e-6
+    s = nbr.two_component(n, nh, 1000.0, 4)
+    rng = np.random.default_rng(7)
+    idx = np.concatenate([rng.choice(nh, 64, replace=False), nh + rng.choice(n - nh, 448, replace=False)])
+    heavy = np.zeros(n, dtype=bool)
+    heavy[:nh] = True
+    for src in (heavy, ~heavy):
+        got = ctx.accel_ij(s["x"][idx], s["y"][idx], s["z"][idx], s["x"][src], s["y"][src], s["z"][src],
+                           s["m"][src], precision=prec, eps2=eps2)
+        # receivers as zero-mass copies in front of the source class
+        X = {k: np.concatenate([s[k][idx], s[k][src]]) for k in ("x", "y", "z")}
+        M = np.concatenate([np.zeros(len(idx)), s["m"][src]])
+        ref = oracle.accel_subset(X["x"], X["y"], X["z"], M, np.arange(len(idx)), eps2=eps2)
+        err = rel_err(got, ref)
+        for cls in (slice(0, 64), slice(64, None)):  # heavy receivers, light receivers
+            if prec == FP64:
+                assert err[cls].max() <= 1e-12
+            else:
+                assert np.median(err[cls]) <= 1e-6 and err[cls].max() <= 1e-4
