@@ -423,27 +423,67 @@ int kick_drift_system(nbr_ctx* c, bool pack, double kick, double drift, bool use
   return NBR_OK;
 }
 
+// Softened potential of the uploaded system on the context stream: phi into
+// dphi (device, may be null) and U = 1/2 sum m_i phi_i into *dU (device).
+// Uses red[red_off ..] for the per-chunk sums.
+int potential_system(nbr_ctx* c, double G, double eps2, double* dphi, size_t red_off,
+                     double** dU) {
+  SysState& s = c->sys;
+  const ForceConfig pc{kPotNI, kPotWarps, 0};
+  int split = auto_split(kFP64, eps2, pc, (long long)s.n, s.ntiles, c->sms);
+  split = std::max(1, std::min(split, s.ntiles));
+  const ForceConfig cfg{kPotNI, kPotWarps, split};
+  int rc = prepare_split(c, cfg, (long long)s.n_pad);
+  if (rc) return rc;
+  const long long chunk = 32LL * kPotNI * kPotWarps;
+  const int chunks = (int)(((long long)s.n + chunk - 1) / chunk);
+  cudaError_t e = c->scr.need_red(red_off + (size_t)chunks + 16);
+  if (e != cudaSuccess) return cuda_fail(c, e, "potential scratch");
+  const int a = s.cur;
+  IParticles ip{s.pos[a][0], s.pos[a][1], s.pos[a][2], s.mass, (long long)s.n};
+  JStream js{s.pos[a][0], s.pos[a][1], s.pos[a][2], s.mass, nullptr, nullptr, s.ntiles, 0, -1};
+  pipeline_params(js);
+  PotentialOut po{};
+  po.G = G;
+  po.phi = dphi;
+  po.blocksum = c->scr.red + red_off;
+  po.part = c->scr.part;
+  po.counters = c->scr.cnt;
+  po.n_pad = (long long)s.n_pad;
+  po.err = c->d_err;
+  e = launch_potential(split, ip, js, po, eps2, c->stream);
+  if (e == cudaSuccess)
+    e = launch_rowsum(po.blocksum, chunks, 1, po.blocksum + chunks, c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "potential launch");
+  *dU = po.blocksum + chunks;
+  return NBR_OK;
+}
+
 int diag_system(nbr_ctx* c, double G, double eps2, nbr_diag* out) {
   SysState& s = c->sys;
   const int a = s.cur;
   const int nb = (int)((s.n + 127) / 128);
-  cudaError_t e = c->scr.need_red((size_t)nb * 9 + 16);
+  // moments (8 x nb), their sums (16), then the potential's chunk sums (<= nb)
+  // and U: sized once here so that nothing below reallocates.
+  cudaError_t e = c->scr.need_red((size_t)nb * 10 + 48);
   if (e != cudaSuccess) return cuda_fail(c, e, "diag scratch");
   double* part = c->scr.red;
-  double* pot = c->scr.red + (size_t)nb * 8;
-  double* res = c->scr.red + (size_t)nb * 9;
+  double* res = c->scr.red + (size_t)nb * 8;
   e = launch_moments((long long)s.n, (long long)s.n_pad, s.pos[a][0], s.pos[a][1], s.pos[a][2],
                      s.vel[0], s.vel[1], s.vel[2], s.mass, part, c->stream);
   if (e == cudaSuccess) e = launch_rowsum(part, nb, 8, res, c->stream);
-  if (e == cudaSuccess)
-    e = launch_potential((long long)s.n, (long long)s.n_pad, s.pos[a][0], s.pos[a][1],
-                         s.pos[a][2], s.mass, G, eps2, nullptr, pot, c->stream);
-  if (e == cudaSuccess) e = launch_rowsum(pot, nb, 1, res + 8, c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "diagnostics");
+  double* dU = nullptr;
+  int rc = potential_system(c, G, eps2, nullptr, (size_t)nb * 9 + 16, &dU);
+  if (rc) return rc;
   double h[9];
+  e = cudaMemcpyAsync(h, res, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(h, res, sizeof(h), cudaMemcpyDeviceToHost, c->stream);
+    e = cudaMemcpyAsync(h + 8, dU, sizeof(double), cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "diagnostics");
+  rc = check_device_error(c);
+  if (rc) return rc;
   out->T = h[0];
   out->P[0] = h[1]; out->P[1] = h[2]; out->P[2] = h[3];
   out->L[0] = h[4]; out->L[1] = h[5]; out->L[2] = h[6];
@@ -816,21 +856,20 @@ int nbr_potential(nbr_ctx* c, double G, double eps2, double* phi, double* U) {
   SysState& s = c->sys;
   if (s.n == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no system uploaded");
   cudaSetDevice(c->device);
-  const int nb = (int)((s.n + 127) / 128);
-  cudaError_t e = c->scr.need_red((size_t)nb + 16);
-  if (e != cudaSuccess) return cuda_fail(c, e, "potential scratch");
   // phi goes to the (otherwise idle) acceleration x array only when requested.
   double* dphi = phi ? s.acc[0] : nullptr;
   if (phi) c->acc_ok = false;
-  e = launch_potential((long long)s.n, (long long)s.n_pad, s.pos[s.cur][0], s.pos[s.cur][1],
-                       s.pos[s.cur][2], s.mass, G, eps2, dphi, c->scr.red, c->stream);
-  if (e == cudaSuccess) e = launch_rowsum(c->scr.red, nb, 1, c->scr.red + nb, c->stream);
+  double* dU = nullptr;
+  int rc = potential_system(c, G, eps2, dphi, 0, &dU);
+  if (rc) return rc;
   double u = 0.0;
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&u, c->scr.red + nb, sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  cudaError_t e = cudaMemcpyAsync(&u, dU, sizeof(double), cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess && phi)
     e = cudaMemcpyAsync(phi, dphi, s.n * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "potential");
+  rc = check_device_error(c);
+  if (rc) return rc;
   if (U) *U = u;
   return NBR_OK;
 }

@@ -461,34 +461,111 @@ __device__ __forceinline__ void block_reduce_store(double (&v)[W], double* out) 
   }
 }
 
-__global__ void __launch_bounds__(128)
-    k_potential(long long n, const double* __restrict__ x, const double* __restrict__ y,
-                const double* __restrict__ z, const double* __restrict__ m, double G, double eps2,
-                double* __restrict__ phi, double* __restrict__ blocksum) {
-  __shared__ double sx[128], sy[128], sz[128], sm[128];
-  const long long i = (long long)blockIdx.x * 128 + threadIdx.x;
-  const bool valid = i < n;
-  const double xi = valid ? x[i] : 0.0, yi = valid ? y[i] : 0.0, zi = valid ? z[i] : 0.0;
-  double acc = 0.0;
-  for (long long j0 = 0; j0 < n; j0 += 128) {
-    const long long jl = j0 + threadIdx.x;
+// Softened potential phi_i = -G sum_{j != i} m_j / sqrt(r^2 + eps2), FP64, with
+// the structure of the FP64 force kernel (receivers in registers, source tiles
+// through the bulk-copy ring, j range split over gridDim.y with a
+// deterministic last-CTA reduction).  Per pair: 3 sub, 3 fma, CUDA's
+// rsqrt(double), 1 fma; the self pair is skipped by index (with eps2 > 0 it
+// would add m_i / eps).  The last CTA of each receiver chunk writes phi and
+// the chunk's sum of 1/2 m_i phi_i (fixed-order tree: deterministic).
+template <int NI, int WARPS, bool EXCL>
+__global__ void __launch_bounds__(WARPS * 32)
+    k_potential_f64(const IParticles ip, const JStream js, const PotentialOut po,
+                    const double eps2) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ double red[WARPS * 32];
+  __shared__ int s_last;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
+  unsigned char* stages = smem + kSmemHead;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long long ibase = ((long long)blockIdx.x * WARPS + warp) * (32 * NI) + lane;
+  const int S = gridDim.y, sp = blockIdx.y;
+  const int t0 = (int)((long long)js.ntiles * sp / S);
+  const int t1 = (int)((long long)js.ntiles * (sp + 1) / S);
+
+  double xi[NI], yi[NI], zi[NI], ph[NI];
+#pragma unroll
+  for (int k = 0; k < NI; ++k) {
+    const long long i = ibase + 32 * k;
+    xi[k] = ip.x[i]; yi[k] = ip.y[i]; zi[k] = ip.z[i];
+    ph[k] = 0.0;
+  }
+  const int i0 = (int)ibase;  // n < 2^31
+  auto issue = [&](int st, int t) {
+    unsigned char* dst = stages + st * kStage64;
+    const uint32_t bar = smem_u32(&bars[st]);
+    const size_t off = (size_t)(t0 + t) * kTile;
+    mbar_expect_tx(bar, kStage64);
+    bulk_g2s(dst, js.x + off, kTile * 8, bar);
+    bulk_g2s(dst + kTile * 8, js.y + off, kTile * 8, bar);
+    bulk_g2s(dst + 2 * kTile * 8, js.z + off, kTile * 8, bar);
+    bulk_g2s(dst + 3 * kTile * 8, js.m + off, kTile * 8, bar);
+  };
+  int tcur = t0;  // the body runs once per tile, in order
+  auto body = [&](int st) {
+    const double* sx = reinterpret_cast<const double*>(stages + st * kStage64);
+    const double* sy = sx + kTile;
+    const double* sz = sy + kTile;
+    const double* sm = sz + kTile;
+    const int jself = i0 - tcur * kTile;  // receiver k's own index in this tile is jself + 32 k
+    ++tcur;
+#pragma unroll 2
+    for (int j = 0; j < kTile; ++j) {
+      const double xj = sx[j], yj = sy[j], zj = sz[j], mj = sm[j];
+#pragma unroll
+      for (int k = 0; k < NI; ++k) {
+        const double dx = xj - xi[k], dy = yj - yi[k], dz = zj - zi[k];
+        double r2 = fma(dx, dx, eps2);
+        r2 = fma(dy, dy, r2);
+        r2 = fma(dz, dz, r2);
+        double y = rsqrt(r2);
+        if (EXCL) y = r2 > 0.0 ? y : 0.0;
+        y = (j == jself + 32 * k) ? 0.0 : y;
+        ph[k] = fma(mj, y, ph[k]);
+      }
+    }
+  };
+  if (!tile_pipeline(bars, t1 - t0, js, po.err, issue, body)) return;
+
+  if (S > 1) {
+    const long long np = po.n_pad;
+    double* P = po.part + (size_t)sp * (size_t)np;
+#pragma unroll
+    for (int k = 0; k < NI; ++k) P[ibase + 32 * k] = ph[k];
+    __threadfence();
     __syncthreads();
-    sx[threadIdx.x] = jl < n ? x[jl] : 0.0;
-    sy[threadIdx.x] = jl < n ? y[jl] : 0.0;
-    sz[threadIdx.x] = jl < n ? z[jl] : 0.0;
-    sm[threadIdx.x] = jl < n ? m[jl] : 0.0;
+    if (threadIdx.x == 0) {
+      const unsigned prev = atomicAdd(&po.counters[blockIdx.x], 1u);
+      s_last = (prev == gridDim.y - 1) ? 1 : 0;
+    }
     __syncthreads();
-    const int cnt = (int)((n - j0) < 128 ? (n - j0) : 128);
-    for (int jj = 0; jj < cnt; ++jj) {
-      if (j0 + jj == i) continue;
-      const double dx = sx[jj] - xi, dy = sy[jj] - yi, dz = sz[jj] - zi;
-      acc += sm[jj] / sqrt(dx * dx + dy * dy + dz * dz + eps2);
+    if (!s_last) return;
+    __threadfence();
+#pragma unroll
+    for (int k = 0; k < NI; ++k) {
+      double v = 0.0;
+      for (int q = 0; q < S; ++q) v += __ldcg(po.part + (size_t)q * (size_t)np + ibase + 32 * k);
+      ph[k] = v;
+    }
+    if (threadIdx.x == 0) po.counters[blockIdx.x] = 0u;
+  }
+  double half = 0.0;
+#pragma unroll
+  for (int k = 0; k < NI; ++k) {
+    const long long i = ibase + 32 * k;
+    if (i < ip.n) {
+      const double p = -po.G * ph[k];
+      if (po.phi) po.phi[i] = p;
+      half += 0.5 * ip.m[i] * p;
     }
   }
-  const double p = -G * acc;
-  if (valid && phi) phi[i] = p;
-  double v[1] = {valid ? 0.5 * m[i] * p : 0.0};
-  block_reduce_store<1>(v, blocksum);
+  red[threadIdx.x] = half;
+  __syncthreads();
+  for (int h = WARPS * 16; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) po.blocksum[blockIdx.x] = red[0];
 }
 
 __global__ void __launch_bounds__(128)
@@ -643,13 +720,16 @@ cudaError_t launch_kick_drift(long long n, long long n_pad, const double* x, con
   return cudaGetLastError();
 }
 
-cudaError_t launch_potential(long long n, long long n_pad, const double* x, const double* y,
-                             const double* z, const double* m, double G, double eps2, double* phi,
-                             double* blocksum, cudaStream_t st) {
-  (void)n_pad;
-  if (n <= 0) return cudaSuccess;
-  const unsigned blocks = (unsigned)((n + 127) / 128);
-  k_potential<<<blocks, 128, 0, st>>>(n, x, y, z, m, G, eps2, phi, blocksum);
+cudaError_t launch_potential(int split, const IParticles& ip, const JStream& js,
+                             const PotentialOut& po, double eps2, cudaStream_t st) {
+  if (ip.n <= 0 || js.ntiles <= 0) return cudaSuccess;
+  const size_t smem = kSmemHead + (size_t)kStages * kStage64;
+  const long long chunk = 32LL * kPotNI * kPotWarps;
+  const dim3 grid((unsigned)((ip.n + chunk - 1) / chunk), (unsigned)(split < 1 ? 1 : split));
+  if (eps2 == 0.0)
+    k_potential_f64<kPotNI, kPotWarps, true><<<grid, kPotWarps * 32, smem, st>>>(ip, js, po, eps2);
+  else
+    k_potential_f64<kPotNI, kPotWarps, false><<<grid, kPotWarps * 32, smem, st>>>(ip, js, po, eps2);
   return cudaGetLastError();
 }
 

@@ -70,11 +70,23 @@ cudaError_t launch_kick_drift(long long n, long long n_pad, const double* x, con
                               double* vx, double* vy, double* vz, double* xn, double* yn,
                               double* zn, float4* rec_next, double4* origin_next,
                               cudaStream_t stream);
-// phi_i = -G sum_{j != i} m_j / sqrt(r^2 + eps2), FP64; per-block partial sums
-// of 1/2 m_i phi_i into blocksum[n_pad / 128].
-cudaError_t launch_potential(long long n, long long n_pad, const double* x, const double* y,
-                             const double* z, const double* m, double G, double eps2, double* phi,
-                             double* blocksum, cudaStream_t stream);
+// Outputs of a potential launch.
+struct PotentialOut {
+  double G;
+  double* phi;         // phi_i (nullptr: not written)
+  double* blocksum;    // per receiver chunk: sum of 1/2 m_i phi_i
+  double* part;        // [split][n_pad] split partials
+  unsigned* counters;  // one per receiver chunk, zero between launches
+  long long n_pad;
+  int* err;            // device error word
+};
+// Receivers per thread and warps per CTA of the potential kernel; a receiver
+// chunk (one blocksum entry) is 32 * kPotNI * kPotWarps particles.
+constexpr int kPotNI = 4, kPotWarps = 4;
+// phi_i = -G sum_{j != i} m_j / sqrt(r^2 + eps2) in FP64 over receivers ip
+// against the FP64 source stream js (x, y, z, m; the receivers themselves).
+cudaError_t launch_potential(int split, const IParticles& ip, const JStream& js,
+                             const PotentialOut& po, double eps2, cudaStream_t stream);
 // Per-block partial sums of T, P, L, M (FP64): 8 values per block into part.
 cudaError_t launch_moments(long long n, long long n_pad, const double* x, const double* y,
                            const double* z, const double* vx, const double* vy, const double* vz,

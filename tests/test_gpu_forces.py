@@ -285,3 +285,19 @@ def test_two_component_error_by_mass_class(ctx, nbr, oracle, prec):
                 assert err[cls].max() <= 1e-12
             else:
                 assert np.median(err[cls]) <= 1e-6 and err[cls].max() <= 1e-4
+
+
+@pytest.mark.parametrize("n", [1, 3, 129, 20000])
+def test_potential_sizes_and_self_term(ctx, nbr, oracle, n):
+    """The tiled FP64 potential: ragged sizes, the split reduction (large n)
+    and the self pair, which with eps > 0 would add m_i / eps if not skipped."""
+    s = nbr.plummer(n, 14)
+    upload(ctx, s)
+    eps2 = 1e-2
+    U, phi = ctx.potential(eps2=eps2, per_particle=True)
+    ref = oracle.potential(s["x"], s["y"], s["z"], s["m"], eps2=eps2)
+    if n == 1:
+        assert phi[0] == 0.0 and U == 0.0
+        return
+    np.testing.assert_allclose(phi, ref, rtol=1e-12)
+    assert abs(U - 0.5 * float(np.dot(s["m"], ref))) <= 1e-12 * abs(U)
