@@ -210,6 +210,16 @@ def run_reference(a):
 
 
 # -------------------------------------------------------------------- ours --
+def measured_hbm_gbs():
+    """The measured copy bandwidth of this pool's B200s (MEASURED_PEAKS.json,
+    written beside bench.py), else the recipe's earlier measurement."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, ValueError, KeyError, TypeError):
+        return 6650.0, "fallback"
+
+
 def profile_traffic():
     try:
         with open(PROFILE_SUMMARY) as f:
@@ -340,6 +350,14 @@ def run_ours(a):
                                "/ 16 FMA-pipe ops per pair (MEASURED_PEAKS.json has no FP32-pipe figure)",
                 "frac_at_max_clock": achieved / (SMS * 128 * 1965e6 / FMA_OPS_PER_PAIR / 1e9),
                 "kernel_ms": 1e3 * t_k, "mufu_peak": SMS * 16 * mhz * 1e6 / 1e9}
+    traffic = roofline["traffic"]
+    hbm_peak, hbm_src = measured_hbm_gbs()
+    if traffic:
+        # The HBM roofline for comparison: the kernel's DRAM bytes per launch
+        # (ncu) over its live launch time, against the measured copy bandwidth.
+        gbs = traffic / t_k / 1e9
+        roofline["hbm_view"] = {"bound": "hbm", "achieved": gbs, "peak": hbm_peak, "unit": "GB/s",
+                                "frac": gbs / hbm_peak, "peak_source": hbm_src}
     fp64 = {"value": pairs / statistics.mean(k64) / 1e9, "unit": UNIT, "kernel_ms": 1e3 * statistics.mean(k64)}
     fp64["fp32c_over_fp64"] = achieved / fp64["value"]
 
