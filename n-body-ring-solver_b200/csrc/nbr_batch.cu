@@ -608,6 +608,7 @@ extern "C" {
 int nbr_batch_upload(nbr_ctx* c, size_t nsys, const size_t* offsets, const double* x,
                      const double* y, const double* z, const double* vx, const double* vy,
                      const double* vz, const double* m) {
+  TraceRange trace_range("nbr_batch_upload");
   if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
   if (nsys == 0 || !offsets || !x || !y || !z || !m)
     return fail(c, NBR_ERR_INVALID_ARG, "empty batch or NULL array");
@@ -641,7 +642,10 @@ int nbr_batch_upload(nbr_ctx* c, size_t nsys, const size_t* offsets, const doubl
   b.pairs_per_eval = pairs;
   const size_t np = (size_t)b.poff[nsys];
   cudaError_t e = b.s.reserve(np);
-  if (e != cudaSuccess) return cuda_fail(c, e, "batch allocation");
+  if (e != cudaSuccess) {
+    b.release();  // no half-built batch is left behind
+    return cuda_fail(c, e, "batch allocation");
+  }
   // Host staging in the padded layout.
   std::vector<double> h(b.s.n_pad, 0.0);
   auto put = [&](double* d, const double* src) {
@@ -660,7 +664,10 @@ int nbr_batch_upload(nbr_ctx* c, size_t nsys, const size_t* offsets, const doubl
     e = cudaMemsetAsync(b.s.pos[1][d], 0, b.s.n_pad * sizeof(double), c->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(b.s.acc[d], 0, b.s.n_pad * sizeof(double), c->stream);
   }
-  if (e != cudaSuccess) return cuda_fail(c, e, "batch upload");
+  if (e != cudaSuccess) {
+    b.release();
+    return cuda_fail(c, e, "batch upload");
+  }
   // Work items ordered by cost (receiver slots x system size), largest first:
   // list 0 with one-tile items only, list 1 pairing a system's tiles into
   // two-tile items (a system's odd last tile stays a one-tile item).
@@ -725,6 +732,7 @@ int nbr_batch_upload(nbr_ctx* c, size_t nsys, const size_t* offsets, const doubl
 
 int nbr_batch_download(nbr_ctx* c, double* x, double* y, double* z, double* vx, double* vy,
                        double* vz) {
+  TraceRange trace_range("nbr_batch_download");
   if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
   BatchState& b = c->bat;
   if (b.nsys == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no batch uploaded");
@@ -747,6 +755,7 @@ int nbr_batch_download(nbr_ctx* c, double* x, double* y, double* z, double* vx, 
 
 int nbr_batch_forces(nbr_ctx* c, int precision, double G, double eps2, int want_force, double* ax,
                      double* ay, double* az) {
+  TraceRange trace_range("nbr_batch_forces");
   if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
   if (precision != NBR_FP64 && precision != NBR_FP32C)
     return fail(c, NBR_ERR_INVALID_ARG, "unknown precision");
@@ -788,6 +797,7 @@ int nbr_batch_forces(nbr_ctx* c, int precision, double G, double eps2, int want_
 
 int nbr_batch_run(nbr_ctx* c, int precision, double dt, size_t steps, double G, double eps2,
                   nbr_run_stats* stats) {
+  TraceRange trace_range("nbr_batch_run");
   if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
   if (precision != NBR_FP64 && precision != NBR_FP32C)
     return fail(c, NBR_ERR_INVALID_ARG, "unknown precision");
@@ -898,6 +908,7 @@ int nbr_batch_set_config(nbr_ctx* c, int precision, int wide, int ctas_per_sm) {
 }
 
 int nbr_batch_autotune(nbr_ctx* c, int precision, double eps2) {
+  TraceRange trace_range("nbr_batch_autotune");
   if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
   if (precision != NBR_FP64 && precision != NBR_FP32C)
     return fail(c, NBR_ERR_INVALID_ARG, "unknown precision");
@@ -948,6 +959,7 @@ int nbr_batch_autotune(nbr_ctx* c, int precision, double eps2) {
 }
 
 int nbr_batch_diagnostics(nbr_ctx* c, double G, double eps2, nbr_diag* out) {
+  TraceRange trace_range("nbr_batch_diagnostics");
   if (!c || !out) return fail(c, NBR_ERR_INVALID_ARG, "NULL argument");
   if (!(eps2 >= 0.0) || !std::isfinite(eps2)) return fail(c, NBR_ERR_INVALID_ARG, "bad eps2");
   BatchState& b = c->bat;

@@ -48,9 +48,30 @@ void dfree(void* p) {
 // zeroing is completed here before any kernel can see the memory (a counter
 // array zeroed late once left split-arrival counters non-zero).  Allocation is
 // rare (buffers only grow), so the device-wide wait costs nothing in a step.
+//
+// Test hook (fault injection on the host, no GPU fault): with
+// NBR_TEST_FAIL_ALLOC=k set, the k-th allocation counted from the moment the
+// variable took its current value reports cudaErrorMemoryAllocation instead of
+// allocating.
 cudaError_t dalloc(void** p, size_t bytes) {
   *p = nullptr;
   if (bytes == 0) bytes = 256;
+  {
+    static std::mutex mu;
+    static std::string armed;
+    static long count = 0;
+    const char* v = std::getenv("NBR_TEST_FAIL_ALLOC");
+    std::lock_guard<std::mutex> lock(mu);
+    if (v && *v) {
+      if (armed != v) {
+        armed = v;
+        count = 0;
+      }
+      if (++count == std::atol(v)) return cudaErrorMemoryAllocation;
+    } else {
+      armed.clear();
+    }
+  }
   cudaError_t e = cudaMalloc(p, bytes);
   if (e != cudaSuccess) return e;
   e = cudaMemset(*p, 0, bytes);
@@ -605,6 +626,7 @@ size_t nbr_system_size(const nbr_ctx* c) { return c ? c->sys.n : 0; }
 
 int nbr_system_upload(nbr_ctx* c, size_t n, const double* x, const double* y, const double* z,
                       const double* vx, const double* vy, const double* vz, const double* m) {
+  TraceRange trace_range("nbr_system_upload");
   if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
   if (n == 0 || !x || !y || !z || !m) return fail(c, NBR_ERR_INVALID_ARG, "empty system or NULL array");
   if ((vx || vy || vz) && !(vx && vy && vz))
@@ -640,7 +662,10 @@ int nbr_system_upload(nbr_ctx* c, size_t n, const double* x, const double* y, co
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(&h_flags, flags, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-  if (e != cudaSuccess) return cuda_fail(c, e, "upload");
+  if (e != cudaSuccess) {
+    s.n = 0;  // no half-copied system is kept
+    return cuda_fail(c, e, "upload");
+  }
   if (h_flags) {
     s.n = 0;  // the rejected system is not kept
     return (h_flags & 1) ? fail(c, NBR_ERR_NONFINITE, "input contains NaN or Inf")
@@ -651,6 +676,7 @@ int nbr_system_upload(nbr_ctx* c, size_t n, const double* x, const double* y, co
 
 int nbr_system_download(nbr_ctx* c, double* x, double* y, double* z, double* vx, double* vy,
                         double* vz) {
+  TraceRange trace_range("nbr_system_download");
   if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
   SysState& s = c->sys;
   if (s.n == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no system uploaded");
@@ -668,6 +694,7 @@ int nbr_system_download(nbr_ctx* c, double* x, double* y, double* z, double* vx,
 
 int nbr_forces(nbr_ctx* c, int precision, double G, double eps2, int want_force, double* ax,
                double* ay, double* az) {
+  TraceRange trace_range("nbr_forces");
   if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
   if (precision != NBR_FP64 && precision != NBR_FP32C)
     return fail(c, NBR_ERR_INVALID_ARG, "unknown precision");
@@ -695,6 +722,7 @@ int nbr_forces(nbr_ctx* c, int precision, double G, double eps2, int want_force,
 }
 
 int nbr_forces_device(nbr_ctx* c, int precision, double G, double eps2) {
+  TraceRange trace_range("nbr_forces_device");
   if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
   if (precision != NBR_FP64 && precision != NBR_FP32C)
     return fail(c, NBR_ERR_INVALID_ARG, "unknown precision");
@@ -712,6 +740,7 @@ int nbr_forces_device(nbr_ctx* c, int precision, double G, double eps2) {
 }
 
 int nbr_forces_download(nbr_ctx* c, double* ax, double* ay, double* az) {
+  TraceRange trace_range("nbr_forces_download");
   if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
   SysState& s = c->sys;
   if (s.n == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no system uploaded");
@@ -732,6 +761,7 @@ int nbr_forces_download(nbr_ctx* c, double* ax, double* ay, double* az) {
 
 int nbr_step_range(nbr_ctx* c, int precision, int scheme, size_t i0, size_t count, double kick,
                    double drift, double G, double eps2) {
+  TraceRange trace_range("nbr_step_range");
   if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
   if (precision != NBR_FP64 && precision != NBR_FP32C)
     return fail(c, NBR_ERR_INVALID_ARG, "unknown precision");
@@ -779,6 +809,7 @@ int nbr_accel_ij(nbr_ctx* c, int precision, size_t n_i, const double* xi, const 
                  const double* zi, const double* mi, size_t n_j, const double* xj,
                  const double* yj, const double* zj, const double* mj, double G, double eps2,
                  int want_force, double* ax, double* ay, double* az) {
+  TraceRange trace_range("nbr_accel_ij");
   if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
   if (precision != NBR_FP64 && precision != NBR_FP32C)
     return fail(c, NBR_ERR_INVALID_ARG, "unknown precision");
@@ -851,6 +882,7 @@ int nbr_accel_ij(nbr_ctx* c, int precision, size_t n_i, const double* xi, const 
 }
 
 int nbr_potential(nbr_ctx* c, double G, double eps2, double* phi, double* U) {
+  TraceRange trace_range("nbr_potential");
   if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
   if (!(eps2 >= 0.0) || !std::isfinite(eps2)) return fail(c, NBR_ERR_INVALID_ARG, "bad eps2");
   SysState& s = c->sys;
@@ -875,6 +907,7 @@ int nbr_potential(nbr_ctx* c, double G, double eps2, double* phi, double* U) {
 }
 
 int nbr_diagnostics(nbr_ctx* c, double G, double eps2, nbr_diag* out) {
+  TraceRange trace_range("nbr_diagnostics");
   if (!c || !out) return fail(c, NBR_ERR_INVALID_ARG, "NULL argument");
   if (!(eps2 >= 0.0) || !std::isfinite(eps2)) return fail(c, NBR_ERR_INVALID_ARG, "bad eps2");
   if (c->sys.n == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no system uploaded");
@@ -889,6 +922,7 @@ int nbr_yoshida_coefficients(int order, double* cc, double* dd) {
 
 int nbr_run(nbr_ctx* c, int precision, int scheme, int order, double dt, size_t steps, double G,
             double eps2, nbr_diag* diag, nbr_run_stats* stats) {
+  TraceRange trace_range("nbr_run");
   if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
   if (precision != NBR_FP64 && precision != NBR_FP32C)
     return fail(c, NBR_ERR_INVALID_ARG, "unknown precision");
@@ -1065,6 +1099,7 @@ const char* nbr_tune_cache_path(void) {
 }
 
 int nbr_autotune(nbr_ctx* c, int precision, double eps2) {
+  TraceRange trace_range("nbr_autotune");
   if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
   if (precision != NBR_FP64 && precision != NBR_FP32C)
     return fail(c, NBR_ERR_INVALID_ARG, "unknown precision");

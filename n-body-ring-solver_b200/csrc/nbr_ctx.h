@@ -5,6 +5,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "nbr.h"
 #include "nbr_kernels.cuh"
 
@@ -84,6 +86,15 @@ struct BatchState {
   int occ[2][2][2] = {};              // occupancy limit per (precision, eps == 0, wide)
 
   void release();
+};
+
+// An NVTX range around a public call (visible to Nsight tools; a no-op when
+// none is attached).
+struct TraceRange {
+  explicit TraceRange(const char* name) { nvtxRangePushA(name); }
+  ~TraceRange() { nvtxRangePop(); }
+  TraceRange(const TraceRange&) = delete;
+  TraceRange& operator=(const TraceRange&) = delete;
 };
 
 // Autotune cache (a JSON file shared by the processes on a host).

@@ -77,6 +77,7 @@ int scratch_address(int device, unsigned char** out) {
 extern "C" int nbr_forces_noalloc(int precision, size_t n, const double* x, const double* y,
                                   const double* z, const double* m, double G, double eps2,
                                   double* ax, double* ay, double* az, void* stream) {
+  TraceRange trace_range("nbr_forces_noalloc");
   if (precision != NBR_FP64 && precision != NBR_FP32C)
     return fail(nullptr, NBR_ERR_INVALID_ARG, "unknown precision");
   if (n > size_t(kMaxN))

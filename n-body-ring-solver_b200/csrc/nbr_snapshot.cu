@@ -103,6 +103,7 @@ extern "C" int nbr_snapshot_read_arrays(const char* path, size_t n, size_t recor
 }
 
 extern "C" int nbr_snapshot_save(nbr_ctx* c, const char* path, size_t time_step, double delta_t) {
+  TraceRange trace_range("nbr_snapshot_save");
   if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
   SysState& s = c->sys;
   if (s.n == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no system uploaded");
@@ -134,6 +135,7 @@ extern "C" int nbr_snapshot_save(nbr_ctx* c, const char* path, size_t time_step,
 
 extern "C" int nbr_snapshot_load(nbr_ctx* c, const char* path, size_t n, size_t record,
                                  double* time) {
+  TraceRange trace_range("nbr_snapshot_load");
   if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
   std::vector<double> h(7 * n);
   double* H[7];
