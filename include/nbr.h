@@ -36,7 +36,9 @@ typedef enum nbr_status {
   NBR_ERR_NO_SYSTEM = 5,    /* no particles uploaded yet */
   NBR_ERR_UNSUPPORTED = 6,  /* no CUDA device / unsupported configuration */
   NBR_ERR_NONFINITE = 7,    /* an input contains NaN or Inf */
-  NBR_ERR_IO = 8            /* a snapshot file could not be opened, read or written */
+  NBR_ERR_IO = 8,           /* a snapshot file could not be opened, read or written */
+  NBR_ERR_BOUNDS = 9        /* libnbr_checked.so only: a kernel index fell outside its
+                               array; the access was skipped (a library defect) */
 } nbr_status;
 
 /* Arithmetic of the pair interaction. */

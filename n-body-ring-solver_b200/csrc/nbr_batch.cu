@@ -65,6 +65,8 @@ struct BatchParams {
   int* err;
   unsigned long long wait_ns;
   int skip_tile;
+  NBR_CHECKED_FIELD(long long len)  // entries allocated in the particle arrays
+  NBR_CHECKED_FIELD(int nsys)
 };
 
 template <int P>
@@ -206,7 +208,8 @@ __device__ __forceinline__ bool run_item(const BatchParams& p, double eps2, u64 
 #pragma unroll
   for (int k = 0; k < NR; ++k) {
     const long long i = rbase + gl + G * k;  // inside the item's tiles for every F
-    xi[k] = p.x[i]; yi[k] = p.y[i]; zi[k] = p.z[i];
+    xi[k] = yi[k] = zi[k] = 0.0;
+    if (NBR_IN(i, p.len, p.err)) { xi[k] = p.x[i]; yi[k] = p.y[i]; zi[k] = p.z[i]; }
   }
   u64 hx[NP], hy[NP], hz[NP], lx[NP], ly[NP], lz[NP];
 #pragma unroll
@@ -223,6 +226,7 @@ __device__ __forceinline__ bool run_item(const BatchParams& p, double eps2, u64 
     unsigned char* dst = ring.stages + st * SB;
     const uint32_t bar = smem_u32(&ring.bars[st]);
     const size_t tile = (size_t)(t_first + t);
+    if (!NBR_IN((long long)(tile + 1) * kTile - 1, p.len, p.err)) return;  // the wait expires
     if (PREC == kFP32C) {
       mbar_expect_tx(bar, kStageB32);
       bulk_g2s(dst, p.rec + tile * kTile * 3, kRec32, bar);
@@ -310,6 +314,7 @@ __device__ __forceinline__ bool run_item(const BatchParams& p, double eps2, u64 
       const int loc = gl + G * k;
       if (loc >= R) continue;
       const long long i = rbase + loc;
+      if (!NBR_IN(i, p.len, p.err)) continue;
       const double gx = p.G * ax[k], gy = p.G * ay[k], gz = p.G * az[k];
       p.ax[i] = gx; p.ay[i] = gy; p.az[i] = gz;
       if (p.mode == 1) {
@@ -323,7 +328,7 @@ __device__ __forceinline__ bool run_item(const BatchParams& p, double eps2, u64 
       }
     }
   }
-  if (p.mode == 1 && p.rec_next) {
+  if (p.mode == 1 && p.rec_next && NBR_IN(rbase + 32 * NR - 1, p.len, p.err)) {
     // Pack each of the item's tiles of the new positions (layout lane + 32k);
     // every tile of an item holds at least one real receiver.
     __syncwarp();
@@ -398,6 +403,7 @@ __global__ void __launch_bounds__(kBWarps * 32) k_batch_force(const BatchParams 
     if (item >= p.n_items) break;
     const int2 it = p.items[item];
     const int s = it.x & ~kWideItem;
+    if (!NBR_IN(s, p.nsys, p.err)) return;
     bool ok;
     if (WIDE && (it.x & kWideItem)) ok = run_item<PREC, EXCL, 8>(p, eps2, EPS2, ring, lane, s, it.y);
     else ok = run_item<PREC, EXCL, 4>(p, eps2, EPS2, ring, lane, s, it.y);
@@ -578,6 +584,7 @@ int batch_eval(nbr_ctx* c, int prec, double G, double eps2, int mode, double kic
   pipeline_params(js);
   p.wait_ns = js.wait_ns;
   p.skip_tile = js.skip_tile;
+  NBR_CHECKED_ONLY(p.len = (long long)s.cap; p.nsys = (int)b.nsys;)
   e = launch_batch(prec, wi == 1, p, eps2, grid, c->stream);
   if (kernels) ++*kernels;
   if (e != cudaSuccess) return cuda_fail(c, e, "batch force launch");

@@ -355,6 +355,9 @@ int check_device_error(nbr_ctx* c) {
     if (c->scr.cnt) cudaMemsetAsync(c->scr.cnt, 0, c->scr.cnt_cap * sizeof(unsigned), c->stream);
     cudaStreamSynchronize(c->stream);
     c->acc_ok = false;
+    if (h == kErrBounds)
+      return fail(c, NBR_ERR_BOUNDS, "a kernel index was outside its array (checked build); "
+                                     "the access was skipped");
     return fail(c, NBR_ERR_TIMEOUT,
                 h == kErrTileWait ? "a j-tile copy did not complete within the wait limit"
                                   : "device wait limit exceeded (code " + std::to_string(h) + ")");
@@ -414,6 +417,12 @@ int eval_system(nbr_ctx* c, int precision, double G, double eps2, int mode, doub
   ep.counters = c->scr.cnt;
   ep.n_pad = np_i;
   ep.err = c->d_err;
+  NBR_CHECKED_ONLY(
+      ip.len = (long long)(s.cap + kRangeSlack) - r0; js.len = (long long)s.cap;
+      ep.part_len = (long long)c->scr.part_cap; ep.cnt_len = (long long)c->scr.cnt_cap;
+      ep.rec_len = (long long)s.cap;
+      // test hook: under-report the receivers' length so that the check trips
+      if (std::getenv("NBR_TEST_SHRINK_BOUNDS")) ip.len = rn - 1;)
   e = launch_force(precision, eps2, cfg, ip, js, ep, c->stream);
   if (kernels) ++*kernels;
   if (e != cudaSuccess) return cuda_fail(c, e, "force launch");
@@ -472,6 +481,10 @@ int potential_system(nbr_ctx* c, double G, double eps2, double* dphi, size_t red
   po.counters = c->scr.cnt;
   po.n_pad = (long long)s.n_pad;
   po.err = c->d_err;
+  NBR_CHECKED_ONLY(
+      ip.len = (long long)(s.cap + kRangeSlack); js.len = (long long)s.cap;
+      po.part_len = (long long)c->scr.part_cap; po.cnt_len = (long long)c->scr.cnt_cap;
+      po.blocksum_len = (long long)(c->scr.red_cap - red_off);)
   e = launch_potential(split, ip, js, po, eps2, c->stream);
   if (e == cudaSuccess)
     e = launch_rowsum(po.blocksum, chunks, 1, po.blocksum + chunks, c->stream);
@@ -869,6 +882,9 @@ int nbr_accel_ij(nbr_ctx* c, int precision, size_t n_i, const double* xi, const 
   ep.counters = c->scr.cnt;
   ep.n_pad = npi;
   ep.err = c->d_err;
+  NBR_CHECKED_ONLY(
+      ip.len = (long long)(r.cap + kRangeSlack); js.len = (long long)r.cap;
+      ep.part_len = (long long)c->scr.part_cap; ep.cnt_len = (long long)c->scr.cnt_cap;)
   e = launch_force(precision, eps2, cfg, ip, js, ep, c->stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "ij force launch");
   rc = check_device_error(c);

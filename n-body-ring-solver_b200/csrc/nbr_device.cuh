@@ -24,6 +24,7 @@ enum : int {
   kErrNone = 0,
   kErrTileWait = 1,    // a j-tile's bulk copy did not complete in time
   kErrDrainWait = 2,   // draining in-flight copies after an abort timed out
+  kErrBounds = 3,      // checked builds: an index outside its array (access skipped)
 };
 
 typedef unsigned long long u64;
@@ -136,5 +137,21 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 __device__ __forceinline__ void record_error(int* err, int code) {
   if (err) atomicCAS(err, 0, code);
 }
+
+// Checked builds (-DNBR_CHECKED, libnbr_checked.so) test every array index
+// against the array's allocated length, passed with the launch, before the
+// access; a failing index is recorded (kErrBounds) and the access skipped.
+// In normal builds NBR_IN is the constant true and the length expression is
+// never compiled.
+__device__ __forceinline__ bool in_bounds(long long idx, long long len, int* err) {
+  if (idx >= 0 && idx < len) return true;
+  record_error(err, kErrBounds);
+  return false;
+}
+#ifdef NBR_CHECKED
+#define NBR_IN(idx, len, err) (::nbr::in_bounds((long long)(idx), (long long)(len), (err)))
+#else
+#define NBR_IN(idx, len, err) true
+#endif
 
 }  // namespace nbr

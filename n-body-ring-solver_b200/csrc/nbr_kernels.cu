@@ -197,7 +197,8 @@ __device__ __forceinline__ void epilogue(const IParticles& ip, const Epilogue& e
       ep.xn[i] = xn[k]; ep.yn[i] = yn[k]; ep.zn[i] = zn[k];
     }
   }
-  if (ep.rec_next) pack_warp<NI>(ip.n, ibase, lane, xn, yn, zn, ip.m, ep.rec_next, ep.origin_next);
+  if (ep.rec_next && NBR_IN(ibase - lane + 32 * NI - 1, ep.rec_len, ep.err))
+    pack_warp<NI>(ip.n, ibase, lane, xn, yn, zn, ip.m, ep.rec_next, ep.origin_next);
 }
 
 // Split reduction (if any) followed by the epilogue.
@@ -212,6 +213,7 @@ __device__ __forceinline__ void finish(const IParticles& ip, const Epilogue& ep,
 #pragma unroll
     for (int k = 0; k < NI; ++k) {
       const long long i = ibase + 32 * k;
+      if (!NBR_IN((long long)blockIdx.y * 3 * np + 2 * np + i, ep.part_len, ep.err)) continue;
       P[i] = ax[k];
       P[np + i] = ay[k];
       P[2 * np + i] = az[k];
@@ -219,7 +221,8 @@ __device__ __forceinline__ void finish(const IParticles& ip, const Epilogue& ep,
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) {
-      const unsigned prev = atomicAdd(&ep.counters[blockIdx.x], 1u);
+      const unsigned prev =
+          NBR_IN(blockIdx.x, ep.cnt_len, ep.err) ? atomicAdd(&ep.counters[blockIdx.x], 1u) : 0u;
       s_last = (prev == gridDim.y - 1) ? 1 : 0;
     }
     __syncthreads();
@@ -231,13 +234,14 @@ __device__ __forceinline__ void finish(const IParticles& ip, const Epilogue& ep,
       double sx = 0.0, sy = 0.0, sz = 0.0;
       for (int s = 0; s < (int)gridDim.y; ++s) {
         const double* Q = ep.part + (size_t)s * 3 * (size_t)np;
+        if (!NBR_IN((long long)s * 3 * np + 2 * np + i, ep.part_len, ep.err)) continue;
         sx += __ldcg(Q + i);
         sy += __ldcg(Q + np + i);
         sz += __ldcg(Q + 2 * np + i);
       }
       ax[k] = sx; ay[k] = sy; az[k] = sz;
     }
-    if (threadIdx.x == 0) ep.counters[blockIdx.x] = 0u;
+    if (threadIdx.x == 0 && NBR_IN(blockIdx.x, ep.cnt_len, ep.err)) ep.counters[blockIdx.x] = 0u;
   }
   epilogue<NI>(ip, ep, ibase, lane, xi, yi, zi, ax, ay, az);
 }
@@ -261,7 +265,8 @@ __global__ void __launch_bounds__(WARPS * 32)
 #pragma unroll
   for (int k = 0; k < NI; ++k) {
     const long long i = ibase + 32 * k;
-    xi[k] = ip.x[i]; yi[k] = ip.y[i]; zi[k] = ip.z[i];
+    xi[k] = yi[k] = zi[k] = 0.0;
+    if (NBR_IN(i, ip.len, ep.err)) { xi[k] = ip.x[i]; yi[k] = ip.y[i]; zi[k] = ip.z[i]; }
   }
   u64 hx[IPAIR], hy[IPAIR], hz[IPAIR], lx[IPAIR], ly[IPAIR], lz[IPAIR];
 #pragma unroll
@@ -271,6 +276,7 @@ __global__ void __launch_bounds__(WARPS * 32)
   auto issue = [&](int st, int t) {
     unsigned char* dst = stages + st * kStage32;
     const uint32_t bar = smem_u32(&bars[st]);
+    if (!NBR_IN((long long)(t0 + t + 1) * kTile - 1, js.len, ep.err)) return;  // the wait expires
     mbar_expect_tx(bar, kStage32);
     bulk_g2s(dst, js.rec + (size_t)(t0 + t) * kTile * 3, kRecBytes, bar);
     bulk_g2s(dst + kRecBytes, js.origin + (t0 + t), 32, bar);
@@ -362,7 +368,8 @@ __global__ void __launch_bounds__(WARPS * 32)
 #pragma unroll
   for (int k = 0; k < NI; ++k) {
     const long long i = ibase + 32 * k;
-    xi[k] = ip.x[i]; yi[k] = ip.y[i]; zi[k] = ip.z[i];
+    xi[k] = yi[k] = zi[k] = 0.0;
+    if (NBR_IN(i, ip.len, ep.err)) { xi[k] = ip.x[i]; yi[k] = ip.y[i]; zi[k] = ip.z[i]; }
     ax[k] = ay[k] = az[k] = 0.0;
   }
 
@@ -370,6 +377,7 @@ __global__ void __launch_bounds__(WARPS * 32)
     unsigned char* dst = stages + st * kStage64;
     const uint32_t bar = smem_u32(&bars[st]);
     const size_t off = (size_t)(t0 + t) * kTile;
+    if (!NBR_IN((long long)off + kTile - 1, js.len, ep.err)) return;  // the wait expires
     mbar_expect_tx(bar, kStage64);
     bulk_g2s(dst, js.x + off, kTile * 8, bar);
     bulk_g2s(dst + kTile * 8, js.y + off, kTile * 8, bar);
@@ -487,7 +495,8 @@ __global__ void __launch_bounds__(WARPS * 32)
 #pragma unroll
   for (int k = 0; k < NI; ++k) {
     const long long i = ibase + 32 * k;
-    xi[k] = ip.x[i]; yi[k] = ip.y[i]; zi[k] = ip.z[i];
+    xi[k] = yi[k] = zi[k] = 0.0;
+    if (NBR_IN(i, ip.len, po.err)) { xi[k] = ip.x[i]; yi[k] = ip.y[i]; zi[k] = ip.z[i]; }
     ph[k] = 0.0;
   }
   const int i0 = (int)ibase;  // n < 2^31
@@ -495,6 +504,7 @@ __global__ void __launch_bounds__(WARPS * 32)
     unsigned char* dst = stages + st * kStage64;
     const uint32_t bar = smem_u32(&bars[st]);
     const size_t off = (size_t)(t0 + t) * kTile;
+    if (!NBR_IN((long long)off + kTile - 1, js.len, po.err)) return;  // the wait expires
     mbar_expect_tx(bar, kStage64);
     bulk_g2s(dst, js.x + off, kTile * 8, bar);
     bulk_g2s(dst + kTile * 8, js.y + off, kTile * 8, bar);
@@ -531,11 +541,13 @@ __global__ void __launch_bounds__(WARPS * 32)
     const long long np = po.n_pad;
     double* P = po.part + (size_t)sp * (size_t)np;
 #pragma unroll
-    for (int k = 0; k < NI; ++k) P[ibase + 32 * k] = ph[k];
+    for (int k = 0; k < NI; ++k)
+      if (NBR_IN((long long)sp * np + ibase + 32 * k, po.part_len, po.err)) P[ibase + 32 * k] = ph[k];
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) {
-      const unsigned prev = atomicAdd(&po.counters[blockIdx.x], 1u);
+      const unsigned prev =
+          NBR_IN(blockIdx.x, po.cnt_len, po.err) ? atomicAdd(&po.counters[blockIdx.x], 1u) : 0u;
       s_last = (prev == gridDim.y - 1) ? 1 : 0;
     }
     __syncthreads();
@@ -544,10 +556,12 @@ __global__ void __launch_bounds__(WARPS * 32)
 #pragma unroll
     for (int k = 0; k < NI; ++k) {
       double v = 0.0;
-      for (int q = 0; q < S; ++q) v += __ldcg(po.part + (size_t)q * (size_t)np + ibase + 32 * k);
+      for (int q = 0; q < S; ++q)
+        if (NBR_IN((long long)q * np + ibase + 32 * k, po.part_len, po.err))
+          v += __ldcg(po.part + (size_t)q * (size_t)np + ibase + 32 * k);
       ph[k] = v;
     }
-    if (threadIdx.x == 0) po.counters[blockIdx.x] = 0u;
+    if (threadIdx.x == 0 && NBR_IN(blockIdx.x, po.cnt_len, po.err)) po.counters[blockIdx.x] = 0u;
   }
   double half = 0.0;
 #pragma unroll
@@ -565,7 +579,7 @@ __global__ void __launch_bounds__(WARPS * 32)
     if ((int)threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
     __syncthreads();
   }
-  if (threadIdx.x == 0) po.blocksum[blockIdx.x] = red[0];
+  if (threadIdx.x == 0 && NBR_IN(blockIdx.x, po.blocksum_len, po.err)) po.blocksum[blockIdx.x] = red[0];
 }
 
 __global__ void __launch_bounds__(128)

@@ -8,6 +8,16 @@ namespace nbr {
 
 enum Precision : int { kFP64 = 0, kFP32C = 1 };
 
+// Fields that only checked builds carry: the allocated lengths the kernels
+// test their indices against (see NBR_IN in nbr_device.cuh).
+#ifdef NBR_CHECKED
+#define NBR_CHECKED_FIELD(decl) decl;
+#define NBR_CHECKED_ONLY(stmt) stmt
+#else
+#define NBR_CHECKED_FIELD(decl)
+#define NBR_CHECKED_ONLY(stmt)
+#endif
+
 // Receivers ("i" particles): FP64 positions, read-only during the launch.
 // Arrays are allocated to a multiple of 1024 entries.
 struct IParticles {
@@ -16,6 +26,7 @@ struct IParticles {
   const double* z;
   const double* m;  // receiver masses (used for force output and the pack)
   long long n;      // real receivers; entries >= n are padding
+  NBR_CHECKED_FIELD(long long len)  // entries allocated from x, y, z, m on
 };
 
 // Sources ("j" particles), streamed tile by tile.  FP64 form: SoA arrays padded
@@ -31,6 +42,7 @@ struct JStream {
   int ntiles;
   unsigned long long wait_ns;  // limit of one bounded tile wait
   int skip_tile;               // test hook: this CTA-local tile is never copied (-1: off)
+  NBR_CHECKED_FIELD(long long len)  // source entries allocated (x..m; rec 3 len, origin len / kTile)
 };
 
 // What happens to each receiver's summed acceleration.
@@ -51,6 +63,9 @@ struct Epilogue {
   unsigned* counters;  // one per CTA chunk, zero between launches
   long long n_pad;
   int* err;            // device error word
+  NBR_CHECKED_FIELD(long long part_len)  // doubles allocated in part
+  NBR_CHECKED_FIELD(long long cnt_len)   // counters allocated
+  NBR_CHECKED_FIELD(long long rec_len)   // particles allocated in rec_next
 };
 
 struct ForceConfig {
@@ -79,6 +94,9 @@ struct PotentialOut {
   unsigned* counters;  // one per receiver chunk, zero between launches
   long long n_pad;
   int* err;            // device error word
+  NBR_CHECKED_FIELD(long long part_len)
+  NBR_CHECKED_FIELD(long long cnt_len)
+  NBR_CHECKED_FIELD(long long blocksum_len)
 };
 // Receivers per thread and warps per CTA of the potential kernel; a receiver
 // chunk (one blocksum entry) is 32 * kPotNI * kPotWarps particles.

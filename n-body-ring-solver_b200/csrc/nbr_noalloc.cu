@@ -149,6 +149,8 @@ extern "C" int nbr_forces_noalloc(int precision, size_t n, const double* x, cons
   ep.counters = cnt;
   ep.n_pad = n_pad;
   ep.err = err;
+  NBR_CHECKED_ONLY(ip.len = kMaxN; js.len = kMaxN; ep.part_len = (long long)kMaxSplit * 3 * kMaxN;
+                   ep.cnt_len = (long long)kCounters;)
   e = launch_force(precision, eps2, cfg, ip, js, ep, st);
   if (e != cudaSuccess) return cuda_fail(nullptr, e, "no-allocation force launch");
 
@@ -156,6 +158,8 @@ extern "C" int nbr_forces_noalloc(int precision, size_t n, const double* x, cons
   e = cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return cuda_fail(nullptr, e, "no-allocation force");
+  if (h == kErrBounds)
+    return fail(nullptr, NBR_ERR_BOUNDS, "a kernel index was outside its array (checked build)");
   if (h != kErrNone)
     return fail(nullptr, NBR_ERR_TIMEOUT, "a j-tile copy did not complete within the wait limit");
   return NBR_OK;

@@ -17,12 +17,14 @@ from typing import Dict, Optional
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libnbr.so")
+# NBR_LIB_PATH selects another build of the library, e.g. libnbr_checked.so.
+LIB_PATH = os.environ.get("NBR_LIB_PATH") or os.path.join(HERE, "libnbr.so")
 
 NBR_OK = 0
 STATUS = {0: "NBR_OK", 1: "NBR_ERR_INVALID_ARG", 2: "NBR_ERR_CUDA", 3: "NBR_ERR_NO_MEMORY",
           4: "NBR_ERR_TIMEOUT", 5: "NBR_ERR_NO_SYSTEM", 6: "NBR_ERR_UNSUPPORTED",
-          7: "NBR_ERR_NONFINITE", 8: "NBR_ERR_IO"}
+          7: "NBR_ERR_NONFINITE", 8: "NBR_ERR_IO",
+          9: "NBR_ERR_BOUNDS"}
 FP64, FP32C = 0, 1
 KDK, DKD, EULER = 0, 1, 2
 KEYS = ("x", "y", "z", "vx", "vy", "vz", "m")
