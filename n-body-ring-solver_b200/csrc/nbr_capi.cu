@@ -292,7 +292,7 @@ void tune_put(const std::string& key, const ForceConfig& cfg) {
 // get at least ~4 waves of resident CTAs, down to 2 tiles per range.
 int auto_split(int precision, double eps2, const ForceConfig& c, long long n_i, int ntiles,
                int sms) {
-  const long long chunk = 32LL * c.ni * c.warps;
+  const long long chunk = force_chunk(c);
   const long long chunks = (n_i + chunk - 1) / chunk;
   int per_sm = force_blocks_per_sm(precision, eps2, c);
   if (per_sm < 1) per_sm = 1;
@@ -312,7 +312,14 @@ ForceConfig choose_config(nbr_ctx* c, int precision, double eps2, long long n_i,
     // Defaults from a configuration sweep on B200 (N = 32768 .. 262144):
     // FP32C is FMA-pipe bound and gains from 4 receiver pairs per thread;
     // FP64 has twice the registers per receiver and prefers 4 per thread.
-    const ForceConfig dflt = precision == kFP32C ? ForceConfig{8, 2, 0} : ForceConfig{4, 4, 0};
+    ForceConfig dflt = precision == kFP32C ? ForceConfig{8, 2, 0} : ForceConfig{4, 4, 0};
+    // Small systems: the warp-splitting kernel.  Lane groups per warp from a
+    // B200 sweep (forces per call, N = 256 .. 262144): FP32C 8 up to 4096
+    // receivers, 2 up to 8192; FP64 8 up to 16384, 4 up to 32768; above
+    // that the large kernels win.
+    const int F = precision == kFP32C ? (n_i <= 4096 ? 8 : n_i <= 8192 ? 2 : 0)
+                                      : (n_i <= 16384 ? 8 : n_i <= 32768 ? 4 : 0);
+    if (F) dflt = ForceConfig{1, F, 0};
     cfg = it != g_tune->end() ? it->second : dflt;
   }
   if (cfg.split <= 0) cfg.split = auto_split(precision, eps2, cfg, n_i, ntiles, c->sms);
@@ -411,7 +418,8 @@ int eval_system(nbr_ctx* c, int precision, double G, double eps2, int mode, doub
   ep.drift = drift;
   ep.vx = s.vel[0] + r0; ep.vy = s.vel[1] + r0; ep.vz = s.vel[2] + r0;
   ep.xn = s.pos[b][0] + r0; ep.yn = s.pos[b][1] + r0; ep.zn = s.pos[b][2] + r0;
-  ep.rec_next = (mode != 0 && precision == kFP32C && !ranged) ? s.rec[b] : nullptr;
+  const bool small = cfg.ni == 1;  // the small-N kernel packs no records
+  ep.rec_next = (mode != 0 && precision == kFP32C && !ranged && !small) ? s.rec[b] : nullptr;
   ep.origin_next = s.org[b];
   ep.part = c->scr.part;
   ep.counters = c->scr.cnt;
@@ -428,7 +436,7 @@ int eval_system(nbr_ctx* c, int precision, double G, double eps2, int mode, doub
   if (e != cudaSuccess) return cuda_fail(c, e, "force launch");
   if (mode != 0) {
     s.cur = b;
-    s.rec_ok[b] = (precision == kFP32C) && !ranged;
+    s.rec_ok[b] = (precision == kFP32C) && !ranged && !small;
     s.rec_ok[a] = false;
   }
   return NBR_OK;
@@ -1123,10 +1131,11 @@ int nbr_autotune(nbr_ctx* c, int precision, double eps2) {
   if (s.n == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no system uploaded");
   cudaSetDevice(c->device);
   const ForceConfig saved = c->override_cfg[precision];
-  const int cand[][2] = {{4, 2}, {4, 4}, {4, 8}, {8, 2}, {8, 4}};
+  const int cand[][2] = {{4, 2}, {4, 4}, {4, 8}, {8, 2}, {8, 4}, {1, 2}, {1, 4}, {1, 8}};
   ForceConfig best{0, 0, 0};
   float best_ms = 1e30f;
   for (auto& cw : cand) {
+    if (cw[0] == 1 && s.n > 65536) continue;  // the small-N kernel only competes on small systems
     ForceConfig base{cw[0], cw[1], 1};
     const int s0 = auto_split(precision, eps2, base, (long long)s.n, s.ntiles, c->sms);
     const int splits[] = {std::max(1, s0 / 2), s0, s0 * 2};

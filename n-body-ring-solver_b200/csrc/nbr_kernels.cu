@@ -411,6 +411,226 @@ __global__ void __launch_bounds__(WARPS * 32)
   finish<NI>(ip, ep, ibase, lane, xi, yi, zi, ax, ay, az);
 }
 
+// ------------------------------------------------- small-N force kernel ----
+// Warp-shuffle splitting for systems too small to fill the GPU with 32 * NI
+// receivers per warp: each warp splits into F lane groups of G = 32 / F
+// lanes; every group holds the same G * kSmallNI receivers (lane gl:
+// receivers base + gl + G k) and takes every F-th source of each tile.  The
+// groups' sums are combined with xor shuffles in a fixed order
+// (deterministic).  A CTA of kSmallWarps warps covers
+// kSmallWarps * G * kSmallNI receivers and, as in the large kernels, one range
+// of the split source tiles.  Pair arithmetic is that of k_force_f32c /
+// k_force_f64.  The fused FP32C record pack is left to the next evaluation's
+// pack kernel.
+template <int PREC, int F, bool EXCL>
+__global__ void __launch_bounds__(kSmallWarps * 32)
+    k_force_small(const IParticles ip, const JStream js, const Epilogue ep, const double eps2) {
+  constexpr int G = 32 / F;
+  constexpr int NI = kSmallNI;
+  constexpr int IPAIR = NI / 2;
+  constexpr int SB = PREC == kFP32C ? kStage32 : kStage64;
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ int s_last;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
+  unsigned char* stages = smem + kSmemHead;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gl = lane % G, phase = lane / G;
+  const long long rbase = ((long long)blockIdx.x * kSmallWarps + warp) * (G * NI) + gl;
+  const int S = gridDim.y, sp = blockIdx.y;
+  const int t0 = (int)((long long)js.ntiles * sp / S);
+  const int t1 = (int)((long long)js.ntiles * (sp + 1) / S);
+
+  double xi[NI], yi[NI], zi[NI], ax[NI], ay[NI], az[NI];
+#pragma unroll
+  for (int k = 0; k < NI; ++k) {
+    const long long i = rbase + G * k;
+    xi[k] = yi[k] = zi[k] = 0.0;
+    if (NBR_IN(i, ip.len, ep.err)) { xi[k] = ip.x[i]; yi[k] = ip.y[i]; zi[k] = ip.z[i]; }
+    ax[k] = ay[k] = az[k] = 0.0;
+  }
+  u64 hx[IPAIR], hy[IPAIR], hz[IPAIR], lx[IPAIR], ly[IPAIR], lz[IPAIR];
+#pragma unroll
+  for (int p = 0; p < IPAIR; ++p) hx[p] = hy[p] = hz[p] = lx[p] = ly[p] = lz[p] = 0ull;
+  const float e2f = (float)eps2;
+  const u64 EPS2 = pack2(e2f, e2f);
+
+  auto issue = [&](int st, int t) {
+    unsigned char* dst = stages + st * SB;
+    const uint32_t bar = smem_u32(&bars[st]);
+    const size_t tile = (size_t)(t0 + t);
+    if (!NBR_IN((long long)(tile + 1) * kTile - 1, js.len, ep.err)) return;  // the wait expires
+    mbar_expect_tx(bar, SB);
+    if (PREC == kFP32C) {
+      bulk_g2s(dst, js.rec + tile * kTile * 3, kRecBytes, bar);
+      bulk_g2s(dst + kRecBytes, js.origin + tile, 32, bar);
+    } else {
+      const size_t off = tile * kTile;
+      bulk_g2s(dst, js.x + off, kTile * 8, bar);
+      bulk_g2s(dst + kTile * 8, js.y + off, kTile * 8, bar);
+      bulk_g2s(dst + 2 * kTile * 8, js.z + off, kTile * 8, bar);
+      bulk_g2s(dst + 3 * kTile * 8, js.m + off, kTile * 8, bar);
+    }
+  };
+  auto body = [&](int st) {
+    const unsigned char* base = stages + st * SB;
+    if (PREC == kFP32C) {
+      const double4 o = *reinterpret_cast<const double4*>(base + kRecBytes);
+      u64 XI[IPAIR], YI[IPAIR], ZI[IPAIR], AX[IPAIR], AY[IPAIR], AZ[IPAIR];
+#pragma unroll
+      for (int p = 0; p < IPAIR; ++p) {
+        XI[p] = pack2(__double2float_rn(xi[2 * p] - o.x), __double2float_rn(xi[2 * p + 1] - o.x));
+        YI[p] = pack2(__double2float_rn(yi[2 * p] - o.y), __double2float_rn(yi[2 * p + 1] - o.y));
+        ZI[p] = pack2(__double2float_rn(zi[2 * p] - o.z), __double2float_rn(zi[2 * p + 1] - o.z));
+        AX[p] = AY[p] = AZ[p] = 0ull;
+      }
+      const ulonglong2* R = reinterpret_cast<const ulonglong2*>(base);
+#pragma unroll 4
+      for (int j = phase; j < kTile; j += F) {
+        const ulonglong2 q0 = R[3 * j];
+        const ulonglong2 q1 = R[3 * j + 1];
+        const u64 bj = R[3 * j + 2].x;
+#pragma unroll
+        for (int p = 0; p < IPAIR; ++p) {
+          const u64 dx = sub2(q0.x, XI[p]);
+          const u64 dy = sub2(q0.y, YI[p]);
+          const u64 dz = sub2(q1.x, ZI[p]);
+          u64 r2 = fma2(dx, dx, EPS2);
+          r2 = fma2(dy, dy, r2);
+          r2 = fma2(dz, dz, r2);
+          u64 y;
+          if (EXCL) {
+            float rl, rh;
+            unpack2(r2, rl, rh);
+            y = pack2(rl > 0.f ? rsqrt_mufu(rl) : 0.f, rh > 0.f ? rsqrt_mufu(rh) : 0.f);
+          } else {
+            y = rsqrt2(r2);
+          }
+          const u64 y2 = mul2(y, y);
+          const u64 pr = mul2(r2, y2);
+          const u64 mg = fma2(q1.y, pr, bj);
+          const u64 y3 = mul2(y2, y);
+          const u64 s = mul2(y3, mg);
+          AX[p] = fma2(s, dx, AX[p]);
+          AY[p] = fma2(s, dy, AY[p]);
+          AZ[p] = fma2(s, dz, AZ[p]);
+        }
+      }
+#pragma unroll
+      for (int p = 0; p < IPAIR; ++p) {
+        two_sum2(hx[p], lx[p], AX[p]);
+        two_sum2(hy[p], ly[p], AY[p]);
+        two_sum2(hz[p], lz[p], AZ[p]);
+      }
+    } else {
+      const double* sx = reinterpret_cast<const double*>(base);
+      const double* sy = sx + kTile;
+      const double* sz = sy + kTile;
+      const double* sm = sz + kTile;
+#pragma unroll 2
+      for (int j = phase; j < kTile; j += F) {
+        const double xj = sx[j], yj = sy[j], zj = sz[j], mj = sm[j];
+#pragma unroll
+        for (int k = 0; k < NI; ++k) {
+          const double dx = xj - xi[k], dy = yj - yi[k], dz = zj - zi[k];
+          double r2 = fma(dx, dx, eps2);
+          r2 = fma(dy, dy, r2);
+          r2 = fma(dz, dz, r2);
+          double y = rsqrt(r2);
+          if (EXCL) y = r2 > 0.0 ? y : 0.0;
+          const double s = mj * (y * y * y);
+          ax[k] = fma(s, dx, ax[k]);
+          ay[k] = fma(s, dy, ay[k]);
+          az[k] = fma(s, dz, az[k]);
+        }
+      }
+    }
+  };
+  if (!tile_pipeline(bars, t1 - t0, js, ep.err, issue, body)) return;
+
+  if (PREC == kFP32C) {
+#pragma unroll
+    for (int p = 0; p < IPAIR; ++p) {
+      float h0, h1, l0, l1;
+      unpack2(hx[p], h0, h1); unpack2(lx[p], l0, l1);
+      ax[2 * p] = (double)h0 + (double)l0; ax[2 * p + 1] = (double)h1 + (double)l1;
+      unpack2(hy[p], h0, h1); unpack2(ly[p], l0, l1);
+      ay[2 * p] = (double)h0 + (double)l0; ay[2 * p + 1] = (double)h1 + (double)l1;
+      unpack2(hz[p], h0, h1); unpack2(lz[p], l0, l1);
+      az[2 * p] = (double)h0 + (double)l0; az[2 * p + 1] = (double)h1 + (double)l1;
+    }
+  }
+  // Lane groups -> one sum per receiver (every lane of a gl ends with it).
+#pragma unroll
+  for (int off = G; off < 32; off <<= 1) {
+#pragma unroll
+    for (int k = 0; k < NI; ++k) {
+      ax[k] += __shfl_xor_sync(0xffffffffu, ax[k], off);
+      ay[k] += __shfl_xor_sync(0xffffffffu, ay[k], off);
+      az[k] += __shfl_xor_sync(0xffffffffu, az[k], off);
+    }
+  }
+  if (S > 1) {
+    const long long np = ep.n_pad;
+    double* P = ep.part + (size_t)sp * 3 * (size_t)np;
+    if (phase == 0) {
+#pragma unroll
+      for (int k = 0; k < NI; ++k) {
+        const long long i = rbase + G * k;
+        if (!NBR_IN((long long)sp * 3 * np + 2 * np + i, ep.part_len, ep.err)) continue;
+        P[i] = ax[k];
+        P[np + i] = ay[k];
+        P[2 * np + i] = az[k];
+      }
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const unsigned prev =
+          NBR_IN(blockIdx.x, ep.cnt_len, ep.err) ? atomicAdd(&ep.counters[blockIdx.x], 1u) : 0u;
+      s_last = (prev == gridDim.y - 1) ? 1 : 0;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    if (phase == 0) {
+#pragma unroll
+      for (int k = 0; k < NI; ++k) {
+        const long long i = rbase + G * k;
+        double sx = 0.0, sy = 0.0, sz = 0.0;
+        for (int q = 0; q < S; ++q) {
+          if (!NBR_IN((long long)q * 3 * np + 2 * np + i, ep.part_len, ep.err)) continue;
+          const double* Q = ep.part + (size_t)q * 3 * (size_t)np;
+          sx += __ldcg(Q + i);
+          sy += __ldcg(Q + np + i);
+          sz += __ldcg(Q + 2 * np + i);
+        }
+        ax[k] = sx; ay[k] = sy; az[k] = sz;
+      }
+    }
+    if (threadIdx.x == 0 && NBR_IN(blockIdx.x, ep.cnt_len, ep.err)) ep.counters[blockIdx.x] = 0u;
+  }
+  if (phase != 0) return;
+#pragma unroll
+  for (int k = 0; k < NI; ++k) {
+    const long long i = rbase + G * k;
+    if (i >= ip.n) continue;
+    if (ep.mode == 0) {
+      const double sc = ep.want_force ? ep.G * ip.m[i] : ep.G;
+      ep.ax[i] = sc * ax[k]; ep.ay[i] = sc * ay[k]; ep.az[i] = sc * az[k];
+      continue;
+    }
+    const double gx = ep.G * ax[k], gy = ep.G * ay[k], gz = ep.G * az[k];
+    ep.ax[i] = gx; ep.ay[i] = gy; ep.az[i] = gz;
+    const double ux = ep.vx[i], uy = ep.vy[i], uz = ep.vz[i];
+    const double vx = ux + ep.kick * gx, vy = uy + ep.kick * gy, vz = uz + ep.kick * gz;
+    ep.vx[i] = vx; ep.vy[i] = vy; ep.vz[i] = vz;
+    const bool euler = ep.mode == 2;
+    ep.xn[i] = xi[k] + ep.drift * (euler ? ux : vx);
+    ep.yn[i] = yi[k] + ep.drift * (euler ? uy : vy);
+    ep.zn[i] = zi[k] + ep.drift * (euler ? uz : vz);
+  }
+}
+
 // --------------------------------------------------- kick / drift / pack ----
 // One warp per kTile particles (4 per lane).  ax == nullptr: no kick;
 // xn == nullptr: positions are not written (pack of x itself, drift ignored).
@@ -663,11 +883,31 @@ cudaError_t launch_f64_t(double eps2, int split, const IParticles& ip, const JSt
 }
 
 #define NBR_CFG_LIST(X) X(4, 2) X(4, 4) X(4, 8) X(8, 2) X(8, 4)
+#define NBR_SMALL_LIST(X) X(2) X(4) X(8)
+
+template <int PREC, int F>
+const void* small_fn(bool ex) {
+  return ex ? (const void*)k_force_small<PREC, F, true> : (const void*)k_force_small<PREC, F, false>;
+}
+
+template <int PREC, int F>
+cudaError_t launch_small_t(double eps2, int split, const IParticles& ip, const JStream& js,
+                           const Epilogue& ep, cudaStream_t st) {
+  const size_t smem = kSmemHead + (size_t)kStages * (PREC == kFP32C ? kStage32 : kStage64);
+  const long long chunk = 32LL * kSmallWarps * kSmallNI / F;
+  const dim3 grid((unsigned)((ip.n + chunk - 1) / chunk), (unsigned)split);
+  if (eps2 == 0.0)
+    k_force_small<PREC, F, true><<<grid, kSmallWarps * 32, smem, st>>>(ip, js, ep, eps2);
+  else
+    k_force_small<PREC, F, false><<<grid, kSmallWarps * 32, smem, st>>>(ip, js, ep, eps2);
+  return cudaGetLastError();
+}
 
 }  // namespace
 
 bool force_config_supported(int precision, const ForceConfig& c) {
   (void)precision;
+  if (c.ni == 1) return (c.warps == 2 || c.warps == 4 || c.warps == 8) && c.split >= 1;
 #define NBR_MATCH(a, b) if (c.ni == a && c.warps == b) return c.split >= 1;
   NBR_CFG_LIST(NBR_MATCH)
 #undef NBR_MATCH
@@ -678,6 +918,17 @@ int force_blocks_per_sm(int precision, double eps2, const ForceConfig& c) {
   int nb = 0;
   const size_t smem = force_smem_bytes(precision, c);
   const bool ex = (eps2 == 0.0);
+  if (c.ni == 1) {
+    const void* fn = nullptr;
+#define NBR_SOCC(f)                                                                        \
+  if (c.warps == f) fn = precision == kFP32C ? small_fn<kFP32C, f>(ex) : small_fn<kFP64, f>(ex);
+    NBR_SMALL_LIST(NBR_SOCC)
+#undef NBR_SOCC
+    if (!fn || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kSmallWarps * 32, smem) !=
+                   cudaSuccess)
+      nb = 0;
+    return nb;
+  }
 #define NBR_OCC(a, b)                                                                          \
   if (c.ni == a && c.warps == b) {                                                             \
     const void* fn = precision == kFP32C                                                       \
@@ -702,6 +953,15 @@ cudaError_t launch_force(int precision, double eps2, const ForceConfig& c, const
                          const JStream& js, const Epilogue& ep, cudaStream_t st) {
   if (ip.n <= 0 || js.ntiles <= 0) return cudaSuccess;
   const bool ex = (eps2 == 0.0);
+  if (c.ni == 1) {
+#define NBR_SGO(f)                                                                         \
+  if (c.warps == f)                                                                        \
+    return precision == kFP32C ? launch_small_t<kFP32C, f>(eps2, c.split, ip, js, ep, st)  \
+                               : launch_small_t<kFP64, f>(eps2, c.split, ip, js, ep, st);
+    NBR_SMALL_LIST(NBR_SGO)
+#undef NBR_SGO
+    return cudaErrorInvalidValue;
+  }
   if (precision == kFP32C) {
     const float e = (float)eps2;
 #define NBR_GO(a, b)                                                                       \

@@ -69,10 +69,21 @@ struct Epilogue {
 };
 
 struct ForceConfig {
-  int ni;      // receivers per thread (4 or 8)
-  int warps;   // warps per CTA (2, 4 or 8)
+  int ni;      // receivers per thread (4 or 8); 1 selects the small-N kernel
+  int warps;   // warps per CTA (2, 4 or 8); for the small-N kernel: lane groups F (2, 4, 8)
   int split;   // j-range splits (>= 1)
 };
+
+// The small-N kernel: kSmallWarps warps per CTA, kSmallNI receivers per lane,
+// F lane groups per warp sharing each tile's sources: 128 * kSmallNI / F
+// receivers per CTA.
+constexpr int kSmallWarps = 4;
+constexpr int kSmallNI = 4;
+// Receivers one CTA of a configuration covers.
+inline long long force_chunk(const ForceConfig& c) {
+  return c.ni == 1 ? 32LL * kSmallWarps * kSmallNI / (c.warps > 0 ? c.warps : 1)
+                   : 32LL * c.ni * c.warps;
+}
 
 // Host-side launchers (nbr_kernels.cu).
 cudaError_t launch_force(int precision, double eps2, const ForceConfig& cfg, const IParticles& ip,

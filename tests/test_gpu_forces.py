@@ -98,8 +98,9 @@ def test_every_kernel_configuration_agrees(ctx, nbr, oracle, prec):
     s = nbr.plummer(6000, 17)
     upload(ctx, s)
     ref = truth(oracle, s, 1e-6)
-    for ni, warps in ((4, 2), (4, 4), (4, 8), (8, 2), (8, 4)):
-        for split in (1, 3, 0):
+    # (1, F): the small-N warp-splitting kernel with F lane groups per warp
+    for ni, warps in ((4, 2), (4, 4), (4, 8), (8, 2), (8, 4), (1, 2), (1, 4), (1, 8)):
+        for split in (1, 3, 0, 47):
             ctx.set_force_config(prec, ni, warps, split)
             err = rel_err(ctx.forces(prec, eps2=1e-6), ref)
             if prec == FP64:
@@ -301,3 +302,32 @@ def test_potential_sizes_and_self_term(ctx, nbr, oracle, n):
         return
     np.testing.assert_allclose(phi, ref, rtol=1e-12)
     assert abs(U - 0.5 * float(np.dot(s["m"], ref))) <= 1e-12 * abs(U)
+
+
+@pytest.mark.parametrize("prec", [FP64, FP32C])
+def test_small_kernel_leapfrog_and_ranges(ctx, nbr, oracle, prec):
+    """The small-N kernel on the paths beyond nbr_forces: a KDK run (its
+    epilogue packs no FP32C records, so every step repacks them) and a
+    receiver range of the multi-GPU partition."""
+    n, eps2 = 1500, 1e-6
+    s = nbr.plummer(n, 21)
+    upload(ctx, s)
+    ctx.set_force_config(prec, 1, 8, 0)
+    try:
+        ctx.run(prec, 0, 2, 1e-3, 10, eps2=eps2)
+        got = ctx.download()
+        want = oracle.kdk(s, 1e-3, 10, eps2=eps2)
+        for k in ("x", "y", "z", "vx", "vy", "vz"):
+            assert np.abs(got[k] - want[k]).max() <= (1e-12 if prec == FP64 else 1e-6), k
+        upload(ctx, s)
+        v0 = {k: s[k].copy() for k in ("vx", "vy", "vz")}
+        ctx.step_range(prec, 0, 256, 700, 1.0, 0.0, 1.0, eps2)  # v += a on [256, 956)
+        ctx.synchronize()
+        st = ctx.state_tensors()
+        dv = np.stack([st[k][:n].cpu().numpy() - v0[k] for k in ("vx", "vy", "vz")])
+        ref = truth(oracle, s, eps2)
+        e = rel_err(dv[:, 256:956], ref[:, 256:956])
+        assert (e.max() <= 1e-12) if prec == FP64 else (np.median(e) <= 1e-6)
+        assert not dv[:, :256].any() and not dv[:, 956:].any()
+    finally:
+        ctx.set_force_config(prec, 0)
