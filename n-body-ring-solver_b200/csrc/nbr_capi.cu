@@ -320,6 +320,9 @@ ForceConfig choose_config(nbr_ctx* c, int precision, double eps2, long long n_i,
     const int F = precision == kFP32C ? (n_i <= 4096 ? 8 : n_i <= 8192 ? 2 : 0)
                                       : (n_i <= 16384 ? 8 : n_i <= 32768 ? 4 : 0);
     if (F) dflt = ForceConfig{1, F, 0};
+    // FP32C from 16384 to 2^20 particles: the Newton-3 kernel (+24 % at
+    // N = 262144, +28 % at 2^20 on B200).
+    else if (precision == kFP32C && n_i >= kN3MinN && n_i <= kN3MaxN) dflt = ForceConfig{3, kN3Warps, 0};
     cfg = it != g_tune->end() ? it->second : dflt;
   }
   if (cfg.split <= 0) cfg.split = auto_split(precision, eps2, cfg, n_i, ntiles, c->sms);
@@ -327,8 +330,22 @@ ForceConfig choose_config(nbr_ctx* c, int precision, double eps2, long long n_i,
   return cfg;
 }
 
+// The large-kernel default for callers that cannot take the Newton-3 kernel
+// (a receiver range, separate receiver and source sets).
+ForceConfig choose_config_large(nbr_ctx* c, int precision, double eps2, long long n_i, int ntiles) {
+  ForceConfig cfg = precision == kFP32C ? ForceConfig{8, 2, 0} : ForceConfig{4, 4, 0};
+  cfg.split = std::max(1, std::min(auto_split(precision, eps2, cfg, n_i, ntiles, c->sms), ntiles));
+  return cfg;
+}
+
 // Prepares scratch for a force launch of `cfg` over n_i receivers.
 int prepare_split(nbr_ctx* c, const ForceConfig& cfg, long long n_pad_i) {
+  if (cfg.ni == 3) {  // Newton-3 (the context's whole system only): its own partial sums
+    (void)n_pad_i;
+    const long long nb = ((long long)c->sys.n + kN3Block - 1) / kN3Block;
+    cudaError_t e = c->scr.need_part((size_t)n3_scratch_doubles(nb));
+    return e == cudaSuccess ? NBR_OK : cuda_fail(c, e, "Newton-3 scratch");
+  }
   if (cfg.split <= 1) return NBR_OK;
   cudaError_t e = c->scr.need_part((size_t)cfg.split * 3 * (size_t)n_pad_i);
   if (e == cudaSuccess) e = c->scr.need_counters((size_t)(n_pad_i / 64 + 1));
@@ -404,6 +421,8 @@ int eval_system(nbr_ctx* c, int precision, double G, double eps2, int mode, doub
   if (precision == kFP32C) e = ensure_records(c, a, kernels);
   if (e != cudaSuccess) return cuda_fail(c, e, "pack");
   ForceConfig cfg = choose_config(c, precision, eps2, rn, s.ntiles);
+  if (cfg.ni == 3 && (ranged || precision != kFP32C || rn > kN3MaxN))  // needs the whole system
+    cfg = choose_config_large(c, precision, eps2, rn, s.ntiles);
   int rc = prepare_split(c, cfg, np_i);
   if (rc) return rc;
   IParticles ip{s.pos[a][0] + r0, s.pos[a][1] + r0, s.pos[a][2] + r0, s.mass + r0, rn};
@@ -431,8 +450,13 @@ int eval_system(nbr_ctx* c, int precision, double G, double eps2, int mode, doub
       ep.rec_len = (long long)s.cap;
       // test hook: under-report the receivers' length so that the check trips
       if (std::getenv("NBR_TEST_SHRINK_BOUNDS")) ip.len = rn - 1;)
-  e = launch_force(precision, eps2, cfg, ip, js, ep, c->stream);
-  if (kernels) ++*kernels;
+  if (cfg.ni == 3) {
+    e = launch_force_n3(eps2, ip, js, ep, c->scr.part, (long long)c->scr.part_cap, c->stream);
+    if (kernels) *kernels += 2;
+  } else {
+    e = launch_force(precision, eps2, cfg, ip, js, ep, c->stream);
+    if (kernels) ++*kernels;
+  }
   if (e != cudaSuccess) return cuda_fail(c, e, "force launch");
   if (mode != 0) {
     s.cur = b;
@@ -606,6 +630,7 @@ int nbr_ctx_create(int device, nbr_ctx** out) {
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
   if (e == cudaSuccess) e = dalloc((void**)&c->d_err, sizeof(int) * 4);
+  if (e == cudaSuccess) e = configure_kernels();
   if (e != cudaSuccess) {
     int rc = cuda_fail(nullptr, e, "context setup");
     nbr_ctx_destroy(c);
@@ -875,6 +900,7 @@ int nbr_accel_ij(nbr_ctx* c, int precision, size_t n_i, const double* xi, const 
     if (e != cudaSuccess) return cuda_fail(c, e, "ij pack");
   }
   ForceConfig cfg = choose_config(c, precision, eps2, (long long)n_i, ntiles);
+  if (cfg.ni == 3) cfg = choose_config_large(c, precision, eps2, (long long)n_i, ntiles);
   int rc = prepare_split(c, cfg, npi);
   if (rc) return rc;
   IParticles ip{r.pos[0][0], r.pos[0][1], r.pos[0][2], r.mass, (long long)n_i};
@@ -1131,11 +1157,12 @@ int nbr_autotune(nbr_ctx* c, int precision, double eps2) {
   if (s.n == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no system uploaded");
   cudaSetDevice(c->device);
   const ForceConfig saved = c->override_cfg[precision];
-  const int cand[][2] = {{4, 2}, {4, 4}, {4, 8}, {8, 2}, {8, 4}, {1, 2}, {1, 4}, {1, 8}};
+  const int cand[][2] = {{4, 2}, {4, 4}, {4, 8}, {8, 2}, {8, 4}, {1, 2}, {1, 4}, {1, 8}, {3, 8}};
   ForceConfig best{0, 0, 0};
   float best_ms = 1e30f;
   for (auto& cw : cand) {
     if (cw[0] == 1 && s.n > 65536) continue;  // the small-N kernel only competes on small systems
+    if (cw[0] == 3 && (precision != kFP32C || s.n < 8192 || (long long)s.n > kN3MaxN)) continue;
     ForceConfig base{cw[0], cw[1], 1};
     const int s0 = auto_split(precision, eps2, base, (long long)s.n, s.ntiles, c->sms);
     const int splits[] = {std::max(1, s0 / 2), s0, s0 * 2};

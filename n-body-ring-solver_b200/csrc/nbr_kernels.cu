@@ -631,6 +631,295 @@ __global__ void __launch_bounds__(kSmallWarps * 32)
   }
 }
 
+// ------------------------------------------ Newton-3 FP32C force kernel ----
+// Every unordered pair is evaluated once and acts on both particles, as the
+// reference's blocked kernels do (compute_forces_avx512_rsqrt_4i_blocked
+// applies +f to the receiver and -f to the source, CPU/force_calculation.cpp:
+// 1137-1561).  Particles form blocks of kN3Block = 256 (2 tiles).  A CTA of
+// kN3Warps warps owns row group g (row blocks 8g .. 8g+7, one per warp, 8
+// receivers per lane as in k_force_f32c) and a chunk of up to p3.cols column
+// blocks starting at the group's first block (n3_cols: 32, fewer on small
+// systems); the column tiles stream through the bulk-copy ring.  Warp a and column block c:
+//   c < a   nothing (the pair of blocks belongs to warp c);
+//   c == a  every ordered pair of the block, action only (the k_force_f32c body);
+//   c > a   each unordered pair once: the 32 sources of a batch sit one per
+//           lane and rotate through the warp with shuffles, carrying their
+//           reaction sums, so after 32 steps every source has met all 256
+//           receivers of the warp and holds its reaction from them.
+// Per unordered pair: the 14 FMA-pipe operations of k_force_f32c plus 5 for
+// the reaction (receiver-mass correction, its product, 3 accumulations), and
+// one MUFU rsqrt: 9.5 operations per ordered pair instead of 14.
+// Results leave as FP64 partial sums: per (CTA, row block) the action, per
+// (CTA, column block) the reaction (summed over the CTA's warps in warp
+// order); k_n3_reduce adds them per particle in a fixed order and runs the
+// epilogue.  Deterministic.
+template <bool EXCL>
+__global__ void __launch_bounds__(kN3Warps * 32)
+    k_force_n3_f32c(const IParticles ip, const JStream js, const N3Params p3, const float eps2f,
+                    int* err) {
+  constexpr int NI = 8, IPAIR = 4;
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
+  unsigned char* stages = smem + kSmemHead;
+  float* red = reinterpret_cast<float*>(stages + kStages * kStage32);  // [warp][3][256]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int g = 0, k = blockIdx.x;
+  const int groups = (int)((p3.nb + kN3Warps - 1) / kN3Warps);
+  while (g < groups) {  // the grid has exactly sum_g n3_chunks(nb, cols, g) CTAs
+    const int K = n3_chunks(p3.nb, p3.cols, g);
+    if (k < K) break;
+    k -= K;
+    ++g;
+  }
+  if (g >= groups) return;
+  const long long r0 = (long long)g * kN3Warps;
+  const long long a = r0 + warp;
+  const long long cs = r0 + (long long)k * p3.cols;
+  const long long ce = min(cs + (long long)p3.cols, p3.nb);
+  const int ntl = (int)(2 * (ce - cs));
+  const bool row_ok = a < p3.nb;
+  const long long ibase = a * kN3Block + lane;
+
+  double xi[NI], yi[NI], zi[NI];
+  u64 AI[IPAIR], BI[IPAIR];
+#pragma unroll
+  for (int q = 0; q < NI; ++q) xi[q] = yi[q] = zi[q] = 0.0;
+#pragma unroll
+  for (int p = 0; p < IPAIR; ++p) {
+    float m0 = 0.f, m1 = 0.f;
+    if (row_ok) {
+      const long long i0 = ibase + 64 * p, i1 = i0 + 32;
+      if (NBR_IN(i1, ip.len, err)) {
+        xi[2 * p] = ip.x[i0]; yi[2 * p] = ip.y[i0]; zi[2 * p] = ip.z[i0];
+        xi[2 * p + 1] = ip.x[i1]; yi[2 * p + 1] = ip.y[i1]; zi[2 * p + 1] = ip.z[i1];
+        m0 = (float)ip.m[i0];
+        m1 = (float)ip.m[i1];
+      }
+    }
+    AI[p] = pack2(-1.5f * m0, -1.5f * m1);
+    BI[p] = pack2(2.5f * m0, 2.5f * m1);
+  }
+  u64 hx[IPAIR], hy[IPAIR], hz[IPAIR], lx[IPAIR], ly[IPAIR], lz[IPAIR];
+#pragma unroll
+  for (int p = 0; p < IPAIR; ++p) hx[p] = hy[p] = hz[p] = lx[p] = ly[p] = lz[p] = 0ull;
+  const u64 EPS2 = pack2(eps2f, eps2f);
+
+  auto issue = [&](int st, int t) {
+    unsigned char* dst = stages + st * kStage32;
+    const uint32_t bar = smem_u32(&bars[st]);
+    const long long tile = 2 * cs + t;
+    if (!NBR_IN((tile + 1) * kTile - 1, js.len, err)) return;  // the wait expires
+    mbar_expect_tx(bar, kStage32);
+    bulk_g2s(dst, js.rec + (size_t)tile * kTile * 3, kRecBytes, bar);
+    bulk_g2s(dst + kRecBytes, js.origin + tile, 32, bar);
+  };
+  int tcur = 0;
+  auto body = [&](int st) {
+    const int t = tcur++;
+    const long long c = cs + t / 2;
+    const int half = t & 1;
+    const unsigned char* base = stages + st * kStage32;
+    const double4 o = *reinterpret_cast<const double4*>(base + kRecBytes);
+    u64 XI[IPAIR], YI[IPAIR], ZI[IPAIR], AX[IPAIR], AY[IPAIR], AZ[IPAIR];
+#pragma unroll
+    for (int p = 0; p < IPAIR; ++p) {
+      // pair p: receivers 2p (lane + 64p) and 2p + 1 (lane + 64p + 32)
+      XI[p] = pack2(__double2float_rn(xi[2 * p] - o.x), __double2float_rn(xi[2 * p + 1] - o.x));
+      YI[p] = pack2(__double2float_rn(yi[2 * p] - o.y), __double2float_rn(yi[2 * p + 1] - o.y));
+      ZI[p] = pack2(__double2float_rn(zi[2 * p] - o.z), __double2float_rn(zi[2 * p + 1] - o.z));
+      AX[p] = AY[p] = AZ[p] = 0ull;
+    }
+    float* myred = red + warp * 3 * kN3Block + half * kTile;
+    if (row_ok && c == a) {
+      const ulonglong2* R = reinterpret_cast<const ulonglong2*>(base);
+#pragma unroll 4
+      for (int j = 0; j < kTile; ++j) {
+        const ulonglong2 q0 = R[3 * j];
+        const ulonglong2 q1 = R[3 * j + 1];
+        const u64 bj = R[3 * j + 2].x;
+#pragma unroll
+        for (int p = 0; p < IPAIR; ++p) {
+          const u64 dx = sub2(q0.x, XI[p]);
+          const u64 dy = sub2(q0.y, YI[p]);
+          const u64 dz = sub2(q1.x, ZI[p]);
+          u64 r2 = fma2(dx, dx, EPS2);
+          r2 = fma2(dy, dy, r2);
+          r2 = fma2(dz, dz, r2);
+          u64 y;
+          if (EXCL) {
+            float rl, rh;
+            unpack2(r2, rl, rh);
+            y = pack2(rl > 0.f ? rsqrt_mufu(rl) : 0.f, rh > 0.f ? rsqrt_mufu(rh) : 0.f);
+          } else {
+            y = rsqrt2(r2);
+          }
+          const u64 y2 = mul2(y, y);
+          const u64 pr = mul2(r2, y2);
+          const u64 mg = fma2(q1.y, pr, bj);
+          const u64 y3 = mul2(y2, y);
+          const u64 s = mul2(y3, mg);
+          AX[p] = fma2(s, dx, AX[p]);
+          AY[p] = fma2(s, dy, AY[p]);
+          AZ[p] = fma2(s, dz, AZ[p]);
+        }
+      }
+#pragma unroll
+      for (int bt = 0; bt < 4; ++bt)
+        myred[bt * 32 + lane] = myred[kN3Block + bt * 32 + lane] = myred[2 * kN3Block + bt * 32 + lane] = 0.f;
+    } else if (row_ok && c > a) {
+      const float4* R4 = reinterpret_cast<const float4*>(base);
+      const int from = (lane + 31) & 31;
+#pragma unroll 1
+      for (int bt = 0; bt < 4; ++bt) {
+        const int j = bt * 32 + lane;
+        const float4 q0 = R4[3 * j], q1 = R4[3 * j + 1], q2 = R4[3 * j + 2];
+        float sx = q0.x, sy = q0.z, sz = q1.x, sa = q1.z, sb = q2.x;
+        u64 RX = 0ull, RY = 0ull, RZ = 0ull;
+#pragma unroll 2
+        for (int step = 0; step < 32; ++step) {
+          const u64 SX = pack2(sx, sx), SY = pack2(sy, sy), SZ = pack2(sz, sz);
+          const u64 SA = pack2(sa, sa), SB = pack2(sb, sb);
+#pragma unroll
+          for (int p = 0; p < IPAIR; ++p) {
+            const u64 dx = sub2(SX, XI[p]);
+            const u64 dy = sub2(SY, YI[p]);
+            const u64 dz = sub2(SZ, ZI[p]);
+            u64 r2 = fma2(dx, dx, EPS2);
+            r2 = fma2(dy, dy, r2);
+            r2 = fma2(dz, dz, r2);
+            u64 y;
+            if (EXCL) {
+              float rl, rh;
+              unpack2(r2, rl, rh);
+              y = pack2(rl > 0.f ? rsqrt_mufu(rl) : 0.f, rh > 0.f ? rsqrt_mufu(rh) : 0.f);
+            } else {
+              y = rsqrt2(r2);
+            }
+            const u64 y2 = mul2(y, y);
+            const u64 pr = mul2(r2, y2);
+            const u64 y3 = mul2(y2, y);
+            const u64 sj = mul2(y3, fma2(SA, pr, SB));  // m_j (1 + 3e/2) y^3
+            const u64 si = mul2(y3, fma2(AI[p], pr, BI[p]));  // m_i (1 + 3e/2) y^3
+            AX[p] = fma2(sj, dx, AX[p]);
+            AY[p] = fma2(sj, dy, AY[p]);
+            AZ[p] = fma2(sj, dz, AZ[p]);
+            RX = fma2(si, dx, RX);
+            RY = fma2(si, dy, RY);
+            RZ = fma2(si, dz, RZ);
+          }
+          sx = __shfl_sync(0xffffffffu, sx, from);
+          sy = __shfl_sync(0xffffffffu, sy, from);
+          sz = __shfl_sync(0xffffffffu, sz, from);
+          sa = __shfl_sync(0xffffffffu, sa, from);
+          sb = __shfl_sync(0xffffffffu, sb, from);
+          RX = __shfl_sync(0xffffffffu, RX, from);
+          RY = __shfl_sync(0xffffffffu, RY, from);
+          RZ = __shfl_sync(0xffffffffu, RZ, from);
+        }
+        // back at its own lane: the force on source j is -sum s_i d
+        float u0, u1;
+        unpack2(RX, u0, u1); myred[bt * 32 + lane] = -(u0 + u1);
+        unpack2(RY, u0, u1); myred[kN3Block + bt * 32 + lane] = -(u0 + u1);
+        unpack2(RZ, u0, u1); myred[2 * kN3Block + bt * 32 + lane] = -(u0 + u1);
+      }
+    } else {
+#pragma unroll
+      for (int bt = 0; bt < 4; ++bt)
+        myred[bt * 32 + lane] = myred[kN3Block + bt * 32 + lane] = myred[2 * kN3Block + bt * 32 + lane] = 0.f;
+    }
+#pragma unroll
+    for (int p = 0; p < IPAIR; ++p) {
+      two_sum2(hx[p], lx[p], AX[p]);
+      two_sum2(hy[p], ly[p], AY[p]);
+      two_sum2(hz[p], lz[p], AZ[p]);
+    }
+    if (half == 1) {
+      // end of column block c: its reaction from this CTA's rows, summed in
+      // warp order in FP64, to the block's partial slot
+      __syncthreads();
+      const int tid = threadIdx.x;  // one source of the block per thread
+      const long long off = ((long long)blockIdx.x * p3.cols + (c - cs)) * 3 * kN3Block;
+      double* out = p3.rea + off;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        double s = 0.0;
+        for (int w = 0; w < kN3Warps; ++w) s += (double)red[(w * 3 + d) * kN3Block + tid];
+        if (NBR_IN((p3.rea - p3.act) + off + d * kN3Block + tid, p3.act_len, err))
+          out[d * kN3Block + tid] = s;
+      }
+      __syncthreads();
+    }
+  };
+  if (!tile_pipeline(bars, ntl, js, err, issue, body)) return;
+  double* act = p3.act + ((size_t)blockIdx.x * kN3Warps + warp) * 3 * kN3Block;
+  if (!NBR_IN(((long long)blockIdx.x * kN3Warps + warp + 1) * 3 * kN3Block - 1, p3.act_len, err))
+    return;
+#pragma unroll
+  for (int p = 0; p < IPAIR; ++p) {
+    float h0, h1, l0, l1;
+    unpack2(hx[p], h0, h1); unpack2(lx[p], l0, l1);
+    act[lane + 64 * p] = (double)h0 + (double)l0;
+    act[lane + 64 * p + 32] = (double)h1 + (double)l1;
+    unpack2(hy[p], h0, h1); unpack2(ly[p], l0, l1);
+    act[kN3Block + lane + 64 * p] = (double)h0 + (double)l0;
+    act[kN3Block + lane + 64 * p + 32] = (double)h1 + (double)l1;
+    unpack2(hz[p], h0, h1); unpack2(lz[p], l0, l1);
+    act[2 * kN3Block + lane + 64 * p] = (double)h0 + (double)l0;
+    act[2 * kN3Block + lane + 64 * p + 32] = (double)h1 + (double)l1;
+  }
+}
+
+// Adds the Newton-3 partial sums of each particle in a fixed order (its row
+// group's chunks, then the reactions from row groups 0 .. its own) and runs the
+// epilogue of the large kernels.  One warp per 128-particle tile.
+__global__ void __launch_bounds__(128)
+    k_n3_reduce(const IParticles ip, const Epilogue ep, const N3Params p3) {
+  const int lane = threadIdx.x & 31;
+  const long long tile = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (tile * kTile >= p3.nb * kN3Block) return;
+  const long long b = tile / 2;                   // block of the tile
+  const int g = (int)(b / kN3Warps), w = (int)(b % kN3Warps);
+  const int jb0 = (int)(tile & 1) * kTile + lane;  // particle index inside the block (k = 0)
+  double ax[4] = {0, 0, 0, 0}, ay[4] = {0, 0, 0, 0}, az[4] = {0, 0, 0, 0};
+  long long prefix = 0;  // CTAs of row groups before g'
+  for (int gp = 0; gp <= g; ++gp) {
+    const int K = n3_chunks(p3.nb, p3.cols, gp);
+    if (gp == g) {
+      for (int k = 0; k < K; ++k) {
+        const double* A = p3.act + ((size_t)(prefix + k) * kN3Warps + w) * 3 * kN3Block;
+        if (!NBR_IN((A - p3.act) + 3 * kN3Block - 1, p3.act_len, ep.err)) continue;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int jb = jb0 + 32 * q;
+          ax[q] += A[jb]; ay[q] += A[kN3Block + jb]; az[q] += A[2 * kN3Block + jb];
+        }
+      }
+    }
+    const long long cs0 = (long long)gp * kN3Warps;
+    const int kk = (int)((b - cs0) / p3.cols);
+    const int col = (int)(b - (cs0 + (long long)kk * p3.cols));
+    const double* Rr = p3.rea + ((size_t)(prefix + kk) * p3.cols + col) * 3 * kN3Block;
+    if (!NBR_IN((Rr - p3.act) + 3 * kN3Block - 1, p3.act_len, ep.err)) {
+      prefix += K;
+      continue;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int jb = jb0 + 32 * q;
+      ax[q] += Rr[jb]; ay[q] += Rr[kN3Block + jb]; az[q] += Rr[2 * kN3Block + jb];
+    }
+    prefix += K;
+  }
+  const long long ibase = tile * kTile + lane;
+  double xi[4], yi[4], zi[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const long long i = ibase + 32 * q;
+    xi[q] = ip.x[i]; yi[q] = ip.y[i]; zi[q] = ip.z[i];
+  }
+  epilogue<4>(ip, ep, ibase, lane, xi, yi, zi, ax, ay, az);
+}
+
 // --------------------------------------------------- kick / drift / pack ----
 // One warp per kTile particles (4 per lane).  ax == nullptr: no kick;
 // xn == nullptr: positions are not written (pack of x itself, drift ignored).
@@ -905,8 +1194,10 @@ cudaError_t launch_small_t(double eps2, int split, const IParticles& ip, const J
 
 }  // namespace
 
+size_t n3_smem_bytes();
+
 bool force_config_supported(int precision, const ForceConfig& c) {
-  (void)precision;
+  if (c.ni == 3) return precision == kFP32C && c.warps == kN3Warps;  // Newton-3 (FP32C only)
   if (c.ni == 1) return (c.warps == 2 || c.warps == 4 || c.warps == 8) && c.split >= 1;
 #define NBR_MATCH(a, b) if (c.ni == a && c.warps == b) return c.split >= 1;
   NBR_CFG_LIST(NBR_MATCH)
@@ -916,6 +1207,13 @@ bool force_config_supported(int precision, const ForceConfig& c) {
 
 int force_blocks_per_sm(int precision, double eps2, const ForceConfig& c) {
   int nb = 0;
+  if (c.ni == 3) {
+    const void* fn = eps2 == 0.0 ? (const void*)k_force_n3_f32c<true> : (const void*)k_force_n3_f32c<false>;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kN3Warps * 32, n3_smem_bytes()) !=
+        cudaSuccess)
+      nb = 0;
+    return nb;
+  }
   const size_t smem = force_smem_bytes(precision, c);
   const bool ex = (eps2 == 0.0);
   if (c.ni == 1) {
@@ -979,6 +1277,48 @@ cudaError_t launch_force(int precision, double eps2, const ForceConfig& c, const
 #undef NBR_GO
   }
   return cudaErrorInvalidValue;
+}
+
+size_t n3_smem_bytes() {
+  return kSmemHead + (size_t)kStages * kStage32 + (size_t)kN3Warps * 3 * kN3Block * sizeof(float);
+}
+
+cudaError_t configure_kernels() {
+  // The Newton-3 kernel needs more than the default 48 KB of dynamic shared
+  // memory; set once per device, outside any stream capture.
+  const int smem = (int)n3_smem_bytes();
+  cudaError_t e = cudaFuncSetAttribute((const void*)k_force_n3_f32c<true>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)k_force_n3_f32c<false>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  return e;
+}
+
+cudaError_t launch_force_n3(double eps2, const IParticles& ip, const JStream& js,
+                            const Epilogue& ep, double* scratch, long long scratch_len,
+                            cudaStream_t st) {
+  (void)scratch_len;
+  if (ip.n <= 0 || js.ntiles <= 0) return cudaSuccess;
+  N3Params p3;
+  p3.nb = (ip.n + kN3Block - 1) / kN3Block;
+  p3.cols = n3_cols(p3.nb);
+  const long long ctas = n3_ctas(p3.nb, p3.cols);
+  if (ctas > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+  p3.act = scratch;
+  p3.rea = scratch + (size_t)ctas * kN3Warps * 3 * kN3Block;
+  NBR_CHECKED_ONLY(p3.act_len = scratch_len;)
+  const size_t smem = n3_smem_bytes();
+  if (eps2 == 0.0)
+    k_force_n3_f32c<true><<<(unsigned)ctas, kN3Warps * 32, smem, st>>>(ip, js, p3, 0.f, ep.err);
+  else
+    k_force_n3_f32c<false><<<(unsigned)ctas, kN3Warps * 32, smem, st>>>(ip, js, p3, (float)eps2,
+                                                                       ep.err);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const long long threads = p3.nb * 2 * 32;  // a warp per tile
+  k_n3_reduce<<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(ip, ep, p3);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_kick_drift(long long n, long long n_pad, const double* x, const double* y,

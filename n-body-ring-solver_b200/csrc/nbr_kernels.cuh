@@ -79,6 +79,55 @@ struct ForceConfig {
 // receivers per CTA.
 constexpr int kSmallWarps = 4;
 constexpr int kSmallNI = 4;
+// The Newton-3 FP32C kernel (ForceConfig ni = 3): blocks of kN3Block
+// particles, kN3Warps row blocks per CTA (one per warp), up to `cols` column
+// blocks per CTA (n3_cols: fewer on small systems, for enough CTAs).
+constexpr int kN3Warps = 8;
+constexpr int kN3Block = 256;
+constexpr int kN3MaxCols = 32;
+struct N3Params {
+  long long nb;  // blocks holding real particles: ceil(n / kN3Block)
+  int cols;      // column blocks per CTA
+  double* act;   // action partials [cta][row block][3][kN3Block]
+  double* rea;   // reaction partials [cta][column block][3][kN3Block]
+  NBR_CHECKED_FIELD(long long act_len)  // doubles from act (through rea's end)
+};
+// Largest system the Newton-3 kernel takes: its partial sums grow as N^2
+// (8.4 GB at 2^20 particles).
+constexpr long long kN3MaxN = 1LL << 20;
+// Smallest system the default configuration gives the Newton-3 kernel.
+constexpr long long kN3MinN = 16384;
+// Column chunks (CTAs) of row group g.
+__host__ __device__ inline int n3_chunks(long long nb, int cols, int g) {
+  const long long left = nb - (long long)g * kN3Warps;
+  return left <= 0 ? 0 : (int)((left + cols - 1) / cols);
+}
+// Column blocks per CTA: kN3MaxCols, or fewer so that a small system still
+// gets about 600 CTAs (4 waves of one CTA per SM).
+inline int n3_cols(long long nb) {
+  const long long c = nb * nb / (16LL * 600);
+  return (int)(c < 1 ? 1 : c > kN3MaxCols ? kN3MaxCols : c);
+}
+// CTAs of a Newton-3 launch and the doubles its partial sums need.
+inline long long n3_ctas(long long nb, int cols) {
+  long long t = 0;
+  for (int g = 0; (long long)g * kN3Warps < nb; ++g) t += n3_chunks(nb, cols, g);
+  return t;
+}
+inline long long n3_scratch_doubles(long long nb) {
+  const int cols = n3_cols(nb);
+  return n3_ctas(nb, cols) * (long long)(kN3Warps + cols) * 3 * kN3Block;
+}
+// One Newton-3 force evaluation (FP32C) over all n_pad receivers of ip
+// against the same particles' records in js, with the epilogue ep:
+// the pair kernel, then the per-particle reduction.  scratch holds
+// n3_scratch_doubles(ceil(n / kN3Block)) doubles.
+cudaError_t launch_force_n3(double eps2, const IParticles& ip, const JStream& js,
+                            const Epilogue& ep, double* scratch, long long scratch_len,
+                            cudaStream_t stream);
+// Kernel attributes that must be set once per device, outside stream capture.
+cudaError_t configure_kernels();
+
 // Receivers one CTA of a configuration covers.
 inline long long force_chunk(const ForceConfig& c) {
   return c.ni == 1 ? 32LL * kSmallWarps * kSmallNI / (c.warps > 0 ? c.warps : 1)

