@@ -40,6 +40,10 @@ METRIC = "GPairs/s FP32-compensated vs FP64 on 1 B200 at median force rel err <=
 UNIT = "GPairs/s"
 SMS = 148
 FMA_OPS_PER_PAIR = 16
+# The Newton-3 kernel evaluates each unordered pair once: the 16 operations of
+# the pair plus 5 for the reaction (receiver-mass correction, its product, 3
+# accumulations), i.e. 10.5 per ordered pair of the N(N-1) the metric counts.
+REACTION_OPS = 5
 PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "force_fp32c_plummer262144.json")
 
 
@@ -340,15 +344,23 @@ def run_ours(a):
     t_k = statistics.mean(k32)
     achieved = pairs / t_k / 1e9
     mhz = clk.get("sm_mhz") or 1965.0
-    peak = SMS * 128 * mhz * 1e6 / FMA_OPS_PER_PAIR / 1e9
+    cfg = ctx.get_force_config(nbr.FP32C, eps2)
+    newton3 = cfg[0] == 3
+    ops = (FMA_OPS_PER_PAIR + REACTION_OPS) / 2 if newton3 else FMA_OPS_PER_PAIR
+    peak = SMS * 128 * mhz * 1e6 / ops / 1e9
     roofline = {"bound": "fp32_fma_pipe", "achieved": achieved, "peak": peak, "unit": UNIT,
                 "frac": achieved / peak, "traffic": profile_traffic(),
                 "algorithmic_bytes": 96 * n,
-                "traffic_note": "dram bytes per launch from profiles/force_fp32c_plummer262144.json; "
-                                "402 MB of it are the split partial sums (written and read once)",
-                "peak_source": "148 SMs x 128 FP32 lanes x median SM clock sampled in the timed region "
-                               "/ 16 FMA-pipe ops per pair (MEASURED_PEAKS.json has no FP32-pipe figure)",
-                "frac_at_max_clock": achieved / (SMS * 128 * 1965e6 / FMA_OPS_PER_PAIR / 1e9),
+                "kernel": ("k_force_n3_f32c + k_n3_reduce (Newton-3: each unordered pair evaluated once)"
+                           if newton3 else f"k_force_f32c<{cfg[0]},{cfg[1]}> split {cfg[2]}"),
+                "fma_ops_per_ordered_pair": ops,
+                "traffic_note": "dram bytes per launch of the pair kernel from "
+                                "profiles/force_fp32c_plummer262144.json",
+                "peak_source": f"148 SMs x 128 FP32 lanes x median SM clock sampled in the timed region "
+                               f"/ {ops:g} FMA-pipe ops per ordered pair (MEASURED_PEAKS.json has no "
+                               "FP32-pipe figure)",
+                "frac_at_max_clock": achieved / (SMS * 128 * 1965e6 / ops / 1e9),
+                "frac_of_16op_roofline": achieved / (SMS * 128 * mhz * 1e6 / FMA_OPS_PER_PAIR / 1e9),
                 "kernel_ms": 1e3 * t_k, "mufu_peak": SMS * 16 * mhz * 1e6 / 1e9}
     traffic = roofline["traffic"]
     hbm_peak, hbm_src = measured_hbm_gbs()

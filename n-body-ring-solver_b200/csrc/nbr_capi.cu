@@ -1142,6 +1142,22 @@ int nbr_set_force_config(nbr_ctx* c, int precision, int ni, int warps, int split
   return NBR_OK;
 }
 
+int nbr_get_force_config(nbr_ctx* c, int precision, double eps2, int* ni, int* warps, int* split) {
+  if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
+  if (precision != NBR_FP64 && precision != NBR_FP32C)
+    return fail(c, NBR_ERR_INVALID_ARG, "unknown precision");
+  SysState& s = c->sys;
+  if (s.n == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no system uploaded");
+  cudaSetDevice(c->device);
+  ForceConfig cfg = choose_config(c, precision, eps2, (long long)s.n, s.ntiles);
+  if (cfg.ni == 3 && (precision != kFP32C || (long long)s.n > kN3MaxN))
+    cfg = choose_config_large(c, precision, eps2, (long long)s.n, s.ntiles);
+  if (ni) *ni = cfg.ni;
+  if (warps) *warps = cfg.warps;
+  if (split) *split = cfg.split;
+  return NBR_OK;
+}
+
 const char* nbr_tune_cache_path(void) {
   std::lock_guard<std::mutex> g(g_tune_mu);
   load_tune_locked();

@@ -87,6 +87,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
                      C.POINTER(Diag), C.POINTER(RunStats)], C.c_int),
         "nbr_yoshida_coefficients": ([C.c_int, _D, _D], C.c_int),
         "nbr_set_force_config": ([C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
+        "nbr_get_force_config": ([C.c_void_p, C.c_int, C.c_double] + [C.POINTER(C.c_int)] * 3, C.c_int),
         "nbr_autotune": ([C.c_void_p, C.c_int, C.c_double], C.c_int),
         "nbr_tune_cache_path": ([], C.c_char_p),
         "nbr_ic_plummer": ([_SZ, _U64] + [_D] * 7, C.c_int),
@@ -416,6 +417,12 @@ class Context:
 
     def set_force_config(self, precision, ni=0, warps=0, split=0):
         self._chk(self.L.nbr_set_force_config(self.h, precision, ni, warps, split), "set_force_config")
+
+    def get_force_config(self, precision, eps2=0.0):
+        v = [C.c_int() for _ in range(3)]
+        self._chk(self.L.nbr_get_force_config(self.h, precision, eps2, *[C.byref(x) for x in v]),
+                  "get_force_config")
+        return tuple(x.value for x in v)
 
     def autotune(self, precision, eps2):
         self._chk(self.L.nbr_autotune(self.h, precision, eps2), "autotune")
