@@ -384,7 +384,8 @@ def run_ours(a):
             cpu = {"error": str(ex)}
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": 1e3 * t_total / a.steps, "higher_is_better": True,
+            "warmup": a.warmup, "ms_per_step": 1e3 * t_total / a.steps,
+            "steps_per_s": a.steps / t_total, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f32" if prec == nbr.FP32C else "f64",
             "data": "synthetic", "config": workload_config(a, {"precision": a.precision}),
             "gpu_launches": launches, "wall_s_timed": t_wall,
