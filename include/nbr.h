@@ -264,13 +264,16 @@ int nbr_snapshot_load(nbr_ctx* ctx, const char* path, size_t n, size_t record, d
 /* Forces a kernel configuration for the given precision (ni receivers per
  * thread: 4 or 8; warps per CTA: 2, 4 or 8; split >= 1 or 0 = automatic;
  * ni = 1: the small-N kernel with warps = 2, 4 or 8 lane groups per warp;
- * ni = 3, warps = 8: the Newton-3 FP32C kernel).  ni = 0 restores the
- * autotuner. */
+ * ni = 3, warps = 8: the Newton-3 kernel, each unordered pair evaluated once
+ * and applied to both particles, for FP32C and for FP64; whole systems of at
+ * most 2^20 particles, other calls fall back to the large kernels).  ni = 0
+ * restores the autotuner. */
 int nbr_set_force_config(nbr_ctx* ctx, int precision, int ni, int warps, int split);
 /* The configuration a force evaluation of the uploaded system would use
  * (forced, autotuned or default): ni = 4 or 8 receivers per thread of the
  * large kernels, ni = 1 the small-N kernel (warps = lane groups per warp),
- * ni = 3 the Newton-3 FP32C kernel (each unordered pair once); split = j
+ * ni = 3 the Newton-3 kernel (each unordered pair once; the FP32C default
+ * from 16384 to 2^20 particles, opt-in or autotuned for FP64); split = j
  * splits (unused by the Newton-3 kernel). */
 int nbr_get_force_config(nbr_ctx* ctx, int precision, double eps2, int* ni, int* warps, int* split);
 /* Times the supported configurations for the uploaded system and stores the

@@ -421,7 +421,7 @@ int eval_system(nbr_ctx* c, int precision, double G, double eps2, int mode, doub
   if (precision == kFP32C) e = ensure_records(c, a, kernels);
   if (e != cudaSuccess) return cuda_fail(c, e, "pack");
   ForceConfig cfg = choose_config(c, precision, eps2, rn, s.ntiles);
-  if (cfg.ni == 3 && (ranged || precision != kFP32C || rn > kN3MaxN))  // needs the whole system
+  if (cfg.ni == 3 && (ranged || rn > kN3MaxN))  // needs the whole system
     cfg = choose_config_large(c, precision, eps2, rn, s.ntiles);
   int rc = prepare_split(c, cfg, np_i);
   if (rc) return rc;
@@ -451,7 +451,8 @@ int eval_system(nbr_ctx* c, int precision, double G, double eps2, int mode, doub
       // test hook: under-report the receivers' length so that the check trips
       if (std::getenv("NBR_TEST_SHRINK_BOUNDS")) ip.len = rn - 1;)
   if (cfg.ni == 3) {
-    e = launch_force_n3(eps2, ip, js, ep, c->scr.part, (long long)c->scr.part_cap, c->stream);
+    e = launch_force_n3(precision, eps2, ip, js, ep, c->scr.part, (long long)c->scr.part_cap,
+                        c->stream);
     if (kernels) *kernels += 2;
   } else {
     e = launch_force(precision, eps2, cfg, ip, js, ep, c->stream);
@@ -1150,7 +1151,7 @@ int nbr_get_force_config(nbr_ctx* c, int precision, double eps2, int* ni, int* w
   if (s.n == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no system uploaded");
   cudaSetDevice(c->device);
   ForceConfig cfg = choose_config(c, precision, eps2, (long long)s.n, s.ntiles);
-  if (cfg.ni == 3 && (precision != kFP32C || (long long)s.n > kN3MaxN))
+  if (cfg.ni == 3 && (long long)s.n > kN3MaxN)
     cfg = choose_config_large(c, precision, eps2, (long long)s.n, s.ntiles);
   if (ni) *ni = cfg.ni;
   if (warps) *warps = cfg.warps;
@@ -1178,7 +1179,7 @@ int nbr_autotune(nbr_ctx* c, int precision, double eps2) {
   float best_ms = 1e30f;
   for (auto& cw : cand) {
     if (cw[0] == 1 && s.n > 65536) continue;  // the small-N kernel only competes on small systems
-    if (cw[0] == 3 && (precision != kFP32C || s.n < 8192 || (long long)s.n > kN3MaxN)) continue;
+    if (cw[0] == 3 && (s.n < 8192 || (long long)s.n > kN3MaxN)) continue;
     ForceConfig base{cw[0], cw[1], 1};
     const int s0 = auto_split(precision, eps2, base, (long long)s.n, s.ntiles, c->sms);
     const int splits[] = {std::max(1, s0 / 2), s0, s0 * 2};

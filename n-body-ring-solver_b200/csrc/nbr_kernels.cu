@@ -869,6 +869,168 @@ __global__ void __launch_bounds__(kN3Warps * 32)
   }
 }
 
+// FP64 form of the Newton-3 kernel (ForceConfig ni = 3 with NBR_FP64): the
+// blocks, CTA map, source rotation and partial-sum layout of k_force_n3_f32c,
+// with every operation in FP64 and the reciprocal square root from CUDA's
+// rsqrt(double), as in k_force_f64; the source tiles are the FP64 x, y, z, m
+// arrays.  Lane L holds receivers a * kN3Block + L + 32 q, q < 8.  Per
+// unordered pair: 3 sub, 3 fma, rsqrt, 2 mul (y^3), 2 mul (m_j y^3, m_i y^3)
+// and 6 fma, against 12 operations and one rsqrt per ordered pair in
+// k_force_f64.  Equal to k_force_f64 up to summation order; deterministic.
+template <bool EXCL>
+__global__ void __launch_bounds__(kN3Warps * 32)
+    k_force_n3_f64(const IParticles ip, const JStream js, const N3Params p3, const double eps2,
+                   int* err) {
+  constexpr int NI = kN3Block / 32;
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
+  unsigned char* stages = smem + kSmemHead;
+  double* red = reinterpret_cast<double*>(stages + kStages * kStage64);  // [warp][3][256]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int g = 0, k = blockIdx.x;
+  const int groups = (int)((p3.nb + kN3Warps - 1) / kN3Warps);
+  while (g < groups) {  // the grid has exactly sum_g n3_chunks(nb, cols, g) CTAs
+    const int K = n3_chunks(p3.nb, p3.cols, g);
+    if (k < K) break;
+    k -= K;
+    ++g;
+  }
+  if (g >= groups) return;
+  const long long r0 = (long long)g * kN3Warps;
+  const long long a = r0 + warp;
+  const long long cs = r0 + (long long)k * p3.cols;
+  const long long ce = min(cs + (long long)p3.cols, p3.nb);
+  const int ntl = (int)(2 * (ce - cs));
+  const bool row_ok = a < p3.nb;
+  const long long ibase = a * kN3Block + lane;
+
+  double xi[NI], yi[NI], zi[NI], mi[NI], AX[NI], AY[NI], AZ[NI];
+#pragma unroll
+  for (int q = 0; q < NI; ++q) {
+    xi[q] = yi[q] = zi[q] = mi[q] = 0.0;
+    AX[q] = AY[q] = AZ[q] = 0.0;
+    const long long i = ibase + 32 * q;
+    if (row_ok && NBR_IN(i, ip.len, err)) {
+      xi[q] = ip.x[i]; yi[q] = ip.y[i]; zi[q] = ip.z[i]; mi[q] = ip.m[i];
+    }
+  }
+
+  auto issue = [&](int st, int t) {
+    unsigned char* dst = stages + st * kStage64;
+    const uint32_t bar = smem_u32(&bars[st]);
+    const size_t off = (size_t)(2 * cs + t) * kTile;
+    if (!NBR_IN((long long)off + kTile - 1, js.len, err)) return;  // the wait expires
+    mbar_expect_tx(bar, kStage64);
+    bulk_g2s(dst, js.x + off, kTile * 8, bar);
+    bulk_g2s(dst + kTile * 8, js.y + off, kTile * 8, bar);
+    bulk_g2s(dst + 2 * kTile * 8, js.z + off, kTile * 8, bar);
+    bulk_g2s(dst + 3 * kTile * 8, js.m + off, kTile * 8, bar);
+  };
+  int tcur = 0;
+  auto body = [&](int st) {
+    const int t = tcur++;
+    const long long c = cs + t / 2;
+    const int half = t & 1;
+    const double* sx = reinterpret_cast<const double*>(stages + st * kStage64);
+    const double* sy = sx + kTile;
+    const double* sz = sy + kTile;
+    const double* sm = sz + kTile;
+    double* myred = red + warp * 3 * kN3Block + half * kTile;
+    if (row_ok && c == a) {
+      // every ordered pair of the block, action only (the k_force_f64 body)
+#pragma unroll 2
+      for (int j = 0; j < kTile; ++j) {
+        const double xj = sx[j], yj = sy[j], zj = sz[j], mj = sm[j];
+#pragma unroll
+        for (int q = 0; q < NI; ++q) {
+          const double dx = xj - xi[q], dy = yj - yi[q], dz = zj - zi[q];
+          double r2 = fma(dx, dx, eps2);
+          r2 = fma(dy, dy, r2);
+          r2 = fma(dz, dz, r2);
+          double y = rsqrt(r2);
+          if (EXCL) y = r2 > 0.0 ? y : 0.0;
+          const double s = mj * (y * y * y);
+          AX[q] = fma(s, dx, AX[q]);
+          AY[q] = fma(s, dy, AY[q]);
+          AZ[q] = fma(s, dz, AZ[q]);
+        }
+      }
+#pragma unroll
+      for (int bt = 0; bt < 4; ++bt)
+        myred[bt * 32 + lane] = myred[kN3Block + bt * 32 + lane] = myred[2 * kN3Block + bt * 32 + lane] = 0.0;
+    } else if (row_ok && c > a) {
+      const int from = (lane + 31) & 31;
+#pragma unroll 1
+      for (int bt = 0; bt < 4; ++bt) {
+        const int j = bt * 32 + lane;
+        double xs = sx[j], ys = sy[j], zs = sz[j], ms = sm[j];
+        double RX = 0.0, RY = 0.0, RZ = 0.0;
+#pragma unroll 2
+        for (int step = 0; step < 32; ++step) {
+#pragma unroll
+          for (int q = 0; q < NI; ++q) {
+            const double dx = xs - xi[q], dy = ys - yi[q], dz = zs - zi[q];
+            double r2 = fma(dx, dx, eps2);
+            r2 = fma(dy, dy, r2);
+            r2 = fma(dz, dz, r2);
+            double y = rsqrt(r2);
+            if (EXCL) y = r2 > 0.0 ? y : 0.0;
+            const double y3 = y * y * y;
+            const double sj = ms * y3, si = mi[q] * y3;
+            AX[q] = fma(sj, dx, AX[q]);
+            AY[q] = fma(sj, dy, AY[q]);
+            AZ[q] = fma(sj, dz, AZ[q]);
+            RX = fma(si, dx, RX);
+            RY = fma(si, dy, RY);
+            RZ = fma(si, dz, RZ);
+          }
+          xs = __shfl_sync(0xffffffffu, xs, from);
+          ys = __shfl_sync(0xffffffffu, ys, from);
+          zs = __shfl_sync(0xffffffffu, zs, from);
+          ms = __shfl_sync(0xffffffffu, ms, from);
+          RX = __shfl_sync(0xffffffffu, RX, from);
+          RY = __shfl_sync(0xffffffffu, RY, from);
+          RZ = __shfl_sync(0xffffffffu, RZ, from);
+        }
+        // back at its own lane: the force on source j is -sum m_i y^3 d
+        myred[bt * 32 + lane] = -RX;
+        myred[kN3Block + bt * 32 + lane] = -RY;
+        myred[2 * kN3Block + bt * 32 + lane] = -RZ;
+      }
+    } else {
+#pragma unroll
+      for (int bt = 0; bt < 4; ++bt)
+        myred[bt * 32 + lane] = myred[kN3Block + bt * 32 + lane] = myred[2 * kN3Block + bt * 32 + lane] = 0.0;
+    }
+    if (half == 1) {
+      // end of column block c: its reaction from this CTA's rows, summed in
+      // warp order, to the block's partial slot
+      __syncthreads();
+      const int tid = threadIdx.x;  // one source of the block per thread
+      const long long off = ((long long)blockIdx.x * p3.cols + (c - cs)) * 3 * kN3Block;
+      double* out = p3.rea + off;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        double s = 0.0;
+        for (int w = 0; w < kN3Warps; ++w) s += red[(w * 3 + d) * kN3Block + tid];
+        if (NBR_IN((p3.rea - p3.act) + off + d * kN3Block + tid, p3.act_len, err))
+          out[d * kN3Block + tid] = s;
+      }
+      __syncthreads();
+    }
+  };
+  if (!tile_pipeline(bars, ntl, js, err, issue, body)) return;
+  double* act = p3.act + ((size_t)blockIdx.x * kN3Warps + warp) * 3 * kN3Block;
+  if (!NBR_IN(((long long)blockIdx.x * kN3Warps + warp + 1) * 3 * kN3Block - 1, p3.act_len, err))
+    return;
+#pragma unroll
+  for (int q = 0; q < NI; ++q) {
+    act[lane + 32 * q] = AX[q];
+    act[kN3Block + lane + 32 * q] = AY[q];
+    act[2 * kN3Block + lane + 32 * q] = AZ[q];
+  }
+}
+
 // Adds the Newton-3 partial sums of each particle in a fixed order (its row
 // group's chunks, then the reactions from row groups 0 .. its own) and runs the
 // epilogue of the large kernels.  One warp per 128-particle tile.
@@ -1194,10 +1356,10 @@ cudaError_t launch_small_t(double eps2, int split, const IParticles& ip, const J
 
 }  // namespace
 
-size_t n3_smem_bytes();
+size_t n3_smem_bytes(int precision);
 
 bool force_config_supported(int precision, const ForceConfig& c) {
-  if (c.ni == 3) return precision == kFP32C && c.warps == kN3Warps;  // Newton-3 (FP32C only)
+  if (c.ni == 3) return c.warps == kN3Warps;  // Newton-3 (FP32C and FP64)
   if (c.ni == 1) return (c.warps == 2 || c.warps == 4 || c.warps == 8) && c.split >= 1;
 #define NBR_MATCH(a, b) if (c.ni == a && c.warps == b) return c.split >= 1;
   NBR_CFG_LIST(NBR_MATCH)
@@ -1208,9 +1370,12 @@ bool force_config_supported(int precision, const ForceConfig& c) {
 int force_blocks_per_sm(int precision, double eps2, const ForceConfig& c) {
   int nb = 0;
   if (c.ni == 3) {
-    const void* fn = eps2 == 0.0 ? (const void*)k_force_n3_f32c<true> : (const void*)k_force_n3_f32c<false>;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kN3Warps * 32, n3_smem_bytes()) !=
-        cudaSuccess)
+    const bool ex = eps2 == 0.0;
+    const void* fn = precision == kFP32C
+                         ? (ex ? (const void*)k_force_n3_f32c<true> : (const void*)k_force_n3_f32c<false>)
+                         : (ex ? (const void*)k_force_n3_f64<true> : (const void*)k_force_n3_f64<false>);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kN3Warps * 32,
+                                                      n3_smem_bytes(precision)) != cudaSuccess)
       nb = 0;
     return nb;
   }
@@ -1279,23 +1444,27 @@ cudaError_t launch_force(int precision, double eps2, const ForceConfig& c, const
   return cudaErrorInvalidValue;
 }
 
-size_t n3_smem_bytes() {
-  return kSmemHead + (size_t)kStages * kStage32 + (size_t)kN3Warps * 3 * kN3Block * sizeof(float);
+// Tile ring plus the per-warp reaction staging (floats for FP32C, doubles for
+// FP64).
+size_t n3_smem_bytes(int precision) {
+  return precision == kFP32C
+             ? kSmemHead + (size_t)kStages * kStage32 + (size_t)kN3Warps * 3 * kN3Block * sizeof(float)
+             : kSmemHead + (size_t)kStages * kStage64 + (size_t)kN3Warps * 3 * kN3Block * sizeof(double);
 }
 
 cudaError_t configure_kernels() {
-  // The Newton-3 kernel needs more than the default 48 KB of dynamic shared
+  // The Newton-3 kernels need more than the default 48 KB of dynamic shared
   // memory; set once per device, outside any stream capture.
-  const int smem = (int)n3_smem_bytes();
-  cudaError_t e = cudaFuncSetAttribute((const void*)k_force_n3_f32c<true>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute((const void*)k_force_n3_f32c<false>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  const int s32 = (int)n3_smem_bytes(kFP32C), s64 = (int)n3_smem_bytes(kFP64);
+  const cudaFuncAttribute at = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  cudaError_t e = cudaFuncSetAttribute((const void*)k_force_n3_f32c<true>, at, s32);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute((const void*)k_force_n3_f32c<false>, at, s32);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute((const void*)k_force_n3_f64<true>, at, s64);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute((const void*)k_force_n3_f64<false>, at, s64);
   return e;
 }
 
-cudaError_t launch_force_n3(double eps2, const IParticles& ip, const JStream& js,
+cudaError_t launch_force_n3(int precision, double eps2, const IParticles& ip, const JStream& js,
                             const Epilogue& ep, double* scratch, long long scratch_len,
                             cudaStream_t st) {
   (void)scratch_len;
@@ -1308,12 +1477,19 @@ cudaError_t launch_force_n3(double eps2, const IParticles& ip, const JStream& js
   p3.act = scratch;
   p3.rea = scratch + (size_t)ctas * kN3Warps * 3 * kN3Block;
   NBR_CHECKED_ONLY(p3.act_len = scratch_len;)
-  const size_t smem = n3_smem_bytes();
-  if (eps2 == 0.0)
-    k_force_n3_f32c<true><<<(unsigned)ctas, kN3Warps * 32, smem, st>>>(ip, js, p3, 0.f, ep.err);
-  else
-    k_force_n3_f32c<false><<<(unsigned)ctas, kN3Warps * 32, smem, st>>>(ip, js, p3, (float)eps2,
-                                                                       ep.err);
+  const size_t smem = n3_smem_bytes(precision);
+  const unsigned grid = (unsigned)ctas, block = kN3Warps * 32;
+  if (precision == kFP32C) {
+    if (eps2 == 0.0)
+      k_force_n3_f32c<true><<<grid, block, smem, st>>>(ip, js, p3, 0.f, ep.err);
+    else
+      k_force_n3_f32c<false><<<grid, block, smem, st>>>(ip, js, p3, (float)eps2, ep.err);
+  } else {
+    if (eps2 == 0.0)
+      k_force_n3_f64<true><<<grid, block, smem, st>>>(ip, js, p3, 0.0, ep.err);
+    else
+      k_force_n3_f64<false><<<grid, block, smem, st>>>(ip, js, p3, eps2, ep.err);
+  }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   const long long threads = p3.nb * 2 * 32;  // a warp per tile

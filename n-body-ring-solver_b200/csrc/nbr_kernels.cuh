@@ -79,7 +79,7 @@ struct ForceConfig {
 // receivers per CTA.
 constexpr int kSmallWarps = 4;
 constexpr int kSmallNI = 4;
-// The Newton-3 FP32C kernel (ForceConfig ni = 3): blocks of kN3Block
+// The Newton-3 kernels (ForceConfig ni = 3, FP32C and FP64): blocks of kN3Block
 // particles, kN3Warps row blocks per CTA (one per warp), up to `cols` column
 // blocks per CTA (n3_cols: fewer on small systems, for enough CTAs).
 constexpr int kN3Warps = 8;
@@ -118,11 +118,11 @@ inline long long n3_scratch_doubles(long long nb) {
   const int cols = n3_cols(nb);
   return n3_ctas(nb, cols) * (long long)(kN3Warps + cols) * 3 * kN3Block;
 }
-// One Newton-3 force evaluation (FP32C) over all n_pad receivers of ip
-// against the same particles' records in js, with the epilogue ep:
-// the pair kernel, then the per-particle reduction.  scratch holds
-// n3_scratch_doubles(ceil(n / kN3Block)) doubles.
-cudaError_t launch_force_n3(double eps2, const IParticles& ip, const JStream& js,
+// One Newton-3 force evaluation over all n_pad receivers of ip against the
+// same particles in js (FP32C: their records; FP64: their x, y, z, m arrays),
+// with the epilogue ep: the pair kernel, then the per-particle reduction.
+// scratch holds n3_scratch_doubles(ceil(n / kN3Block)) doubles.
+cudaError_t launch_force_n3(int precision, double eps2, const IParticles& ip, const JStream& js,
                             const Epilogue& ep, double* scratch, long long scratch_len,
                             cudaStream_t stream);
 // Kernel attributes that must be set once per device, outside stream capture.

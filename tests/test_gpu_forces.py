@@ -99,10 +99,8 @@ def test_every_kernel_configuration_agrees(ctx, nbr, oracle, prec):
     upload(ctx, s)
     ref = truth(oracle, s, 1e-6)
     # (1, F): the small-N warp-splitting kernel with F lane groups per warp;
-    # (3, 8): the Newton-3 kernel (FP32C only)
-    cfgs = [(4, 2), (4, 4), (4, 8), (8, 2), (8, 4), (1, 2), (1, 4), (1, 8)]
-    if prec == FP32C:
-        cfgs.append((3, 8))
+    # (3, 8): the Newton-3 kernel
+    cfgs = [(4, 2), (4, 4), (4, 8), (8, 2), (8, 4), (1, 2), (1, 4), (1, 8), (3, 8)]
     for ni, warps in cfgs:
         for split in (1, 3, 0, 47):
             ctx.set_force_config(prec, ni, warps, split)
@@ -367,3 +365,41 @@ def test_newton3_kernel(ctx, nbr, oracle, n):
                 assert np.abs(got[k] - want[k]).max() <= 1e-6, k
     finally:
         ctx.set_force_config(FP32C, 0)
+
+
+@pytest.mark.parametrize("n,eps2", [(300, 1e-6), (4097, 1e-6), (20000, 1e-6), (70000, 1e-6),
+                                    (300, 0.0), (4097, 0.0), (20000, 0.0)])
+def test_newton3_kernel_fp64(ctx, nbr, oracle, n, eps2):
+    """The Newton-3 FP64 kernel (set_force_config(FP64, 3, 8)): the FP64
+    drop-in bound of 1e-12 against the extended-precision oracle, with and
+    without softening (eps2 = 0 excludes the self pair), bit-for-bit
+    repeatability, agreement with the plain FP64 kernel to summation order,
+    momentum balance, and a KDK run through its reduction epilogue."""
+    s = nbr.plummer(n, 29)
+    upload(ctx, s)
+    ctx.set_force_config(FP64, 3, 8, 0)
+    try:
+        assert ctx.get_force_config(FP64, eps2)[0] == 3
+        a = ctx.forces(FP64, eps2=eps2)
+        b = ctx.forces(FP64, eps2=eps2)
+        np.testing.assert_array_equal(a, b)
+        idx = np.arange(0, n, max(1, n // 500))
+        ref = oracle.accel_subset(s["x"], s["y"], s["z"], s["m"], idx, eps2=eps2)
+        e = rel_err(a[:, idx], ref)
+        assert e.max() <= 1e-12, e.max()
+        ctx.set_force_config(FP64, 4, 4, 0)
+        plain = ctx.forces(FP64, eps2=eps2)
+        assert rel_err(a, plain).max() <= 1e-12
+        net = np.abs((s["m"] * a).sum(axis=1)).max()
+        scale = (s["m"] * np.linalg.norm(a, axis=0)).sum()
+        assert net <= 1e-12 * scale
+        if n <= 20000 and eps2 > 0:
+            ctx.set_force_config(FP64, 3, 8, 0)
+            upload(ctx, s)
+            ctx.run(FP64, 0, 2, 1e-3, 5, eps2=eps2)
+            got = ctx.download()
+            want = oracle.kdk(s, 1e-3, 5, eps2=eps2)
+            for k in ("x", "y", "z", "vx", "vy", "vz"):
+                assert np.abs(got[k] - want[k]).max() <= 1e-11, k
+    finally:
+        ctx.set_force_config(FP64, 0)
