@@ -272,9 +272,9 @@ int nbr_set_force_config(nbr_ctx* ctx, int precision, int ni, int warps, int spl
 /* The configuration a force evaluation of the uploaded system would use
  * (forced, autotuned or default): ni = 4 or 8 receivers per thread of the
  * large kernels, ni = 1 the small-N kernel (warps = lane groups per warp),
- * ni = 3 the Newton-3 kernel (each unordered pair once; the FP32C default
- * from 16384 to 2^20 particles, opt-in or autotuned for FP64); split = j
- * splits (unused by the Newton-3 kernel). */
+ * ni = 3 the Newton-3 kernel (each unordered pair once; the default of both
+ * precisions from 16384 to 2^20 particles); split = j splits (unused by the
+ * Newton-3 kernel). */
 int nbr_get_force_config(nbr_ctx* ctx, int precision, double eps2, int* ni, int* warps, int* split);
 /* Times the supported configurations for the uploaded system and stores the
  * fastest in the autotune cache file (see nbr_tune_cache_path). */

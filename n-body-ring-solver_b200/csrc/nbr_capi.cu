@@ -319,10 +319,11 @@ ForceConfig choose_config(nbr_ctx* c, int precision, double eps2, long long n_i,
     // that the large kernels win.
     const int F = precision == kFP32C ? (n_i <= 4096 ? 8 : n_i <= 8192 ? 2 : 0)
                                       : (n_i <= 16384 ? 8 : n_i <= 32768 ? 4 : 0);
-    if (F) dflt = ForceConfig{1, F, 0};
-    // FP32C from 16384 to 2^20 particles: the Newton-3 kernel (+24 % at
-    // N = 262144, +28 % at 2^20 on B200).
-    else if (precision == kFP32C && n_i >= kN3MinN && n_i <= kN3MaxN) dflt = ForceConfig{3, kN3Warps, 0};
+    // From 16384 to 2^20 particles: the Newton-3 kernels (B200, against the
+    // best other kernel: FP32C +24 % at N = 262144 and +28 % at 2^20; FP64
+    // +16 % at 16384, +20 % at 32768, +30 % at 262144, +33 % at 2^20).
+    if (n_i >= kN3MinN && n_i <= kN3MaxN) dflt = ForceConfig{3, kN3Warps, 0};
+    else if (F) dflt = ForceConfig{1, F, 0};
     cfg = it != g_tune->end() ? it->second : dflt;
   }
   if (cfg.split <= 0) cfg.split = auto_split(precision, eps2, cfg, n_i, ntiles, c->sms);

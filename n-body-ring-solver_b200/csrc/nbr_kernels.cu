@@ -873,20 +873,24 @@ __global__ void __launch_bounds__(kN3Warps * 32)
 // blocks, CTA map, source rotation and partial-sum layout of k_force_n3_f32c,
 // with every operation in FP64 and the reciprocal square root from CUDA's
 // rsqrt(double), as in k_force_f64; the source tiles are the FP64 x, y, z, m
-// arrays.  Lane L holds receivers a * kN3Block + L + 32 q, q < 8.  Per
+// arrays.  Two warps share each row block: warp w of the CTA takes row block
+// a = r0 + w / 2 and, in lane L, its receivers a * kN3Block + 128 (w % 2) +
+// L + 32 q, q < 4 (16 warps, under 128 registers: twice the warps per SM of
+// a one-warp-per-block layout, for the long FP64 rsqrt chain).  Per
 // unordered pair: 3 sub, 3 fma, rsqrt, 2 mul (y^3), 2 mul (m_j y^3, m_i y^3)
 // and 6 fma, against 12 operations and one rsqrt per ordered pair in
 // k_force_f64.  Equal to k_force_f64 up to summation order; deterministic.
 template <bool EXCL>
-__global__ void __launch_bounds__(kN3Warps * 32)
+__global__ void __launch_bounds__(kN3F64Warps * 32)
     k_force_n3_f64(const IParticles ip, const JStream js, const N3Params p3, const double eps2,
                    int* err) {
-  constexpr int NI = kN3Block / 32;
+  constexpr int NI = kN3Block / 64;
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
   unsigned char* stages = smem + kSmemHead;
   double* red = reinterpret_cast<double*>(stages + kStages * kStage64);  // [warp][3][256]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int rb = warp >> 1, hf = warp & 1;  // row block in the group, its receiver half
   int g = 0, k = blockIdx.x;
   const int groups = (int)((p3.nb + kN3Warps - 1) / kN3Warps);
   while (g < groups) {  // the grid has exactly sum_g n3_chunks(nb, cols, g) CTAs
@@ -897,12 +901,12 @@ __global__ void __launch_bounds__(kN3Warps * 32)
   }
   if (g >= groups) return;
   const long long r0 = (long long)g * kN3Warps;
-  const long long a = r0 + warp;
+  const long long a = r0 + rb;
   const long long cs = r0 + (long long)k * p3.cols;
   const long long ce = min(cs + (long long)p3.cols, p3.nb);
   const int ntl = (int)(2 * (ce - cs));
   const bool row_ok = a < p3.nb;
-  const long long ibase = a * kN3Block + lane;
+  const long long ibase = a * kN3Block + hf * (kN3Block / 2) + lane;
 
   double xi[NI], yi[NI], zi[NI], mi[NI], AX[NI], AY[NI], AZ[NI];
 #pragma unroll
@@ -1007,21 +1011,23 @@ __global__ void __launch_bounds__(kN3Warps * 32)
       // warp order, to the block's partial slot
       __syncthreads();
       const int tid = threadIdx.x;  // one source of the block per thread
-      const long long off = ((long long)blockIdx.x * p3.cols + (c - cs)) * 3 * kN3Block;
-      double* out = p3.rea + off;
+      if (tid < kN3Block) {
+        const long long off = ((long long)blockIdx.x * p3.cols + (c - cs)) * 3 * kN3Block;
+        double* out = p3.rea + off;
 #pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        double s = 0.0;
-        for (int w = 0; w < kN3Warps; ++w) s += red[(w * 3 + d) * kN3Block + tid];
-        if (NBR_IN((p3.rea - p3.act) + off + d * kN3Block + tid, p3.act_len, err))
-          out[d * kN3Block + tid] = s;
+        for (int d = 0; d < 3; ++d) {
+          double s = 0.0;
+          for (int w = 0; w < kN3F64Warps; ++w) s += red[(w * 3 + d) * kN3Block + tid];
+          if (NBR_IN((p3.rea - p3.act) + off + d * kN3Block + tid, p3.act_len, err))
+            out[d * kN3Block + tid] = s;
+        }
       }
       __syncthreads();
     }
   };
   if (!tile_pipeline(bars, ntl, js, err, issue, body)) return;
-  double* act = p3.act + ((size_t)blockIdx.x * kN3Warps + warp) * 3 * kN3Block;
-  if (!NBR_IN(((long long)blockIdx.x * kN3Warps + warp + 1) * 3 * kN3Block - 1, p3.act_len, err))
+  double* act = p3.act + ((size_t)blockIdx.x * kN3Warps + rb) * 3 * kN3Block + hf * (kN3Block / 2);
+  if (!NBR_IN(((long long)blockIdx.x * kN3Warps + rb + 1) * 3 * kN3Block - 1, p3.act_len, err))
     return;
 #pragma unroll
   for (int q = 0; q < NI; ++q) {
@@ -1374,8 +1380,9 @@ int force_blocks_per_sm(int precision, double eps2, const ForceConfig& c) {
     const void* fn = precision == kFP32C
                          ? (ex ? (const void*)k_force_n3_f32c<true> : (const void*)k_force_n3_f32c<false>)
                          : (ex ? (const void*)k_force_n3_f64<true> : (const void*)k_force_n3_f64<false>);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kN3Warps * 32,
-                                                      n3_smem_bytes(precision)) != cudaSuccess)
+    const int threads = (precision == kFP32C ? kN3Warps : kN3F64Warps) * 32;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, threads, n3_smem_bytes(precision)) !=
+        cudaSuccess)
       nb = 0;
     return nb;
   }
@@ -1449,7 +1456,7 @@ cudaError_t launch_force(int precision, double eps2, const ForceConfig& c, const
 size_t n3_smem_bytes(int precision) {
   return precision == kFP32C
              ? kSmemHead + (size_t)kStages * kStage32 + (size_t)kN3Warps * 3 * kN3Block * sizeof(float)
-             : kSmemHead + (size_t)kStages * kStage64 + (size_t)kN3Warps * 3 * kN3Block * sizeof(double);
+             : kSmemHead + (size_t)kStages * kStage64 + (size_t)kN3F64Warps * 3 * kN3Block * sizeof(double);
 }
 
 cudaError_t configure_kernels() {
@@ -1478,7 +1485,7 @@ cudaError_t launch_force_n3(int precision, double eps2, const IParticles& ip, co
   p3.rea = scratch + (size_t)ctas * kN3Warps * 3 * kN3Block;
   NBR_CHECKED_ONLY(p3.act_len = scratch_len;)
   const size_t smem = n3_smem_bytes(precision);
-  const unsigned grid = (unsigned)ctas, block = kN3Warps * 32;
+  const unsigned grid = (unsigned)ctas, block = (precision == kFP32C ? kN3Warps : kN3F64Warps) * 32;
   if (precision == kFP32C) {
     if (eps2 == 0.0)
       k_force_n3_f32c<true><<<grid, block, smem, st>>>(ip, js, p3, 0.f, ep.err);

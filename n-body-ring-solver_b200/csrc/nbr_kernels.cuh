@@ -83,6 +83,7 @@ constexpr int kSmallNI = 4;
 // particles, kN3Warps row blocks per CTA (one per warp), up to `cols` column
 // blocks per CTA (n3_cols: fewer on small systems, for enough CTAs).
 constexpr int kN3Warps = 8;
+constexpr int kN3F64Warps = 2 * kN3Warps;  // FP64: two warps per row block
 constexpr int kN3Block = 256;
 constexpr int kN3MaxCols = 32;
 struct N3Params {
