@@ -74,7 +74,8 @@ def workload_config(a, extra=None):
     cfg = {"workload": f"plummer_n{a.n}_seed{a.seed}_eps{a.eps:g}_kdk_dt{a.dt:g}",
            "n": a.n, "ic": "plummer", "seed": a.seed, "eps": a.eps, "dt": a.dt,
            "scheme": "kdk", "pairs_per_step": a.n * (a.n - 1),
-           "l2": "flushed between timed steps (256 MiB write); j-stream 12.6 MB is L2-resident within a step"}
+           "l2": f"flushed between timed steps (256 MiB write); j-stream {48 * a.n / 1e6:.1f} MB "
+                 "is L2-resident within a step"}
     if extra:
         cfg.update(extra)
     return cfg
