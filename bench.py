@@ -40,6 +40,8 @@ sys.path.insert(0, PKG)
 
 METRIC = "GPairs/s FP32-compensated vs FP64 on 1 B200 at median force rel err <=1e-6"
 UNIT = "GPairs/s"
+# SM count of the device (set in run_ours / run_sharded from the device
+# properties; 148 on B200).
 SMS = 148
 FMA_OPS_PER_PAIR = 16
 # The Newton-3 kernel evaluates each unordered pair once: the 16 operations of
@@ -63,6 +65,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-accuracy", action="store_true")
     p.add_argument("--no-batch", action="store_true")
+    p.add_argument("--no-configs", action="store_true",
+                   help="skip the N=2048 (100 KDK steps) and N=1048576 (5 steps) lines")
     p.add_argument("--no-config-accuracy", action="store_true",
                    help="skip the cold-collapse and two-component accuracy runs")
     p.add_argument("--shard", action="store_true",
@@ -133,86 +137,143 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------ CPU baseline --
-def cpu_reference_sample(n, seed, target_s, max_s):
-    """The reference's fastest CPU force kernel (AVX-512 rsqrt 4i, or AVX2
-    blocked on a host without AVX-512) on this host's cores, on rank 0's share
-    of its own ring decomposition (hybrid_ring_solver) of one N-particle force
-    evaluation: N(N-1)/comm_sz effective pairs per share.  comm_sz is the
-    smallest power of two whose share takes at most target_s."""
+# The reference's CPU solver (oracle/_ref, compiled from its sources) is timed
+# in two legs, both on this host's cores with every OpenMP thread, FP64,
+# unsoftened (the reference has no softening; the pair count is the same):
+#   * force only: its fastest kernel (AVX-512 rsqrt 4i; AVX2 blocked without
+#     AVX-512), on rank 0's share of its own ring decomposition
+#     (hybrid_ring_solver) of one force evaluation -- the counterpart of our
+#     force kernel;
+#   * end to end: reduced_solver_omp_lf (CPU/omp_solver.cpp:257-456), the
+#     solver behind main.cpp's -i lf: DKD leapfrog order 2 with the AVX2 blocked
+#     kernel, whole steps of the whole system -- the counterpart of our C-ABI
+#     step.  Throughput = steps x N(N-1) / seconds (the reference's own
+#     effective-pair count, CPU/omp_solver.cpp:745-752).
+# Inputs come from the oracle's samplers (bit-identical to the product's), so
+# a process timing the reference never loads the product library.
+
+def _reference():
     sys.path.insert(0, ORACLE)
-    import nbr
-    from oracle import Reference, reference_available
+    from oracle import Oracle, Reference, reference_available
     if not reference_available():
-        return None
+        return None, None
     ref = Reference()
     ref.set_threads(os.cpu_count() or 1)
-    s = nbr.plummer(n, seed)
-    # calibrate on a small share
+    return ref, Oracle()
+
+
+def _ref_kernel_name(ref):
+    return "AVX512-RSQRT-4I" if ref.has_avx512 else "AVX2-blocked"
+
+
+def ref_force_leg(ref, s, per_call_s, target_s, max_s, warmup=0, calls=None):
+    """Force-only leg: the rank-0 share (1/comm_sz of one N-particle force
+    evaluation) whose time is at most per_call_s, repeated until target_s
+    (or exactly `calls` times)."""
+    n = len(s["x"])
     comm = 1
-    while comm < n and n % (comm * 2) == 0 and comm < 256:
+    while comm < n and n % (comm * 2) == 0 and comm < 1024:
         comm *= 2
     t = ref.ring_share(s, comm)
-    while comm > 1 and t * 2 <= target_s:
+    while comm > 1 and t * 2 <= per_call_s:
         comm //= 2
         t = ref.ring_share(s, comm)
-    reps, total, pairs = 0, 0.0, 0.0
-    while total < target_s and total + t <= max_s or reps == 0:
-        tt = ref.ring_share(s, comm)
-        total += tt
-        pairs += n * (n - 1) / comm
-        reps += 1
-        if total >= target_s:
-            break
-    kernel = "AVX512-RSQRT-4I" if ref.has_avx512 else "AVX2-blocked"
-    return {"value": pairs / total / 1e9, "unit": UNIT, "cores": ref.threads(), "kind": "reference",
-            "seconds": total,
-            "sample": f"{reps} x rank-0 share (1/{comm}) of one N={n} force evaluation of the reference's "
-                      f"{kernel} kernel (ring decomposition of hybrid_ring_solver, eps=0, FP64), "
-                      f"{ref.threads()} OpenMP threads"}
+    for _ in range(warmup):
+        ref.ring_share(s, comm)
+    secs = []
+    while (calls is None and (sum(secs) < target_s and sum(secs) + t <= max_s or not secs)) or \
+            (calls is not None and len(secs) < calls):
+        secs.append(ref.ring_share(s, comm))
+    total = sum(secs)
+    value = len(secs) * n * (n - 1) / comm / total / 1e9
+    kernel = _ref_kernel_name(ref)
+    return {"value": value, "unit": UNIT, "cores": ref.threads(), "kind": "reference",
+            "seconds": total, "calls": len(secs), "comm_sz": comm, "kernel": kernel,
+            "sample": f"{len(secs)} x rank-0 share (1/{comm}) of one N={n} force evaluation of the "
+                      f"reference's {kernel} kernel (hybrid_ring_solver's ring decomposition), eps=0, "
+                      f"FP64, {ref.threads()} OpenMP threads"}, secs
+
+
+def ref_e2e_leg(ref, s, dt, target_s, max_steps):
+    """End-to-end leg: reduced_solver_omp_lf (DKD order 2, AVX2 blocked FP64)
+    on the whole system: one untimed step, then as many whole steps as fit in
+    about target_s (at least one, at most max_steps) in one solver call."""
+    n = len(s["x"])
+    _, t1 = ref.lf(s, dt, 1, order=2)
+    k = int(max(1, min(max_steps, target_s // max(t1, 1e-9))))
+    _, secs = ref.lf(s, dt, k, order=2)
+    return {"value": k * n * (n - 1) / secs / 1e9, "unit": UNIT, "cores": ref.threads(),
+            "kind": "reference", "steps": k, "seconds": secs, "steps_per_s": k / secs,
+            "ms_per_step": 1e3 * secs / k,
+            "sample": f"{k} whole DKD steps (order 2, dt={dt:g}) of the N={n} system through the "
+                      f"reference's reduced_solver_omp_lf (AVX2 blocked FP64 kernel, eps=0), "
+                      f"{ref.threads()} OpenMP threads, after one untimed step"}
+
+
+def ref_config0_leg(ref, orc, steps=100):
+    """The small-system configuration on the reference's solver:
+    reduced_solver_omp_lf on Plummer N = 2048 (seed 0), DKD order 2, dt 1e-3,
+    100 steps (eps=0)."""
+    s = orc.plummer(2048, 0)
+    ref.lf(s, 1e-3, 5, order=2)
+    _, secs = ref.lf(s, 1e-3, steps, order=2)
+    return {"steps_per_s": steps / secs, "gpairs": steps * 2048 * 2047 / secs / 1e9,
+            "seconds": secs, "cores": ref.threads(),
+            "sample": f"{steps} DKD steps (order 2, dt=1e-3) of Plummer N=2048 seed 0 through "
+                      f"reduced_solver_omp_lf (AVX2 blocked FP64, eps=0), {ref.threads()} threads"}
+
+
+def cpu_reference_sample(n, seed, dt, target_s=10.0, max_s=30.0):
+    """cpu_baseline of our line: both legs on a bounded sample (about 10 s
+    each) plus the small-system configuration."""
+    ref, orc = _reference()
+    if ref is None:
+        return None
+    s = orc.plummer(n, seed)
+    force, _ = ref_force_leg(ref, s, per_call_s=target_s, target_s=target_s, max_s=max_s)
+    e2e = ref_e2e_leg(ref, s, dt, target_s=target_s, max_steps=50)
+    out = dict(force)
+    out["legs"] = {"force_only": force, "end_to_end": e2e, "config0": ref_config0_leg(ref, orc)}
+    return out
 
 
 def run_reference(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    sys.path.insert(0, ORACLE)
-    from oracle import reference_available
-    if not reference_available():
+    ref, orc = _reference()
+    if ref is None:
         print(json.dumps({"impl": "reference", "unavailable":
                           "reference CPU solver (oracle/_ref) was not built here"}))
         return
-    import nbr
-    from oracle import Reference
-    ref = Reference()
-    ref.set_threads(os.cpu_count() or 1)
     n = a.n
-    s = nbr.plummer(n, a.seed)
+    s = orc.plummer(n, a.seed)
     # per-step budget so that warmup + steps end within about two minutes
     per_step = min(3.0, 120.0 / max(1, a.steps + a.warmup))
-    comm = 1
-    while comm < n and n % (comm * 2) == 0 and comm < 1024:
-        comm *= 2
-    t = ref.ring_share(s, comm)
-    while comm > 1 and t * 2 <= per_step:
-        comm //= 2
-        t = ref.ring_share(s, comm)
-    for _ in range(a.warmup):
-        ref.ring_share(s, comm)
-    secs = [ref.ring_share(s, comm) for _ in range(a.steps)]
+    force, secs = ref_force_leg(ref, s, per_call_s=per_step, target_s=0, max_s=0, warmup=a.warmup,
+                                calls=a.steps)
     total = sum(secs)
-    pairs = a.steps * n * (n - 1) / comm
-    value = pairs / total / 1e9
-    kernel = "AVX512-RSQRT-4I" if ref.has_avx512 else "AVX2-blocked"
+    value = force["value"]
+    e2e = ref_e2e_leg(ref, s, a.dt, target_s=20.0, max_steps=a.steps)
+    cfg0 = ref_config0_leg(ref, orc)
+    cpu = dict(force)
+    cpu["sample"] = ("each step: " + force["sample"])
+    cpu["legs"] = {"force_only": force, "end_to_end": e2e, "config0": cfg0}
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * total / a.steps,
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": workload_config(a, {"reference_kernel": kernel,
-                                                               "comm_sz": comm}),
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": ref.threads(), "kind": "reference",
-                             "sample": f"each step: rank-0 share (1/{comm}) of one N={n} force evaluation "
-                                       f"of the reference's {kernel} kernel (hybrid_ring_solver's ring "
-                                       f"decomposition), eps=0 FP64, {ref.threads()} threads"},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "data": "synthetic", "config": workload_config(a),
+            "reference_run": {"force_kernel": force["kernel"], "comm_sz": force["comm_sz"],
+                              "eps": 0.0, "scheme_e2e": "dkd order 2",
+                              "note": "the reference has no softening and no KDK scheme: it runs "
+                                      "the same Plummer system unsoftened (same pair count, one "
+                                      "add fewer per pair) with its own DKD leapfrog"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0, "steps_per_s": e2e["steps_per_s"],
+                    "ms_per_step": e2e["ms_per_step"], "steps": e2e["steps"],
+                    "solver": "reduced_solver_omp_lf (DKD order 2, AVX2 blocked FP64), whole steps"},
+            "config0": cfg0}
     print(json.dumps(line))
 
 
@@ -246,6 +307,8 @@ def run_ours(a):
     if world > 1 or a.shard:
         return run_sharded(a, rank, world, local)
     torch.cuda.set_device(local)
+    global SMS
+    SMS = torch.cuda.get_device_properties(local).multi_processor_count
     prec = nbr.FP32C if a.precision == "fp32c" else nbr.FP64
     eps2 = a.eps * a.eps
     n = a.n
@@ -368,7 +431,7 @@ def run_ours(a):
                 "fma_ops_per_ordered_pair": ops,
                 "traffic_note": "dram bytes per launch of the pair kernel from "
                                 "profiles/force_fp32c_plummer262144.json",
-                "peak_source": f"148 SMs x 128 FP32 lanes x median SM clock sampled in the timed region "
+                "peak_source": f"{SMS} SMs x 128 FP32 lanes x median SM clock sampled in the timed region "
                                f"/ {ops:g} FMA-pipe ops per ordered pair (MEASURED_PEAKS.json has no "
                                "FP32-pipe figure)",
                 "frac_at_max_clock": achieved / (SMS * 128 * 1965e6 / ops / 1e9),
@@ -395,13 +458,15 @@ def run_ours(a):
                        "over_plain": n3v / fp64["value"], "fp32c_over_fp64_default": achieved / n3v,
                        "max_rel_diff_vs_plain": float(d64.max())}
 
-    batched = None if a.no_batch else measure_batch(ctx, ext, eps2, value)
+    config0 = None if a.no_configs else measure_config0(ctx, l2_flush, mhz)
+    large = None if a.no_configs else measure_large(ctx, l2_flush, mhz)
+    batched = None if a.no_batch else measure_batch(ctx, eps2, value)
     config_acc = None if a.no_config_accuracy else measure_config_accuracy(ctx)
 
     cpu = None
     if not a.no_cpu_baseline and rank == 0:
         try:
-            cpu = cpu_reference_sample(n, a.seed, target_s=10.0, max_s=30.0)
+            cpu = cpu_reference_sample(n, a.seed, a.dt)
         except Exception as ex:  # the baseline is reported, never required
             cpu = {"error": str(ex)}
 
@@ -409,41 +474,110 @@ def run_ours(a):
             "warmup": a.warmup, "ms_per_step": 1e3 * t_total / a.steps,
             "steps_per_s": a.steps / t_total, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f32" if prec == nbr.FP32C else "f64",
-            "data": "synthetic", "config": workload_config(a, {"precision": a.precision}),
+            "precision": a.precision, "data": "synthetic", "config": workload_config(a),
             "gpu_launches": launches, "wall_s_timed": t_wall,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 7 * 8 * n,
                     "d2h_bytes_per_step": 6 * 8 * n, "scheme": "dkd order 2 (reduced_solver_omp_lf's)",
                     "ms_per_step": 1e3 * sum(e2e_s) / a.steps},
             "roofline": roofline, "fp64": fp64, "accuracy": acc, "clocks": clk,
-            "batched": batched, "config_accuracy": config_acc, "cpu_baseline": cpu}
+            "config0": config0, "n1048576": large, "batched": batched,
+            "config_accuracy": config_acc, "cpu_baseline": cpu}
     print(json.dumps(line))
     ctx.close()
 
 
-def measure_batch(ctx, ext, eps2, single_value, steps=10, nsys=4096, seed=3):
+def measure_batch(ctx, eps2, single_value, steps=100, nsys=4096, seed=3):
     """The batched workload: 4096 Plummer systems, sizes log-uniform in
-    [64, 4096] (seed 3, system s seeded by index), KDK dt = 1e-3, one persistent
-    work-queue launch per step, the step loop in one CUDA graph."""
-    import torch
+    [64, 4096] (seed 3, system s seeded by index), KDK dt = 1e-3 for 100 steps,
+    one persistent work-queue launch per step, the step loop in one CUDA graph.
+    The time is the graph launch alone (nbr_run_stats.gpu_ms: CUDA events on
+    the context stream around cudaGraphLaunch), capture and instantiation
+    excluded."""
     import nbr
     off, st = nbr.batch_plummer(nsys, seed)
-    ctx.batch_upload(off, st)
     out = {"workload": f"{nsys} Plummer systems, N log-uniform in [64, 4096], seed {seed}, "
-                       f"eps 1e-3, KDK dt 1e-3", "systems": nsys, "particles": int(off[-1])}
+                       f"eps 1e-3, KDK dt 1e-3, {steps} steps", "systems": nsys,
+           "particles": int(off[-1])}
     for prec, name in ((nbr.FP32C, "fp32c"), (nbr.FP64, "fp64")):
         ctx.batch_upload(off, st)
         ctx.batch_run(prec, dt=1e-3, steps=2, eps2=eps2)  # warm-up (and FSAL)
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(ext)
         r = ctx.batch_run(prec, dt=1e-3, steps=steps, eps2=eps2)
-        e1.record(ext)
-        e1.synchronize()
-        t = e0.elapsed_time(e1) * 1e-3
+        t = r["gpu_ms"] * 1e-3
         out[name] = {"gpairs": r["pairs"] / t / 1e9, "systems_steps_per_s": nsys * steps / t,
-                     "ms_per_step": 1e3 * t / steps, "force_evals": r["force_evals"],
+                     "ms_per_step": 1e3 * t / steps, "steps": steps, "force_evals": r["force_evals"],
                      "kernels": r["kernels"]}
     out["fp32c"]["frac_of_single_system"] = out["fp32c"]["gpairs"] / single_value
+    return out
+
+
+def fp64_peak(mhz, ops=FMA_OPS_PER_PAIR):
+    """Pairs/s of the FP64 pipe: SMs x 64 FP64 lanes x clock / ops per pair."""
+    return SMS * 64 * mhz * 1e6 / ops / 1e9
+
+
+def measure_config0(ctx, l2_flush, mhz, n=2048, steps=100):
+    """The small-system configuration: Plummer N = 2048 (seed 0), eps = 1e-3,
+    KDK dt = 1e-3 for 100 steps, FP64 (and FP32C beside it): one nbr_run call,
+    whose 100 steps run as one CUDA graph launch; time = nbr_run_stats.gpu_ms
+    (events around the graph launch; the first call's capture is untimed)."""
+    import nbr
+    s = nbr.plummer(n, 0)
+    eps2 = 1e-6
+    out = {"workload": f"plummer_n{n}_seed0_eps0.001_kdk_dt0.001_{steps}steps"}
+    for prec, name in ((nbr.FP64, "fp64"), (nbr.FP32C, "fp32c")):
+        times = []
+        for rep in range(4):
+            ctx.upload(s)
+            l2_flush()
+            r = ctx.run(prec, nbr.KDK, 2, 1e-3, steps, eps2=eps2)
+            if rep > 0:
+                times.append(r["gpu_ms"] * 1e-3)
+        t = min(times)
+        cfg = ctx.get_force_config(prec, eps2)
+        gp = r["pairs"] / t / 1e9
+        out[name] = {"steps_per_s": steps / t, "ms_per_step": 1e3 * t / steps, "gpairs": gp,
+                     "force_evals": r["force_evals"], "kernels_per_run": r["kernels"],
+                     "config": list(cfg), "runs_timed": len(times), "time": "best of 3 graph launches"}
+    out["fp64"]["frac_of_fp64_16op_roofline"] = out["fp64"]["gpairs"] / fp64_peak(mhz)
+    out["fp32c"]["frac_of_fp32_16op_roofline"] = out["fp32c"]["gpairs"] / (
+        SMS * 128 * mhz * 1e6 / FMA_OPS_PER_PAIR / 1e9)
+    out["reference_published_steps_per_s"] = {
+        "value": 3866, "hardware": "2x Xeon Gold 6148, 40 cores, AVX512-RSQRT-4I, Euler, eps=0",
+        "source": "final_results/single_node_combined.csv:10"}
+    return out
+
+
+def measure_large(ctx, l2_flush, mhz, n=1048576, steps=5, seed=2):
+    """The large single system: Plummer N = 1048576 (seed 2), eps = 1e-3, KDK
+    dt = 5e-4 for 5 steps, FP32C and FP64 (each the default kernel for this
+    size), plus the FP32C force error against FP64 on all particles."""
+    import numpy as np
+    import nbr
+    s = nbr.plummer(n, seed)
+    eps2 = 1e-6
+    pairs = float(n) * float(n - 1)
+    out = {"workload": f"plummer_n{n}_seed{seed}_eps0.001_kdk_dt0.0005_{steps}steps"}
+    for prec, name in ((nbr.FP32C, "fp32c"), (nbr.FP64, "fp64")):
+        ctx.upload(s)
+        ctx.run(prec, nbr.KDK, 2, 5e-4, steps, eps2=eps2)  # capture + warm-up
+        ctx.upload(s)
+        l2_flush()
+        r = ctx.run(prec, nbr.KDK, 2, 5e-4, steps, eps2=eps2)
+        t = r["gpu_ms"] * 1e-3
+        cfg = ctx.get_force_config(prec, eps2)
+        out[name] = {"gpairs": r["pairs"] / t / 1e9, "steps_per_s": steps / t,
+                     "ms_per_step": 1e3 * t / steps, "force_evals": r["force_evals"],
+                     "config": list(cfg)}
+    ctx.upload(s)
+    a32 = ctx.forces(nbr.FP32C, eps2=eps2)
+    a64 = ctx.forces(nbr.FP64, eps2=eps2)
+    e = _rel(a32, a64)
+    out["fp32c_over_fp64"] = out["fp32c"]["gpairs"] / out["fp64"]["gpairs"]
+    out["fp32c_vs_fp64_force_median_rel_err"] = float(np.median(e))
+    out["fp32c_vs_fp64_force_max_rel_err"] = float(e.max())
+    out["fp32c"]["frac_of_16op_roofline"] = out["fp32c"]["gpairs"] / (
+        SMS * 128 * mhz * 1e6 / FMA_OPS_PER_PAIR / 1e9)
+    del a32, a64
     return out
 
 
@@ -523,6 +657,8 @@ def run_sharded(a, rank, world, local):
     from nbr_shard import ShardedSystem
 
     torch.cuda.set_device(local)
+    global SMS
+    SMS = torch.cuda.get_device_properties(local).multi_processor_count
     for k, v in (("MASTER_ADDR", "127.0.0.1"), ("MASTER_PORT", "29533"), ("RANK", str(rank)),
                  ("WORLD_SIZE", str(world))):
         os.environ.setdefault(k, v)
@@ -621,7 +757,7 @@ def run_sharded(a, rank, world, local):
                     "roofline": {"bound": "fp32_fma_pipe", "achieved": achieved, "peak": peak,
                                  "unit": UNIT, "frac": achieved / peak if achieved else None,
                                  "traffic": None,
-                                 "peak_source": f"{world} GPUs x 148 SMs x 128 FP32 lanes x rank-0 "
+                                 "peak_source": f"{world} GPUs x {SMS} SMs x 128 FP32 lanes x rank-0 "
                                                 "median SM clock / 16 FMA-pipe ops per pair",
                                  "kernel_ms_max_over_ranks": 1e3 * k_max},
                     "clocks": clk, "cpu_baseline": None, "collectives_per_step": 1}

@@ -270,6 +270,127 @@ int orc_ring_predict(size_t n, double R, double omega, size_t step, size_t steps
   return 0;
 }
 
+/* ------------------------------------------------------------ samplers ----
+ * The seeded synthetic systems the benchmark and the tests run on, restated
+ * here so that a process that must not load the product (the timed reference
+ * arm) can build the same inputs.  Same algorithms and the same generator as
+ * the product's samplers (nbr_ic_plummer & co.), so a seed gives the same bits:
+ *   - xoshiro256** (Blackman & Vigna, 2018) seeded through splitmix64;
+ *   - 53 random bits -> a double in [0, 1) or (0, 1];
+ *   - Plummer sphere in N-body units (G = M = 1, scale radius a = 3 pi / 16),
+ *     Aarseth, Henon & Wielen (1974): r = a / sqrt(X^(-2/3) - 1) with the
+ *     enclosed mass fraction X <= 0.999, speed q v_esc(r) with q by von Neumann
+ *     rejection from q^2 (1 - q^2)^(7/2) (bound 0.1), isotropic directions,
+ *     then centre of mass and momentum moved to zero;
+ *   - uniform ball by rejection from the cube [-1, 1]^3.
+ * tests/test_oracle.py checks bit-identity with the product's samplers. */
+typedef struct { unsigned long long s[4]; } orc_rng;
+
+static unsigned long long orc_splitmix64(unsigned long long* s) {
+  unsigned long long z = (*s += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+static unsigned long long orc_rotl(unsigned long long x, int k) { return (x << k) | (x >> (64 - k)); }
+static void orc_rng_seed(orc_rng* g, unsigned long long seed) {
+  unsigned long long z = seed;
+  for (int i = 0; i < 4; ++i) g->s[i] = orc_splitmix64(&z);
+}
+static unsigned long long orc_rng_next(orc_rng* g) {
+  unsigned long long* s = g->s;
+  const unsigned long long r = orc_rotl(s[1] * 5, 7) * 9, t = s[1] << 17;
+  s[2] ^= s[0]; s[3] ^= s[1]; s[1] ^= s[2]; s[0] ^= s[3];
+  s[2] ^= t; s[3] = orc_rotl(s[3], 45);
+  return r;
+}
+static double orc_u01(orc_rng* g) { return (double)(orc_rng_next(g) >> 11) * 0x1.0p-53; }
+static double orc_u01_pos(orc_rng* g) { return (double)((orc_rng_next(g) >> 11) + 1) * 0x1.0p-53; }
+
+static void orc_isotropic(orc_rng* g, double r, double* x, double* y, double* z) {
+  const double c = 1.0 - 2.0 * orc_u01(g);
+  const double ph = 2.0 * ORC_PI * orc_u01(g);
+  const double s = sqrt(fmax(0.0, 1.0 - c * c));
+  *x = r * s * cos(ph);
+  *y = r * s * sin(ph);
+  *z = r * c;
+}
+
+static void orc_recentre(size_t n, double* a, double* b, double* c, const double* m) {
+  long double sa = 0, sb = 0, sc = 0, sm = 0;
+  for (size_t i = 0; i < n; ++i) {
+    sa += (long double)m[i] * a[i]; sb += (long double)m[i] * b[i]; sc += (long double)m[i] * c[i];
+    sm += m[i];
+  }
+  if (sm <= 0) return;
+  const double ma = (double)(sa / sm), mb = (double)(sb / sm), mc = (double)(sc / sm);
+  for (size_t i = 0; i < n; ++i) { a[i] -= ma; b[i] -= mb; c[i] -= mc; }
+}
+
+static void orc_plummer_draw(size_t n, unsigned long long seed, double* x, double* y, double* z,
+                             double* vx, double* vy, double* vz) {
+  orc_rng g;
+  orc_rng_seed(&g, seed);
+  const double a = 3.0 * ORC_PI / 16.0;
+  const double vscale = sqrt(2.0 / a);
+  for (size_t i = 0; i < n; ++i) {
+    const double X = 0.999 * orc_u01_pos(&g);
+    const double r = a / sqrt(pow(X, -2.0 / 3.0) - 1.0);
+    orc_isotropic(&g, r, &x[i], &y[i], &z[i]);
+    double q, h;
+    do {
+      q = orc_u01(&g);
+      h = 0.1 * orc_u01(&g);
+    } while (h > q * q * pow(1.0 - q * q, 3.5));
+    const double v = q * vscale * pow(1.0 + r * r / (a * a), -0.25);
+    orc_isotropic(&g, v, &vx[i], &vy[i], &vz[i]);
+  }
+}
+
+/* Plummer sphere of n equal masses 1/n. */
+int orc_plummer(size_t n, unsigned long long seed, double* x, double* y, double* z, double* vx,
+                double* vy, double* vz, double* m) {
+  if (n == 0) return -1;
+  orc_plummer_draw(n, seed, x, y, z, vx, vy, vz);
+  for (size_t i = 0; i < n; ++i) m[i] = 1.0 / (double)n;
+  orc_recentre(n, x, y, z, m);
+  orc_recentre(n, vx, vy, vz, m);
+  return 0;
+}
+
+/* Plummer positions and velocities; the first n_heavy particles are `ratio`
+ * times heavier than the rest, total mass 1. */
+int orc_two_component(size_t n, size_t n_heavy, double ratio, unsigned long long seed, double* x,
+                      double* y, double* z, double* vx, double* vy, double* vz, double* m) {
+  if (n == 0 || n_heavy > n || !(ratio > 0.0)) return -1;
+  orc_plummer_draw(n, seed, x, y, z, vx, vy, vz);
+  const double ml = 1.0 / ((double)(n - n_heavy) + ratio * (double)n_heavy);
+  for (size_t i = 0; i < n; ++i) m[i] = i < n_heavy ? ratio * ml : ml;
+  orc_recentre(n, x, y, z, m);
+  orc_recentre(n, vx, vy, vz, m);
+  return 0;
+}
+
+/* n equal masses uniform in the unit ball, at rest. */
+int orc_uniform_ball(size_t n, unsigned long long seed, double* x, double* y, double* z, double* vx,
+                     double* vy, double* vz, double* m) {
+  if (n == 0) return -1;
+  orc_rng g;
+  orc_rng_seed(&g, seed);
+  for (size_t i = 0; i < n; ++i) {
+    double a, b, c;
+    do {
+      a = 2.0 * orc_u01(&g) - 1.0;
+      b = 2.0 * orc_u01(&g) - 1.0;
+      c = 2.0 * orc_u01(&g) - 1.0;
+    } while (a * a + b * b + c * c > 1.0);
+    x[i] = a; y[i] = b; z[i] = c;
+    vx[i] = vy[i] = vz[i] = 0.0;
+    m[i] = 1.0 / (double)n;
+  }
+  return 0;
+}
+
 int orc_num_threads(void) {
 #ifdef _OPENMP
   return omp_get_max_threads();

@@ -22,6 +22,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 _D = C.POINTER(C.c_double)
 _SZ = C.c_size_t
+# State arrays of a system, in the order the samplers fill them.
+KEYS = ("x", "y", "z", "vx", "vy", "vz", "m")
 
 # Reference force kernels selectable through ref_forces().
 REF_SIMPLE, REF_AVX2, REF_AVX2_BLOCKED, REF_AVX512_RSQRT, REF_AVX512_RSQRT_4I = range(5)
@@ -69,6 +71,12 @@ class Oracle:
         L.orc_ring_predict.argtypes = [_SZ, C.c_double, C.c_double, _SZ, _SZ] + [_D] * 6
         L.orc_ring_predict.restype = C.c_int
         L.orc_num_threads.restype = C.c_int
+        samp = [_SZ, C.c_ulonglong] + [_D] * 7
+        for name in ("orc_plummer", "orc_uniform_ball"):
+            getattr(L, name).argtypes = samp
+            getattr(L, name).restype = C.c_int
+        L.orc_two_component.argtypes = [_SZ, _SZ, C.c_double, C.c_ulonglong] + [_D] * 7
+        L.orc_two_component.restype = C.c_int
 
     def accel(self, x, y, z, m, G=1.0, eps2=0.0, extended=False):
         n = len(x)
@@ -129,6 +137,23 @@ class Oracle:
             raise ValueError("ring needs n >= 2")
         keys = ("x", "y", "z", "vx", "vy", "vz", "m", "fx", "fy", "fz")
         return dict(zip(keys, arrs))
+
+    def _sample(self, fn, n, *args):
+        s = {k: np.zeros(n) for k in KEYS}
+        if fn(n, *args, *[_p(s[k]) for k in KEYS]) != 0:
+            raise ValueError("bad sampler arguments")
+        return s
+
+    def plummer(self, n, seed):
+        """Plummer sphere of n equal masses, the same bits as the product's
+        nbr_ic_plummer for the same seed."""
+        return self._sample(self.lib.orc_plummer, n, seed)
+
+    def uniform_ball(self, n, seed):
+        return self._sample(self.lib.orc_uniform_ball, n, seed)
+
+    def two_component(self, n, n_heavy, ratio, seed):
+        return self._sample(self.lib.orc_two_component, n, n_heavy, ratio, seed)
 
     def ring_predict(self, n, step, steps_per_rev, R=1.0, omega=2 * np.pi):
         arrs = [np.zeros(n) for _ in range(6)]

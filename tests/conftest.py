@@ -18,6 +18,10 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PKG = os.path.join(ROOT, "n-body-ring-solver_b200")
 ORACLE_DIR = os.path.join(ROOT, "oracle")
 GOLDEN = os.path.join(ROOT, "tests", "golden")
+# The reference checkout, where present (this container only; GPU tests never
+# read it): $NBR_REFERENCE_DIR, else the directory "reference" beside the repo.
+REFERENCE_CPU = os.path.join(os.path.abspath(os.environ.get("NBR_REFERENCE_DIR")
+                                             or os.path.join(ROOT, os.pardir, "reference")), "CPU")
 for p in (PKG, ORACLE_DIR):
     if p not in sys.path:
         sys.path.insert(0, p)

@@ -1,9 +1,11 @@
 """The reference arm of bench.py on the host cores (no GPU).
 
-`bench.py --impl reference` times the reference's own CPU force kernel, built
-from its sources into oracle/_ref, on the bench workload's inputs; its one
-JSON line must carry the keys the driver reads.  A small N keeps the run to
-seconds.
+`bench.py --impl reference` times the reference's own CPU solver, built from
+its sources into oracle/_ref, on the bench workload's inputs: its fastest force
+kernel (the line's value) and its end-to-end leapfrog solver
+reduced_solver_omp_lf (the line's e2e).  Its one JSON line must carry the keys
+the driver reads, and the process must never load the product library (the
+inputs come from the oracle's samplers).  A small N keeps the run to seconds.
 """
 import json
 import os
@@ -16,9 +18,13 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def test_reference_arm_json_line():
-    p = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
-                        "--n", "4096", "--steps", "2", "--warmup", "1"],
-                       capture_output=True, text=True, cwd=ROOT, timeout=600)
+    # run bench.py's main, then report on stderr whether libnbr.so was mapped
+    probe = ("import runpy, sys; sys.argv = ['bench.py', '--impl', 'reference', '--n', '4096', "
+             "'--steps', '2', '--warmup', '1']; runpy.run_path('bench.py', run_name='__main__'); "
+             "maps = open('/proc/self/maps').read(); "
+             "sys.stderr.write('LIBNBR_MAPPED=%d' % ('libnbr.so' in maps))")
+    p = subprocess.run([sys.executable, "-c", probe], capture_output=True, text=True, cwd=ROOT,
+                       timeout=600)
     assert p.returncode == 0, p.stderr[-2000:]
     lines = [l for l in p.stdout.splitlines() if l.strip()]
     assert len(lines) == 1, p.stdout
@@ -34,6 +40,10 @@ def test_reference_arm_json_line():
     cb = line["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["sample"]
     assert cb["value"] == line["value"]
+    assert set(cb["legs"]) == {"force_only", "end_to_end", "config0"}
     e2e = line["e2e"]
-    assert e2e["value"] == line["value"] and e2e["unit"] == line["unit"]
+    assert e2e["value"] > 0 and e2e["unit"] == line["unit"] and e2e["steps"] >= 1
+    assert e2e["value"] == cb["legs"]["end_to_end"]["value"]
     assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
+    assert line["config0"]["steps_per_s"] > 0
+    assert "LIBNBR_MAPPED=0" in p.stderr, p.stderr[-500:]

@@ -9,7 +9,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from conftest import PKG, ROOT
+from conftest import PKG, REFERENCE_CPU, ROOT
 
 HEADERS = [os.path.join(ROOT, "include", f) for f in sorted(os.listdir(os.path.join(ROOT, "include")))
            if f.endswith(".h")]
@@ -147,7 +147,7 @@ def test_adapter_header_compiles_with_reference_layout(tmp_path):
 
 
 def test_adapter_compiles_against_reference_header(tmp_path):
-    ref = "/root/reference/CPU"
+    ref = REFERENCE_CPU
     if not os.path.isdir(ref):
         pytest.skip("reference sources not present")
     src = tmp_path / "t.cpp"

@@ -155,3 +155,16 @@ def test_oracle_subset_matches_full(oracle, nbr):
     full = oracle.accel(s["x"], s["y"], s["z"], s["m"], eps2=1e-6, extended=True)
     sub = oracle.accel_subset(s["x"], s["y"], s["z"], s["m"], idx, eps2=1e-6)
     np.testing.assert_array_equal(sub, full[:, idx])
+
+
+@pytest.mark.parametrize("kind, args", [("plummer", (2048, 0)), ("plummer", (262144, 2)),
+                                        ("plummer", (1000, 7)), ("uniform_ball", (32768, 1)),
+                                        ("two_component", (131072, 1311, 1000.0, 4))])
+def test_oracle_samplers_are_bit_identical_to_the_products(oracle, nbr, kind, args):
+    """The oracle's samplers build the benchmark inputs in processes that must
+    not load the product (the timed reference arm); they must give exactly
+    the product's inputs."""
+    a = getattr(oracle, kind)(*args)
+    b = getattr(nbr, kind)(*args)
+    for k in ("x", "y", "z", "vx", "vy", "vz", "m"):
+        assert np.array_equal(a[k], b[k]), k
