@@ -147,6 +147,8 @@ int nbr_forces_download(nbr_ctx* ctx, double* ax, double* ay, double* az);
  *  - the first call on a device looks up the scratch array's device address
  *    (cudaGetSymbolAddress, with that device current); make that first call
  *    before any stream capture;
+ *  - the looked-up address is kept for the life of the process: after a
+ *    cudaDeviceReset of a device, do not call this entry point on it again;
  *  - all calls on a device share the scratch array, which keeps the last
  *    call's contents (each call clears what must start at zero); calls that
  *    overlap on the same GPU, from several streams or host threads, race on it

@@ -59,7 +59,10 @@ std::mutex g_setup_mu;
 unsigned char* g_scratch_addr[kMaxDevices] = {};
 
 // Device address of the scratch on the current device, looked up once per
-// device (with that device current) on its first call.
+// device (with that device current) on its first call and kept for the life
+// of the process.  A cudaDeviceReset on that device unloads the module and
+// invalidates the kept address, so a caller must not use this entry point on
+// a device after resetting it.
 int scratch_address(int device, unsigned char** out) {
   std::lock_guard<std::mutex> lock(g_setup_mu);
   if (!g_scratch_addr[device]) {
@@ -97,8 +100,9 @@ extern "C" int nbr_forces_noalloc(int precision, size_t n, const double* x, cons
   unsigned char* base = nullptr;
   int rc = scratch_address(device, &base);
   if (rc) return rc;
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  int sms = 0;
+  e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaDeviceGetAttribute(SM count)");
 
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const long long nn = (long long)n;
@@ -140,6 +144,7 @@ extern "C" int nbr_forces_noalloc(int precision, size_t n, const double* x, cons
                                                                (long long)ntiles}));
   IParticles ip{X, Y, Z, M, nn};
   JStream js{X, Y, Z, M, rec, org, ntiles, kWaitLimitNs, -1};
+  pipeline_params(js);  // NBR_WAIT_LIMIT_MS, and the NBR_TEST_SKIP_TILE test hook
   Epilogue ep{};
   ep.mode = 0;
   ep.G = G;

@@ -63,4 +63,26 @@ with nbr.Context(0) as ctx:
             out[f"batch_{prec}_{wide}"] = float(np.abs(a).sum())
     ctx.batch_diagnostics(eps2=1e-6)
     calls += 1
+# the no-allocation entry point: its scratch regions inside the static array
+# are checked against their own lengths
+import ctypes as C  # noqa: E402
+import torch  # noqa: E402
+lib = nbr.load()
+fna = lib.nbr_forces_noalloc
+fna.argtypes = [C.c_int, C.c_size_t] + [C.c_void_p] * 4 + [C.c_double, C.c_double] + [C.c_void_p] * 4
+fna.restype = C.c_int
+for n in (1, 128, 1025, 32768):
+    s = nbr.plummer(n, 50 + n)
+    dev = {k: torch.from_numpy(s[k]).cuda() for k in ("x", "y", "z", "m")}
+    for prec in (FP64, FP32C):
+        a = torch.zeros((3, n), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        rc = fna(prec, n, dev["x"].data_ptr(), dev["y"].data_ptr(), dev["z"].data_ptr(),
+                 dev["m"].data_ptr(), 1.0, 1e-6, a[0].data_ptr(), a[1].data_ptr(), a[2].data_ptr(),
+                 C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        if rc != 0:
+            raise SystemExit(f"nbr_forces_noalloc n={n} prec={prec}: status {rc}: "
+                             f"{lib.nbr_last_error_string(None)}")
+        calls += 1
+        out[f"noalloc_{n}_{prec}"] = float(a.abs().sum().item())
 print(json.dumps({"calls": calls, "results": out}))

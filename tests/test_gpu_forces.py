@@ -241,23 +241,39 @@ def test_potential_and_diagnostics(ctx, nbr, oracle):
     assert abs(d["M"] - 1.0) < 1e-13
 
 
+# Worst-particle bound of the FP32C kernels at full size, against the
+# extended-precision oracle.  The error of the worst particles comes from
+# close pairs: source and receiver coordinates are rounded to FP32 relative to
+# the FP64 origin of the source tile (a tile is 128 particles in index order,
+# so it spans the system), and for a pair much closer than that distance the
+# rounding of the two coordinates is a large fraction of their difference.
+# Accumulation is not the cause: summing the same FP32 pair terms in FP64
+# changes the worst errors by under 10 %.  The median stays near 4e-8.
+FP32C_WORST = {262144: 5e-4, 1048576: 2e-3}
+
+
 @pytest.mark.parametrize("n,seed", [(262144, 2), (1048576, 2)])
 def test_full_size_plummer_sampled(ctx, nbr, oracle, n, seed):
-    """Full-size Plummer systems: sampled receivers against the
-    extended-precision oracle, and Newton's third law over all particles."""
+    """Full-size Plummer systems: random receivers and the 64 worst particles
+    of the FP32C-vs-FP64 comparison over all particles, against the
+    extended-precision oracle; Newton's third law over all particles."""
     s = nbr.plummer(n, seed)
     upload(ctx, s)
     eps2 = 1e-6
     a64 = ctx.forces(FP64, eps2=eps2)
     a32 = ctx.forces(FP32C, eps2=eps2)
-    idx = np.random.default_rng(0).choice(n, 256, replace=False)
-    ref = oracle.accel_subset(s["x"], s["y"], s["z"], s["m"], idx, eps2=eps2)
-    assert rel_err(a64[:, idx], ref).max() <= 1e-12
-    e32 = rel_err(a32[:, idx], ref)
-    assert np.median(e32) <= 1e-6
-    # FP32C against FP64 over every particle
     eall = rel_err(a32, a64)
     assert np.median(eall) <= 1e-6
+    rnd = np.random.default_rng(0).choice(n, 192, replace=False)
+    worst = np.argsort(eall)[-64:]
+    idx = np.concatenate([rnd, worst])
+    ref = oracle.accel_subset(s["x"], s["y"], s["z"], s["m"], idx, eps2=eps2)
+    # FP64 is exact to 1e-12 on every sampled particle, the worst included,
+    # so the FP32C-vs-FP64 error is the FP32C kernel's own
+    assert rel_err(a64[:, idx], ref).max() <= 1e-12
+    e32 = rel_err(a32[:, idx], ref)
+    assert np.median(e32[:192]) <= 1e-6, np.median(e32[:192])
+    assert e32.max() <= FP32C_WORST[n], e32.max()
     # total momentum change sum m a ~ 0 relative to sum m |a|
     for a in (a64, a32):
         net = np.abs((a * s["m"]).sum(axis=1)).max()

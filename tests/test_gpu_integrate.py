@@ -146,18 +146,38 @@ def test_higher_order_is_more_accurate(ctx, nbr, order):
     assert errs[order] < errs[2] / 10
 
 
-def test_fp32c_energy_drift_within_twice_fp64(ctx, nbr):
-    """Cold collapse of a uniform ball (N = 32768, eps = 1e-2, dt = 1e-4): the
-    FP32C run conserves energy as well as the FP64 run (within 2x, plus a
-    floor at the FP64 diagnostic's own precision)."""
-    s = nbr.uniform_ball(32768, 1)
-    drift = {}
+def _drifts(ctx, s, dt, steps, eps2):
+    out = {}
     for prec in (FP64, FP32C):
         ctx.upload(s)
-        st = ctx.run(prec, KDK, 2, 1e-4, 200, eps2=1e-4, diag=True)
+        st = ctx.run(prec, KDK, 2, dt, steps, eps2=eps2, diag=True)
         e0, e1 = st["diag"]
-        drift[prec] = abs(e1["E"] - e0["E"]) / abs(e0["E"])
-    assert drift[FP32C] <= 2 * drift[FP64] + 1e-9, drift
+        out[prec] = abs(e1["E"] - e0["E"]) / abs(e0["E"])
+    return out
+
+
+# Floor: the FP64 diagnostic's own rounding (E is a sum of O(N) FP64 terms
+# of either sign, relative rounding ~1e-15 .. 1e-14).
+DRIFT_FLOOR = 1e-14
+
+
+def test_fp32c_energy_drift_within_twice_fp64(ctx, nbr):
+    """Plummer N = 20000 (eps = 1e-3, dt = 1e-3, 50 KDK steps), where the
+    integrator's own error sets the drift: the FP32C run conserves energy
+    within 2x of the FP64 run."""
+    d = _drifts(ctx, nbr.plummer(20000, 2), 1e-3, 50, 1e-6)
+    assert d[FP64] > 10 * DRIFT_FLOOR, d
+    assert d[FP32C] <= 2 * d[FP64] + DRIFT_FLOOR, d
+
+
+def test_fp32c_energy_drift_cold_collapse(ctx, nbr):
+    """Cold collapse of a uniform ball (N = 32768, eps = 1e-2, dt = 1e-4, 200
+    steps): the FP64 drift here is ~1e-12, below the level of FP32 pair
+    rounding, so the FP32C drift is larger: stated bound 6x the FP64 drift
+    (measured ~4x), and both under 1e-10."""
+    d = _drifts(ctx, nbr.uniform_ball(32768, 1), 1e-4, 200, 1e-4)
+    assert d[FP64] <= 1e-10 and d[FP32C] <= 1e-10, d
+    assert d[FP32C] <= 6 * d[FP64] + DRIFT_FLOOR, d
 
 
 def test_fp32c_trajectory_tracks_fp64(ctx, nbr):

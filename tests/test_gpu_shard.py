@@ -81,7 +81,11 @@ def _emulated_run(nbr, s, precision, scheme, dt, steps, world, eps2):
 @pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "fp32c"])
 @pytest.mark.parametrize("scheme", [0, 2], ids=["kdk", "euler"])
 @pytest.mark.parametrize("n,world", [(8192, 2), (5000, 3)])
-def test_emulated_ranks_match_whole_run(nbr, precision, scheme, n, world):
+def test_emulated_ranks_match_whole_run(nbr, oracle, precision, scheme, n, world):
+    """Bit for bit against one whole-system run, and directly against the
+    oracle's trajectory (KDK or Euler in FP64, every ordered pair in index
+    order): FP64 within 1e-11, FP32C within 1e-6 (absolute, positions and
+    velocities of order 1)."""
     s = nbr.plummer(n, 5)
     eps2, dt, steps = 1e-6, 1e-3, 3
     whole = nbr.Context(0)
@@ -93,6 +97,11 @@ def test_emulated_ranks_match_whole_run(nbr, precision, scheme, n, world):
     got = _emulated_run(nbr, s, precision, scheme, dt, steps, world, eps2)
     for k in ("x", "y", "z", "vx", "vy", "vz"):
         np.testing.assert_array_equal(got[k], ref[k], err_msg=k)
+    want = (oracle.kdk(s, dt, steps, eps2=eps2) if scheme == nbr.KDK
+            else oracle.euler(s, dt, steps, eps2=eps2))
+    tol = 1e-11 if precision == nbr.FP64 else 1e-6
+    for k in ("x", "y", "z", "vx", "vy", "vz"):
+        assert np.abs(got[k] - want[k]).max() <= tol, k
 
 
 def test_step_range_matches_oracle_forces(nbr, oracle):
