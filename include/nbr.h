@@ -267,10 +267,24 @@ int nbr_snapshot_load(nbr_ctx* ctx, const char* path, size_t n, size_t record, d
  * thread: 4 or 8; warps per CTA: 2, 4 or 8; split >= 1 or 0 = automatic;
  * ni = 1: the small-N kernel with warps = 2, 4 or 8 lane groups per warp;
  * ni = 3, warps = 8: the Newton-3 kernel, each unordered pair evaluated once
- * and applied to both particles, for FP32C and for FP64; whole systems of at
- * most 2^20 particles, other calls fall back to the large kernels).  ni = 0
+ * and applied to both particles, for FP32C and for FP64; for FP32C also
+ * warps = 16, two warps per 256-particle row block; whole systems of at most
+ * 2^20 particles, other calls fall back to the large kernels; ni = 2, FP64
+ * only, warps = 4, 8 or 16 lane groups: nbr_run of a system of at most 4096
+ * particles as one cooperative launch for all steps (the default for such
+ * systems), evaluations outside nbr_run use the default kernels).  ni = 0
  * restores the autotuner. */
 int nbr_set_force_config(nbr_ctx* ctx, int precision, int ni, int warps, int split);
+/* The j-tile (sources per stage of the shared-memory ring: 64, 128 or 256)
+ * and the unroll depth of the source loop (2, 4 or 8) of the large kernels,
+ * for a configuration forced with nbr_set_force_config (ni 4 or 8); 0 takes
+ * the default (128; unroll 4 for FP32C, 2 for FP64).  Built for the default
+ * large configurations FP32C (8, 2) and FP64 (4, 4); other (tile, unroll)
+ * pairs return NBR_ERR_INVALID_ARG. */
+int nbr_set_force_tiling(nbr_ctx* ctx, int precision, int tile, int unroll);
+/* The j-tile and unroll depth a force evaluation of the uploaded system would
+ * use (0 and 0 when the chosen kernel is not a large one). */
+int nbr_get_force_tiling(nbr_ctx* ctx, int precision, double eps2, int* tile, int* unroll);
 /* The configuration a force evaluation of the uploaded system would use
  * (forced, autotuned or default): ni = 4 or 8 receivers per thread of the
  * large kernels, ni = 1 the small-N kernel (warps = lane groups per warp),
@@ -279,7 +293,12 @@ int nbr_set_force_config(nbr_ctx* ctx, int precision, int ni, int warps, int spl
  * Newton-3 kernel). */
 int nbr_get_force_config(nbr_ctx* ctx, int precision, double eps2, int* ni, int* warps, int* split);
 /* Times the supported configurations for the uploaded system and stores the
- * fastest in the autotune cache file (see nbr_tune_cache_path). */
+ * fastest in the autotune cache file (see nbr_tune_cache_path) under the
+ * system's (precision, log2 N, log2 source tiles, eps == 0) bucket: receivers
+ * per thread and warps per CTA (the i-tile), three j-splits, the small-N and
+ * Newton-3 kernels, and, when the large kernel's default configuration wins,
+ * its j-tile (64, 128, 256) and unroll depth (2, 4, 8).  Later evaluations in
+ * the same bucket use the stored winner. */
 int nbr_autotune(nbr_ctx* ctx, int precision, double eps2);
 /* Path of the JSON autotune cache ($NBR_TUNE_CACHE or the library directory). */
 const char* nbr_tune_cache_path(void);

@@ -84,6 +84,7 @@ bool RunKey::operator==(const RunKey& o) const {
       G != o.G || eps2 != o.eps2 || steps != o.steps || n != o.n || cap != o.cap ||
       fsal != o.fsal || cur != o.cur || rec_ok[0] != o.rec_ok[0] || rec_ok[1] != o.rec_ok[1] ||
       cfg.ni != o.cfg.ni || cfg.warps != o.cfg.warps || cfg.split != o.cfg.split ||
+      cfg.tile != o.cfg.tile || cfg.unroll != o.cfg.unroll ||
       wait_ns != o.wait_ns || skip_tile != o.skip_tile)
     return false;
   for (int i = 0; i < 6; ++i)
@@ -230,7 +231,8 @@ std::string tune_key(int precision, long long n_i, int ntiles, bool excl) {
   return k.str();
 }
 
-// The cache is a flat JSON object {"key": [ni, warps, split], ...}.
+// The cache is a flat JSON object {"key": [ni, warps, split, tile, unroll], ...}
+// (entries with three numbers leave tile and unroll at their defaults).
 void load_tune_locked() {
   if (g_tune) return;
   g_tune = new std::map<std::string, ForceConfig>();
@@ -249,9 +251,11 @@ void load_tune_locked() {
     size_t lb = s.find('[', q), rb = s.find(']', q);
     if (lb == std::string::npos || rb == std::string::npos) break;
     ForceConfig c{0, 0, 0};
-    if (std::sscanf(s.c_str() + lb + 1, "%d , %d , %d", &c.ni, &c.warps, &c.split) == 3 &&
-        force_config_supported(0, c))
-      (*g_tune)[key] = c;
+    const int got = std::sscanf(s.c_str() + lb + 1, "%d , %d , %d , %d , %d", &c.ni, &c.warps,
+                                &c.split, &c.tile, &c.unroll);
+    const int prec = key.compare(0, 5, "fp32c") == 0 ? kFP32C : kFP64;
+    if (got < 5) c.tile = c.unroll = 0;
+    if (got >= 3 && force_config_supported(prec, c)) (*g_tune)[key] = c;
     p = rb + 1;
   }
 }
@@ -263,7 +267,8 @@ void save_tune_locked() {
   size_t k = 0;
   for (auto& kv : *g_tune) {
     f << "  \"" << kv.first << "\": [" << kv.second.ni << ", " << kv.second.warps << ", "
-      << kv.second.split << "]" << (++k < g_tune->size() ? ",\n" : "\n");
+      << kv.second.split << ", " << kv.second.tile << ", " << kv.second.unroll << "]"
+      << (++k < g_tune->size() ? ",\n" : "\n");
   }
   f << "}\n";
 }
@@ -305,6 +310,7 @@ int auto_split(int precision, double eps2, const ForceConfig& c, long long n_i, 
 
 ForceConfig choose_config(nbr_ctx* c, int precision, double eps2, long long n_i, int ntiles) {
   ForceConfig cfg = c->override_cfg[precision];
+  if (cfg.ni == kPersistNI) cfg = ForceConfig{0, 0, 0};  // a run-level choice: evaluations use the default
   if (cfg.ni == 0) {
     std::lock_guard<std::mutex> g(g_tune_mu);
     load_tune_locked();
@@ -327,7 +333,10 @@ ForceConfig choose_config(nbr_ctx* c, int precision, double eps2, long long n_i,
     cfg = it != g_tune->end() ? it->second : dflt;
   }
   if (cfg.split <= 0) cfg.split = auto_split(precision, eps2, cfg, n_i, ntiles, c->sms);
-  if (cfg.split > ntiles) cfg.split = std::max(1, ntiles);
+  // at most one split per ring stage of sources (j-tile: 128 by default)
+  const int tj = (cfg.ni == 4 || cfg.ni == 8) && cfg.tile > 0 ? cfg.tile : kTile;
+  const int stages = (int)(((long long)ntiles * kTile + tj - 1) / tj);
+  if (cfg.split > stages) cfg.split = std::max(1, stages);
   return cfg;
 }
 
@@ -452,8 +461,8 @@ int eval_system(nbr_ctx* c, int precision, double G, double eps2, int mode, doub
       // test hook: under-report the receivers' length so that the check trips
       if (std::getenv("NBR_TEST_SHRINK_BOUNDS")) ip.len = rn - 1;)
   if (cfg.ni == 3) {
-    e = launch_force_n3(precision, eps2, ip, js, ep, c->scr.part, (long long)c->scr.part_cap,
-                        c->stream);
+    e = launch_force_n3(precision, cfg.warps, eps2, ip, js, ep, c->scr.part,
+                        (long long)c->scr.part_cap, c->stream);
     if (kernels) *kernels += 2;
   } else {
     e = launch_force(precision, eps2, cfg, ip, js, ep, c->stream);
@@ -628,6 +637,7 @@ int nbr_ctx_create(int device, nbr_ctx** out) {
   nbr_ctx* c = new nbr_ctx();
   c->device = device;
   c->sms = prop.multiProcessorCount;
+  c->coop = prop.cooperativeLaunch != 0;
   e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
@@ -995,7 +1005,20 @@ int nbr_run(nbr_ctx* c, int precision, int scheme, int order, double dt, size_t 
     if (rc) return rc;
   }
   nbr_run_stats st{};
-  if (steps > 0) {
+  if (steps > 0 && persistent_run_applies(c, precision, s.n)) {
+    // small FP64 systems: every step in one cooperative launch
+    const bool fsal = (scheme == NBR_KDK) && c->acc_ok && c->acc_prec == precision &&
+                      c->acc_G == G && c->acc_eps2 == eps2;
+    rc = run_persistent(c, precision, scheme, dt, steps, G, eps2, fsal, cc, dd, lf, &st);
+    if (rc) {
+      c->acc_ok = false;
+      return rc;
+    }
+    c->acc_ok = scheme == NBR_KDK;
+    c->acc_prec = precision;
+    c->acc_G = G;
+    c->acc_eps2 = eps2;
+  } else if (steps > 0) {
     // Allocate everything the sequence needs before capture.
     ForceConfig cfg = choose_config(c, precision, eps2, (long long)s.n, s.ntiles);
     rc = prepare_split(c, cfg, (long long)s.n_pad);
@@ -1144,6 +1167,39 @@ int nbr_set_force_config(nbr_ctx* c, int precision, int ni, int warps, int split
   return NBR_OK;
 }
 
+int nbr_set_force_tiling(nbr_ctx* c, int precision, int tile, int unroll) {
+  if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
+  if (precision != NBR_FP64 && precision != NBR_FP32C)
+    return fail(c, NBR_ERR_INVALID_ARG, "unknown precision");
+  ForceConfig cfg = c->override_cfg[precision];
+  if (cfg.ni != 4 && cfg.ni != 8)
+    return fail(c, NBR_ERR_INVALID_ARG, "force a large-kernel configuration (ni 4 or 8) first");
+  cfg.tile = tile;
+  cfg.unroll = unroll;
+  ForceConfig probe = cfg;
+  if (probe.split < 1) probe.split = 1;
+  if (!force_config_supported(precision, probe))
+    return fail(c, NBR_ERR_INVALID_ARG, "unsupported (tile, unroll) for this configuration");
+  c->override_cfg[precision] = cfg;
+  return NBR_OK;
+}
+
+int nbr_get_force_tiling(nbr_ctx* c, int precision, double eps2, int* tile, int* unroll) {
+  if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
+  if (precision != NBR_FP64 && precision != NBR_FP32C)
+    return fail(c, NBR_ERR_INVALID_ARG, "unknown precision");
+  SysState& s = c->sys;
+  if (s.n == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no system uploaded");
+  cudaSetDevice(c->device);
+  ForceConfig cfg = choose_config(c, precision, eps2, (long long)s.n, s.ntiles);
+  if (cfg.ni == 3 && (long long)s.n > kN3MaxN)
+    cfg = choose_config_large(c, precision, eps2, (long long)s.n, s.ntiles);
+  const bool large = cfg.ni == 4 || cfg.ni == 8;
+  if (tile) *tile = large ? (cfg.tile > 0 ? cfg.tile : kDefaultTileJ) : 0;
+  if (unroll) *unroll = large ? (cfg.unroll > 0 ? cfg.unroll : default_unroll(precision)) : 0;
+  return NBR_OK;
+}
+
 int nbr_get_force_config(nbr_ctx* c, int precision, double eps2, int* ni, int* warps, int* split) {
   if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
   if (precision != NBR_FP64 && precision != NBR_FP32C)
@@ -1175,12 +1231,14 @@ int nbr_autotune(nbr_ctx* c, int precision, double eps2) {
   if (s.n == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no system uploaded");
   cudaSetDevice(c->device);
   const ForceConfig saved = c->override_cfg[precision];
-  const int cand[][2] = {{4, 2}, {4, 4}, {4, 8}, {8, 2}, {8, 4}, {1, 2}, {1, 4}, {1, 8}, {3, 8}};
+  const int cand[][2] = {{4, 2}, {4, 4}, {4, 8}, {8, 2}, {8, 4}, {1, 2},
+                         {1, 4}, {1, 8}, {3, 8}, {3, 16}};
   ForceConfig best{0, 0, 0};
   float best_ms = 1e30f;
   for (auto& cw : cand) {
     if (cw[0] == 1 && s.n > 65536) continue;  // the small-N kernel only competes on small systems
     if (cw[0] == 3 && (s.n < 8192 || (long long)s.n > kN3MaxN)) continue;
+    if (cw[0] == 3 && cw[1] == 16 && precision != kFP32C) continue;  // FP64 has one Newton-3 layout
     ForceConfig base{cw[0], cw[1], 1};
     const int s0 = auto_split(precision, eps2, base, (long long)s.n, s.ntiles, c->sms);
     const int splits[] = {std::max(1, s0 / 2), s0, s0 * 2};
@@ -1203,6 +1261,35 @@ int nbr_autotune(nbr_ctx* c, int precision, double eps2) {
         best = ForceConfig{cw[0], cw[1], sp};
       }
     }
+  }
+  // The j-tile (sources per ring stage) and the unroll depth of the source
+  // loop, for the large kernel's default configuration when it won.
+  const bool large_default = (precision == kFP32C && best.ni == 8 && best.warps == 2) ||
+                             (precision == kFP64 && best.ni == 4 && best.warps == 4);
+  if (large_default) {
+    for (int tj : {64, 128, 256})
+      for (int u : {2, 4, 8}) {
+        ForceConfig cand = best;
+        cand.tile = tj;
+        cand.unroll = u;
+        if (!force_config_supported(precision, cand)) continue;
+        c->override_cfg[precision] = cand;
+        float tot = 0.f;
+        bool ok = true;
+        for (int rep = 0; rep < 3 && ok; ++rep) {
+          cudaEventRecord(c->ev0, c->stream);
+          ok = eval_system(c, precision, 1.0, eps2, 0, 0.0, 0.0, 0, nullptr) == NBR_OK;
+          cudaEventRecord(c->ev1, c->stream);
+          ok = ok && check_device_error(c) == NBR_OK;
+          float ms = 0.f;
+          cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+          if (rep > 0) tot += ms;
+        }
+        if (ok && tot < best_ms) {
+          best_ms = tot;
+          best = cand;
+        }
+      }
   }
   c->override_cfg[precision] = saved;
   c->acc_ok = false;

@@ -109,6 +109,13 @@ bool finite_array(const double* a, size_t n);
 int check_device_error(nbr_ctx* c);
 // Bounded-wait limit and tile-skip test hook from the environment.
 void pipeline_params(JStream& js);
+// The persistent small-system run (nbr_persist.cu): whether it serves an
+// nbr_run of this system, and the run itself (the schedule of nbr_run's
+// launch sequence; cc/dd/lf the Yoshida tables for DKD).
+bool persistent_run_applies(nbr_ctx* c, int precision, size_t n);
+int run_persistent(nbr_ctx* c, int precision, int scheme, double dt, size_t steps, double G,
+                   double eps2, bool fsal, const double* cc, const double* dd, int lf,
+                   nbr_run_stats* st);
 
 }  // namespace nbr
 
@@ -143,6 +150,7 @@ struct RunGraph {
 struct nbr_ctx {
   int device = 0;
   int sms = 148;
+  bool coop = false;       // the device supports cooperative launches
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::string err;

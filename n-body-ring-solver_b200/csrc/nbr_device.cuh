@@ -25,6 +25,7 @@ enum : int {
   kErrTileWait = 1,    // a j-tile's bulk copy did not complete in time
   kErrDrainWait = 2,   // draining in-flight copies after an abort timed out
   kErrBounds = 3,      // checked builds: an index outside its array (access skipped)
+  kErrGridWait = 4,    // a grid-wide barrier of a persistent launch did not complete in time
 };
 
 typedef unsigned long long u64;

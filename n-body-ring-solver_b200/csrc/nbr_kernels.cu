@@ -247,10 +247,22 @@ __device__ __forceinline__ void finish(const IParticles& ip, const Epilogue& ep,
 }
 
 // ------------------------------------------------------ FP32C kernel ----
-template <int NI, int WARPS, bool EXCL>
+// Stage bytes of the large FP32C kernel with TJ sources per stage: the
+// records plus the FP64 origins of the 128-particle tiles the stage spans (one
+// for TJ = 64, the origin of the tile it lies in).
+template <int TJ>
+__host__ __device__ constexpr int stage32_bytes() { return TJ * 48 + 32 * (TJ >= kTile ? TJ / kTile : 1); }
+
+// TJ: sources per ring stage (64, 128, 256); UNR: unroll depth of the source
+// loop.  The compensated sum works per 128-source tile (per 64 for TJ = 64),
+// whatever TJ is.
+template <int NI, int WARPS, bool EXCL, int TJ, int UNR>
 __global__ void __launch_bounds__(WARPS * 32)
     k_force_f32c(const IParticles ip, const JStream js, const Epilogue ep, const float eps2f) {
   constexpr int IPAIR = NI / 2;
+  constexpr int SUB = TJ >= kTile ? kTile : TJ;  // sources per origin
+  constexpr int NSUB = TJ / SUB;
+  constexpr int SB = stage32_bytes<TJ>();
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
   unsigned char* stages = smem + kSmemHead;
@@ -258,8 +270,9 @@ __global__ void __launch_bounds__(WARPS * 32)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const long long ibase = ((long long)blockIdx.x * WARPS + warp) * (32 * NI) + lane;
   const int S = gridDim.y, sp = blockIdx.y;
-  const int t0 = (int)((long long)js.ntiles * sp / S);
-  const int t1 = (int)((long long)js.ntiles * (sp + 1) / S);
+  const int nch = (int)(((long long)js.ntiles * kTile + TJ - 1) / TJ);  // stages of sources
+  const int t0 = (int)((long long)nch * sp / S);
+  const int t1 = (int)((long long)nch * (sp + 1) / S);
 
   double xi[NI], yi[NI], zi[NI];
 #pragma unroll
@@ -274,61 +287,69 @@ __global__ void __launch_bounds__(WARPS * 32)
   const u64 EPS2 = pack2(eps2f, eps2f);
 
   auto issue = [&](int st, int t) {
-    unsigned char* dst = stages + st * kStage32;
+    unsigned char* dst = stages + st * SB;
     const uint32_t bar = smem_u32(&bars[st]);
-    if (!NBR_IN((long long)(t0 + t + 1) * kTile - 1, js.len, ep.err)) return;  // the wait expires
-    mbar_expect_tx(bar, kStage32);
-    bulk_g2s(dst, js.rec + (size_t)(t0 + t) * kTile * 3, kRecBytes, bar);
-    bulk_g2s(dst + kRecBytes, js.origin + (t0 + t), 32, bar);
+    const long long first = (long long)(t0 + t) * TJ;  // first source of the stage
+    if (!NBR_IN(first + TJ - 1, js.len, ep.err)) return;  // the wait expires
+    mbar_expect_tx(bar, SB);
+    bulk_g2s(dst, js.rec + (size_t)first * 3, TJ * 48, bar);
+    bulk_g2s(dst + TJ * 48, js.origin + first / kTile, 32 * NSUB, bar);
   };
+  int tcur = t0;
   auto body = [&](int st) {
-    const unsigned char* base = stages + st * kStage32;
-    const double4 o = *reinterpret_cast<const double4*>(base + kRecBytes);
-    u64 XI[IPAIR], YI[IPAIR], ZI[IPAIR], AX[IPAIR], AY[IPAIR], AZ[IPAIR];
+    const unsigned char* base = stages + st * SB;
+    const long long first = (long long)(tcur++) * TJ;
 #pragma unroll
-    for (int p = 0; p < IPAIR; ++p) {
-      XI[p] = pack2(__double2float_rn(xi[2 * p] - o.x), __double2float_rn(xi[2 * p + 1] - o.x));
-      YI[p] = pack2(__double2float_rn(yi[2 * p] - o.y), __double2float_rn(yi[2 * p + 1] - o.y));
-      ZI[p] = pack2(__double2float_rn(zi[2 * p] - o.z), __double2float_rn(zi[2 * p + 1] - o.z));
-      AX[p] = AY[p] = AZ[p] = 0ull;
-    }
-    const ulonglong2* R = reinterpret_cast<const ulonglong2*>(base);
-#pragma unroll 4
-    for (int j = 0; j < kTile; ++j) {
-      const ulonglong2 q0 = R[3 * j];
-      const ulonglong2 q1 = R[3 * j + 1];
-      const u64 bj = R[3 * j + 2].x;
+    for (int sb = 0; sb < NSUB; ++sb) {
+      // a 128-tile past the system's last one holds no records of it
+      if (NSUB > 1 && (first + sb * SUB) / kTile >= js.ntiles) break;
+      const double4 o = *reinterpret_cast<const double4*>(base + TJ * 48 + 32 * sb);
+      u64 XI[IPAIR], YI[IPAIR], ZI[IPAIR], AX[IPAIR], AY[IPAIR], AZ[IPAIR];
 #pragma unroll
       for (int p = 0; p < IPAIR; ++p) {
-        const u64 dx = sub2(q0.x, XI[p]);
-        const u64 dy = sub2(q0.y, YI[p]);
-        const u64 dz = sub2(q1.x, ZI[p]);
-        u64 r2 = fma2(dx, dx, EPS2);
-        r2 = fma2(dy, dy, r2);
-        r2 = fma2(dz, dz, r2);
-        u64 y;
-        if (EXCL) {
-          float rl, rh;
-          unpack2(r2, rl, rh);
-          y = pack2(rl > 0.f ? rsqrt_mufu(rl) : 0.f, rh > 0.f ? rsqrt_mufu(rh) : 0.f);
-        } else {
-          y = rsqrt2(r2);
-        }
-        const u64 y2 = mul2(y, y);
-        const u64 pr = mul2(r2, y2);
-        const u64 mg = fma2(q1.y, pr, bj);
-        const u64 y3 = mul2(y2, y);
-        const u64 s = mul2(y3, mg);
-        AX[p] = fma2(s, dx, AX[p]);
-        AY[p] = fma2(s, dy, AY[p]);
-        AZ[p] = fma2(s, dz, AZ[p]);
+        XI[p] = pack2(__double2float_rn(xi[2 * p] - o.x), __double2float_rn(xi[2 * p + 1] - o.x));
+        YI[p] = pack2(__double2float_rn(yi[2 * p] - o.y), __double2float_rn(yi[2 * p + 1] - o.y));
+        ZI[p] = pack2(__double2float_rn(zi[2 * p] - o.z), __double2float_rn(zi[2 * p + 1] - o.z));
+        AX[p] = AY[p] = AZ[p] = 0ull;
       }
-    }
+      const ulonglong2* R = reinterpret_cast<const ulonglong2*>(base) + 3 * SUB * sb;
+#pragma unroll UNR
+      for (int j = 0; j < SUB; ++j) {
+        const ulonglong2 q0 = R[3 * j];
+        const ulonglong2 q1 = R[3 * j + 1];
+        const u64 bj = R[3 * j + 2].x;
 #pragma unroll
-    for (int p = 0; p < IPAIR; ++p) {
-      two_sum2(hx[p], lx[p], AX[p]);
-      two_sum2(hy[p], ly[p], AY[p]);
-      two_sum2(hz[p], lz[p], AZ[p]);
+        for (int p = 0; p < IPAIR; ++p) {
+          const u64 dx = sub2(q0.x, XI[p]);
+          const u64 dy = sub2(q0.y, YI[p]);
+          const u64 dz = sub2(q1.x, ZI[p]);
+          u64 r2 = fma2(dx, dx, EPS2);
+          r2 = fma2(dy, dy, r2);
+          r2 = fma2(dz, dz, r2);
+          u64 y;
+          if (EXCL) {
+            float rl, rh;
+            unpack2(r2, rl, rh);
+            y = pack2(rl > 0.f ? rsqrt_mufu(rl) : 0.f, rh > 0.f ? rsqrt_mufu(rh) : 0.f);
+          } else {
+            y = rsqrt2(r2);
+          }
+          const u64 y2 = mul2(y, y);
+          const u64 pr = mul2(r2, y2);
+          const u64 mg = fma2(q1.y, pr, bj);
+          const u64 y3 = mul2(y2, y);
+          const u64 s = mul2(y3, mg);
+          AX[p] = fma2(s, dx, AX[p]);
+          AY[p] = fma2(s, dy, AY[p]);
+          AZ[p] = fma2(s, dz, AZ[p]);
+        }
+      }
+#pragma unroll
+      for (int p = 0; p < IPAIR; ++p) {
+        two_sum2(hx[p], lx[p], AX[p]);
+        two_sum2(hy[p], ly[p], AY[p]);
+        two_sum2(hz[p], lz[p], AZ[p]);
+      }
     }
   };
   if (!tile_pipeline(bars, t1 - t0, js, ep.err, issue, body)) return;
@@ -350,10 +371,12 @@ __global__ void __launch_bounds__(WARPS * 32)
 // ------------------------------------------------------- FP64 kernel ----
 // The drop-in form: every operation in FP64, the reciprocal square root from
 // CUDA's rsqrt(double).  Matches the reference's double-precision forces up to
-// summation order.
-template <int NI, int WARPS, bool EXCL>
+// summation order.  TJ sources per ring stage (x, y, z, m: 32 TJ bytes), UNR
+// the unroll depth of the source loop.
+template <int NI, int WARPS, bool EXCL, int TJ, int UNR>
 __global__ void __launch_bounds__(WARPS * 32)
     k_force_f64(const IParticles ip, const JStream js, const Epilogue ep, const double eps2) {
+  constexpr int SB = 32 * TJ;
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
   unsigned char* stages = smem + kSmemHead;
@@ -361,8 +384,9 @@ __global__ void __launch_bounds__(WARPS * 32)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const long long ibase = ((long long)blockIdx.x * WARPS + warp) * (32 * NI) + lane;
   const int S = gridDim.y, sp = blockIdx.y;
-  const int t0 = (int)((long long)js.ntiles * sp / S);
-  const int t1 = (int)((long long)js.ntiles * (sp + 1) / S);
+  const int nch = (int)(((long long)js.ntiles * kTile + TJ - 1) / TJ);
+  const int t0 = (int)((long long)nch * sp / S);
+  const int t1 = (int)((long long)nch * (sp + 1) / S);
 
   double xi[NI], yi[NI], zi[NI], ax[NI], ay[NI], az[NI];
 #pragma unroll
@@ -374,23 +398,23 @@ __global__ void __launch_bounds__(WARPS * 32)
   }
 
   auto issue = [&](int st, int t) {
-    unsigned char* dst = stages + st * kStage64;
+    unsigned char* dst = stages + st * SB;
     const uint32_t bar = smem_u32(&bars[st]);
-    const size_t off = (size_t)(t0 + t) * kTile;
-    if (!NBR_IN((long long)off + kTile - 1, js.len, ep.err)) return;  // the wait expires
-    mbar_expect_tx(bar, kStage64);
-    bulk_g2s(dst, js.x + off, kTile * 8, bar);
-    bulk_g2s(dst + kTile * 8, js.y + off, kTile * 8, bar);
-    bulk_g2s(dst + 2 * kTile * 8, js.z + off, kTile * 8, bar);
-    bulk_g2s(dst + 3 * kTile * 8, js.m + off, kTile * 8, bar);
+    const size_t off = (size_t)(t0 + t) * TJ;
+    if (!NBR_IN((long long)off + TJ - 1, js.len, ep.err)) return;  // the wait expires
+    mbar_expect_tx(bar, SB);
+    bulk_g2s(dst, js.x + off, TJ * 8, bar);
+    bulk_g2s(dst + TJ * 8, js.y + off, TJ * 8, bar);
+    bulk_g2s(dst + 2 * TJ * 8, js.z + off, TJ * 8, bar);
+    bulk_g2s(dst + 3 * TJ * 8, js.m + off, TJ * 8, bar);
   };
   auto body = [&](int st) {
-    const double* sx = reinterpret_cast<const double*>(stages + st * kStage64);
-    const double* sy = sx + kTile;
-    const double* sz = sy + kTile;
-    const double* sm = sz + kTile;
-#pragma unroll 2
-    for (int j = 0; j < kTile; ++j) {
+    const double* sx = reinterpret_cast<const double*>(stages + st * SB);
+    const double* sy = sx + TJ;
+    const double* sz = sy + TJ;
+    const double* sm = sz + TJ;
+#pragma unroll UNR
+    for (int j = 0; j < TJ; ++j) {
       const double xj = sx[j], yj = sy[j], zj = sz[j], mj = sm[j];
 #pragma unroll
       for (int k = 0; k < NI; ++k) {
@@ -869,6 +893,233 @@ __global__ void __launch_bounds__(kN3Warps * 32)
   }
 }
 
+// Two warps per row block (ForceConfig {3, 16} for FP32C): the blocks, CTA
+// map, source rotation and partial-sum layout of k_force_n3_f32c, with 16
+// warps per CTA: warp w takes row block a = r0 + w / 2 and, in lane L, its
+// receivers a * kN3Block + 128 (w % 2) + L + 32 q, q < 4 (two packed pairs).
+// Half the receivers per lane keeps a thread under 128 registers, so twice
+// the warps share an SM and hide the latency of the rotation's dependent
+// shuffles, at 11 shuffles per 4 unordered pairs instead of per 8.  The
+// reaction staging sums the two warps' halves in warp order; the results
+// equal k_force_n3_f32c's to FP32 rounding of the per-warp reaction sums.
+template <bool EXCL>
+__global__ void __launch_bounds__(kN3F64Warps * 32, 1)
+    k_force_n3_f32c_w2(const IParticles ip, const JStream js, const N3Params p3, const float eps2f,
+                       int* err) {
+  constexpr int NI = 4, IPAIR = 2, WARPS = kN3F64Warps;
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
+  unsigned char* stages = smem + kSmemHead;
+  float* red = reinterpret_cast<float*>(stages + kStages * kStage32);  // [warp][3][256]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int rb = warp >> 1, hf = warp & 1;  // row block in the group, its receiver half
+  int g = 0, k = blockIdx.x;
+  const int groups = (int)((p3.nb + kN3Warps - 1) / kN3Warps);
+  while (g < groups) {  // the grid has exactly sum_g n3_chunks(nb, cols, g) CTAs
+    const int K = n3_chunks(p3.nb, p3.cols, g);
+    if (k < K) break;
+    k -= K;
+    ++g;
+  }
+  if (g >= groups) return;
+  const long long r0 = (long long)g * kN3Warps;
+  const long long a = r0 + rb;
+  const long long cs = r0 + (long long)k * p3.cols;
+  const long long ce = min(cs + (long long)p3.cols, p3.nb);
+  const int ntl = (int)(2 * (ce - cs));
+  const bool row_ok = a < p3.nb;
+  const long long ibase = a * kN3Block + hf * (kN3Block / 2) + lane;
+
+  double xi[NI], yi[NI], zi[NI];
+  u64 AI[IPAIR], BI[IPAIR];
+#pragma unroll
+  for (int q = 0; q < NI; ++q) xi[q] = yi[q] = zi[q] = 0.0;
+#pragma unroll
+  for (int p = 0; p < IPAIR; ++p) {
+    float m0 = 0.f, m1 = 0.f;
+    if (row_ok) {
+      const long long i0 = ibase + 64 * p, i1 = i0 + 32;
+      if (NBR_IN(i1, ip.len, err)) {
+        xi[2 * p] = ip.x[i0]; yi[2 * p] = ip.y[i0]; zi[2 * p] = ip.z[i0];
+        xi[2 * p + 1] = ip.x[i1]; yi[2 * p + 1] = ip.y[i1]; zi[2 * p + 1] = ip.z[i1];
+        m0 = (float)ip.m[i0];
+        m1 = (float)ip.m[i1];
+      }
+    }
+    AI[p] = pack2(-1.5f * m0, -1.5f * m1);
+    BI[p] = pack2(2.5f * m0, 2.5f * m1);
+  }
+  u64 hx[IPAIR], hy[IPAIR], hz[IPAIR], lx[IPAIR], ly[IPAIR], lz[IPAIR];
+#pragma unroll
+  for (int p = 0; p < IPAIR; ++p) hx[p] = hy[p] = hz[p] = lx[p] = ly[p] = lz[p] = 0ull;
+  const u64 EPS2 = pack2(eps2f, eps2f);
+
+  auto issue = [&](int st, int t) {
+    unsigned char* dst = stages + st * kStage32;
+    const uint32_t bar = smem_u32(&bars[st]);
+    const long long tile = 2 * cs + t;
+    if (!NBR_IN((tile + 1) * kTile - 1, js.len, err)) return;  // the wait expires
+    mbar_expect_tx(bar, kStage32);
+    bulk_g2s(dst, js.rec + (size_t)tile * kTile * 3, kRecBytes, bar);
+    bulk_g2s(dst + kRecBytes, js.origin + tile, 32, bar);
+  };
+  int tcur = 0;
+  auto body = [&](int st) {
+    const int t = tcur++;
+    const long long c = cs + t / 2;
+    const int half = t & 1;
+    const unsigned char* base = stages + st * kStage32;
+    const double4 o = *reinterpret_cast<const double4*>(base + kRecBytes);
+    u64 XI[IPAIR], YI[IPAIR], ZI[IPAIR], AX[IPAIR], AY[IPAIR], AZ[IPAIR];
+#pragma unroll
+    for (int p = 0; p < IPAIR; ++p) {
+      XI[p] = pack2(__double2float_rn(xi[2 * p] - o.x), __double2float_rn(xi[2 * p + 1] - o.x));
+      YI[p] = pack2(__double2float_rn(yi[2 * p] - o.y), __double2float_rn(yi[2 * p + 1] - o.y));
+      ZI[p] = pack2(__double2float_rn(zi[2 * p] - o.z), __double2float_rn(zi[2 * p + 1] - o.z));
+      AX[p] = AY[p] = AZ[p] = 0ull;
+    }
+    float* myred = red + warp * 3 * kN3Block + half * kTile;
+    if (row_ok && c == a) {
+      const ulonglong2* R = reinterpret_cast<const ulonglong2*>(base);
+#pragma unroll 4
+      for (int j = 0; j < kTile; ++j) {
+        const ulonglong2 q0 = R[3 * j];
+        const ulonglong2 q1 = R[3 * j + 1];
+        const u64 bj = R[3 * j + 2].x;
+#pragma unroll
+        for (int p = 0; p < IPAIR; ++p) {
+          const u64 dx = sub2(q0.x, XI[p]);
+          const u64 dy = sub2(q0.y, YI[p]);
+          const u64 dz = sub2(q1.x, ZI[p]);
+          u64 r2 = fma2(dx, dx, EPS2);
+          r2 = fma2(dy, dy, r2);
+          r2 = fma2(dz, dz, r2);
+          u64 y;
+          if (EXCL) {
+            float rl, rh;
+            unpack2(r2, rl, rh);
+            y = pack2(rl > 0.f ? rsqrt_mufu(rl) : 0.f, rh > 0.f ? rsqrt_mufu(rh) : 0.f);
+          } else {
+            y = rsqrt2(r2);
+          }
+          const u64 y2 = mul2(y, y);
+          const u64 pr = mul2(r2, y2);
+          const u64 mg = fma2(q1.y, pr, bj);
+          const u64 y3 = mul2(y2, y);
+          const u64 s = mul2(y3, mg);
+          AX[p] = fma2(s, dx, AX[p]);
+          AY[p] = fma2(s, dy, AY[p]);
+          AZ[p] = fma2(s, dz, AZ[p]);
+        }
+      }
+#pragma unroll
+      for (int bt = 0; bt < 4; ++bt)
+        myred[bt * 32 + lane] = myred[kN3Block + bt * 32 + lane] = myred[2 * kN3Block + bt * 32 + lane] = 0.f;
+    } else if (row_ok && c > a) {
+      const float4* R4 = reinterpret_cast<const float4*>(base);
+      const int from = (lane + 31) & 31;
+#pragma unroll 1
+      for (int bt = 0; bt < 4; ++bt) {
+        const int j = bt * 32 + lane;
+        const float4 q0 = R4[3 * j], q1 = R4[3 * j + 1], q2 = R4[3 * j + 2];
+        float sx = q0.x, sy = q0.z, sz = q1.x, sa = q1.z, sb = q2.x;
+        u64 RX = 0ull, RY = 0ull, RZ = 0ull;
+#pragma unroll 2
+        for (int step = 0; step < 32; ++step) {
+          const u64 SX = pack2(sx, sx), SY = pack2(sy, sy), SZ = pack2(sz, sz);
+          const u64 SA = pack2(sa, sa), SB = pack2(sb, sb);
+#pragma unroll
+          for (int p = 0; p < IPAIR; ++p) {
+            const u64 dx = sub2(SX, XI[p]);
+            const u64 dy = sub2(SY, YI[p]);
+            const u64 dz = sub2(SZ, ZI[p]);
+            u64 r2 = fma2(dx, dx, EPS2);
+            r2 = fma2(dy, dy, r2);
+            r2 = fma2(dz, dz, r2);
+            u64 y;
+            if (EXCL) {
+              float rl, rh;
+              unpack2(r2, rl, rh);
+              y = pack2(rl > 0.f ? rsqrt_mufu(rl) : 0.f, rh > 0.f ? rsqrt_mufu(rh) : 0.f);
+            } else {
+              y = rsqrt2(r2);
+            }
+            const u64 y2 = mul2(y, y);
+            const u64 pr = mul2(r2, y2);
+            const u64 y3 = mul2(y2, y);
+            const u64 sj = mul2(y3, fma2(SA, pr, SB));  // m_j (1 + 3e/2) y^3
+            const u64 si = mul2(y3, fma2(AI[p], pr, BI[p]));  // m_i (1 + 3e/2) y^3
+            AX[p] = fma2(sj, dx, AX[p]);
+            AY[p] = fma2(sj, dy, AY[p]);
+            AZ[p] = fma2(sj, dz, AZ[p]);
+            RX = fma2(si, dx, RX);
+            RY = fma2(si, dy, RY);
+            RZ = fma2(si, dz, RZ);
+          }
+          sx = __shfl_sync(0xffffffffu, sx, from);
+          sy = __shfl_sync(0xffffffffu, sy, from);
+          sz = __shfl_sync(0xffffffffu, sz, from);
+          sa = __shfl_sync(0xffffffffu, sa, from);
+          sb = __shfl_sync(0xffffffffu, sb, from);
+          RX = __shfl_sync(0xffffffffu, RX, from);
+          RY = __shfl_sync(0xffffffffu, RY, from);
+          RZ = __shfl_sync(0xffffffffu, RZ, from);
+        }
+        // back at its own lane: the force on source j is -sum s_i d
+        float u0, u1;
+        unpack2(RX, u0, u1); myred[bt * 32 + lane] = -(u0 + u1);
+        unpack2(RY, u0, u1); myred[kN3Block + bt * 32 + lane] = -(u0 + u1);
+        unpack2(RZ, u0, u1); myred[2 * kN3Block + bt * 32 + lane] = -(u0 + u1);
+      }
+    } else {
+#pragma unroll
+      for (int bt = 0; bt < 4; ++bt)
+        myred[bt * 32 + lane] = myred[kN3Block + bt * 32 + lane] = myred[2 * kN3Block + bt * 32 + lane] = 0.f;
+    }
+#pragma unroll
+    for (int p = 0; p < IPAIR; ++p) {
+      two_sum2(hx[p], lx[p], AX[p]);
+      two_sum2(hy[p], ly[p], AY[p]);
+      two_sum2(hz[p], lz[p], AZ[p]);
+    }
+    if (half == 1) {
+      // end of column block c: its reaction from this CTA's rows, summed in
+      // warp order in FP64, to the block's partial slot
+      __syncthreads();
+      const int tid = threadIdx.x;  // one source of the block per thread
+      if (tid < kN3Block) {
+        const long long off = ((long long)blockIdx.x * p3.cols + (c - cs)) * 3 * kN3Block;
+        double* out = p3.rea + off;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          double s = 0.0;
+          for (int w = 0; w < WARPS; ++w) s += (double)red[(w * 3 + d) * kN3Block + tid];
+          if (NBR_IN((p3.rea - p3.act) + off + d * kN3Block + tid, p3.act_len, err))
+            out[d * kN3Block + tid] = s;
+        }
+      }
+      __syncthreads();
+    }
+  };
+  if (!tile_pipeline(bars, ntl, js, err, issue, body)) return;
+  double* act = p3.act + ((size_t)blockIdx.x * kN3Warps + rb) * 3 * kN3Block + hf * (kN3Block / 2);
+  if (!NBR_IN(((long long)blockIdx.x * kN3Warps + rb + 1) * 3 * kN3Block - 1, p3.act_len, err))
+    return;
+#pragma unroll
+  for (int p = 0; p < IPAIR; ++p) {
+    float h0, h1, l0, l1;
+    unpack2(hx[p], h0, h1); unpack2(lx[p], l0, l1);
+    act[lane + 64 * p] = (double)h0 + (double)l0;
+    act[lane + 64 * p + 32] = (double)h1 + (double)l1;
+    unpack2(hy[p], h0, h1); unpack2(ly[p], l0, l1);
+    act[kN3Block + lane + 64 * p] = (double)h0 + (double)l0;
+    act[kN3Block + lane + 64 * p + 32] = (double)h1 + (double)l1;
+    unpack2(hz[p], h0, h1); unpack2(lz[p], l0, l1);
+    act[2 * kN3Block + lane + 64 * p] = (double)h0 + (double)l0;
+    act[2 * kN3Block + lane + 64 * p + 32] = (double)h1 + (double)l1;
+  }
+}
+
 // FP64 form of the Newton-3 kernel (ForceConfig ni = 3 with NBR_FP64): the
 // blocks, CTA map, source rotation and partial-sum layout of k_force_n3_f32c,
 // with every operation in FP64 and the reciprocal square root from CUDA's
@@ -1318,29 +1569,71 @@ __global__ void __launch_bounds__(256) k_validate(long long n, const double* __r
 }
 
 // -------------------------------------------------------------- dispatch ----
-template <int NI, int W, bool EX>
-cudaError_t launch_f32c_t(float eps2f, int split, const IParticles& ip, const JStream& js,
-                          const Epilogue& ep, cudaStream_t st) {
-  const size_t smem = kSmemHead + (size_t)kStages * kStage32;
-  const long long chunk = 32LL * NI * W;
-  const unsigned gx = (unsigned)((ip.n + chunk - 1) / chunk);
-  dim3 grid(gx, (unsigned)split);
-  k_force_f32c<NI, W, EX><<<grid, W * 32, smem, st>>>(ip, js, ep, eps2f);
-  return cudaGetLastError();
-}
-template <int NI, int W, bool EX>
-cudaError_t launch_f64_t(double eps2, int split, const IParticles& ip, const JStream& js,
-                         const Epilogue& ep, cudaStream_t st) {
-  const size_t smem = kSmemHead + (size_t)kStages * kStage64;
-  const long long chunk = 32LL * NI * W;
-  const unsigned gx = (unsigned)((ip.n + chunk - 1) / chunk);
-  dim3 grid(gx, (unsigned)split);
-  k_force_f64<NI, W, EX><<<grid, W * 32, smem, st>>>(ip, js, ep, eps2);
-  return cudaGetLastError();
-}
-
 #define NBR_CFG_LIST(X) X(4, 2) X(4, 4) X(4, 8) X(8, 2) X(8, 4)
 #define NBR_SMALL_LIST(X) X(2) X(4) X(8)
+// (j-tile, unroll) variants built for the default large configurations
+#define NBR_TU_LIST(X) X(64, 2) X(64, 4) X(64, 8) X(128, 2) X(128, 4) X(128, 8) \
+                       X(256, 2) X(256, 4) X(256, 8)
+
+int norm_tile(const ForceConfig& c) { return c.tile > 0 ? c.tile : kDefaultTileJ; }
+int norm_unroll(int precision, const ForceConfig& c) {
+  return c.unroll > 0 ? c.unroll : default_unroll(precision);
+}
+
+// The large kernel of a configuration, or nullptr if that variant is not built.
+const void* large_fn(int precision, int ni, int w, int tj, int u, bool ex) {
+  if (precision == kFP32C) {
+#define NBR_F32(a, b)                                                                        \
+  if (ni == a && w == b && tj == kDefaultTileJ && u == 4)                                    \
+    return ex ? (const void*)k_force_f32c<a, b, true, kDefaultTileJ, 4>                      \
+              : (const void*)k_force_f32c<a, b, false, kDefaultTileJ, 4>;
+    NBR_CFG_LIST(NBR_F32)
+#undef NBR_F32
+#define NBR_F32TU(t, v)                                                                      \
+  if (ni == 8 && w == 2 && tj == t && u == v)                                                \
+    return ex ? (const void*)k_force_f32c<8, 2, true, t, v> : (const void*)k_force_f32c<8, 2, false, t, v>;
+    NBR_TU_LIST(NBR_F32TU)
+#undef NBR_F32TU
+  } else {
+#define NBR_F64(a, b)                                                                        \
+  if (ni == a && w == b && tj == kDefaultTileJ && u == 2)                                    \
+    return ex ? (const void*)k_force_f64<a, b, true, kDefaultTileJ, 2>                       \
+              : (const void*)k_force_f64<a, b, false, kDefaultTileJ, 2>;
+    NBR_CFG_LIST(NBR_F64)
+#undef NBR_F64
+#define NBR_F64TU(t, v)                                                                      \
+  if (ni == 4 && w == 4 && tj == t && u == v)                                                \
+    return ex ? (const void*)k_force_f64<4, 4, true, t, v> : (const void*)k_force_f64<4, 4, false, t, v>;
+    NBR_TU_LIST(NBR_F64TU)
+#undef NBR_F64TU
+  }
+  return nullptr;
+}
+
+size_t large_smem(int precision, int tj) {
+  size_t stage = 0;
+  if (precision == kFP32C)
+    stage = tj == 64 ? stage32_bytes<64>() : tj == 256 ? stage32_bytes<256>() : stage32_bytes<128>();
+  else
+    stage = 32 * (size_t)tj;
+  return kSmemHead + (size_t)kStages * stage;
+}
+
+cudaError_t launch_large(int precision, double eps2, const ForceConfig& c, const IParticles& ip,
+                         const JStream& js, const Epilogue& ep, cudaStream_t st) {
+  const int tj = norm_tile(c), u = norm_unroll(precision, c);
+  const void* fn = large_fn(precision, c.ni, c.warps, tj, u, eps2 == 0.0);
+  if (!fn) return cudaErrorInvalidValue;
+  const long long chunk = 32LL * c.ni * c.warps;
+  const dim3 grid((unsigned)((ip.n + chunk - 1) / chunk), (unsigned)c.split);
+  IParticles a0 = ip;
+  JStream a1 = js;
+  Epilogue a2 = ep;
+  float e32 = (float)eps2;
+  double e64 = eps2;
+  void* args[] = {&a0, &a1, &a2, precision == kFP32C ? (void*)&e32 : (void*)&e64};
+  return cudaLaunchKernel(fn, grid, dim3(c.warps * 32), args, large_smem(precision, tj), st);
+}
 
 template <int PREC, int F>
 const void* small_fn(bool ex) {
@@ -1362,26 +1655,28 @@ cudaError_t launch_small_t(double eps2, int split, const IParticles& ip, const J
 
 }  // namespace
 
-size_t n3_smem_bytes(int precision);
+size_t n3_smem_bytes(int precision, int warps);
 
 bool force_config_supported(int precision, const ForceConfig& c) {
-  if (c.ni == 3) return c.warps == kN3Warps;  // Newton-3 (FP32C and FP64)
+  if (c.ni == kPersistNI) return precision == kFP64 && (c.warps == 4 || c.warps == 8 || c.warps == 16);
+  if (c.ni == 3)  // Newton-3: FP32C one or two warps per row block; FP64 (two)
+    return c.warps == kN3Warps || (precision == kFP32C && c.warps == kN3F64Warps);
   if (c.ni == 1) return (c.warps == 2 || c.warps == 4 || c.warps == 8) && c.split >= 1;
-#define NBR_MATCH(a, b) if (c.ni == a && c.warps == b) return c.split >= 1;
-  NBR_CFG_LIST(NBR_MATCH)
-#undef NBR_MATCH
-  return false;
+  if (c.split < 1) return false;
+  return large_fn(precision, c.ni, c.warps, norm_tile(c), norm_unroll(precision, c), false) != nullptr;
 }
 
 int force_blocks_per_sm(int precision, double eps2, const ForceConfig& c) {
   int nb = 0;
   if (c.ni == 3) {
     const bool ex = eps2 == 0.0;
+    const bool w2 = precision == kFP32C && c.warps == kN3F64Warps;
     const void* fn = precision == kFP32C
-                         ? (ex ? (const void*)k_force_n3_f32c<true> : (const void*)k_force_n3_f32c<false>)
+                         ? (w2 ? (ex ? (const void*)k_force_n3_f32c_w2<true> : (const void*)k_force_n3_f32c_w2<false>)
+                               : (ex ? (const void*)k_force_n3_f32c<true> : (const void*)k_force_n3_f32c<false>))
                          : (ex ? (const void*)k_force_n3_f64<true> : (const void*)k_force_n3_f64<false>);
-    const int threads = (precision == kFP32C ? kN3Warps : kN3F64Warps) * 32;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, threads, n3_smem_bytes(precision)) !=
+    const int threads = (precision == kFP32C && !w2 ? kN3Warps : kN3F64Warps) * 32;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, threads, n3_smem_bytes(precision, c.warps)) !=
         cudaSuccess)
       nb = 0;
     return nb;
@@ -1399,24 +1694,15 @@ int force_blocks_per_sm(int precision, double eps2, const ForceConfig& c) {
       nb = 0;
     return nb;
   }
-#define NBR_OCC(a, b)                                                                          \
-  if (c.ni == a && c.warps == b) {                                                             \
-    const void* fn = precision == kFP32C                                                       \
-                         ? (ex ? (const void*)k_force_f32c<a, b, true>                         \
-                               : (const void*)k_force_f32c<a, b, false>)                       \
-                         : (ex ? (const void*)k_force_f64<a, b, true>                          \
-                               : (const void*)k_force_f64<a, b, false>);                       \
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, b * 32, smem) != cudaSuccess)   \
-      nb = 0;                                                                                  \
-    return nb;                                                                                 \
-  }
-  NBR_CFG_LIST(NBR_OCC)
-#undef NBR_OCC
-  return 0;
+  const void* fn = large_fn(precision, c.ni, c.warps, norm_tile(c), norm_unroll(precision, c), ex);
+  if (!fn || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, c.warps * 32, smem) != cudaSuccess)
+    nb = 0;
+  return nb;
 }
 
-size_t force_smem_bytes(int precision, const ForceConfig&) {
-  return kSmemHead + (size_t)kStages * (precision == kFP32C ? kStage32 : kStage64);
+size_t force_smem_bytes(int precision, const ForceConfig& c) {
+  if (c.ni == 1) return kSmemHead + (size_t)kStages * (precision == kFP32C ? kStage32 : kStage64);
+  return large_smem(precision, norm_tile(c));
 }
 
 cudaError_t launch_force(int precision, double eps2, const ForceConfig& c, const IParticles& ip,
@@ -1432,48 +1718,44 @@ cudaError_t launch_force(int precision, double eps2, const ForceConfig& c, const
 #undef NBR_SGO
     return cudaErrorInvalidValue;
   }
-  if (precision == kFP32C) {
-    const float e = (float)eps2;
-#define NBR_GO(a, b)                                                                       \
-  if (c.ni == a && c.warps == b)                                                           \
-    return ex ? launch_f32c_t<a, b, true>(e, c.split, ip, js, ep, st)                      \
-              : launch_f32c_t<a, b, false>(e, c.split, ip, js, ep, st);
-    NBR_CFG_LIST(NBR_GO)
-#undef NBR_GO
-  } else {
-#define NBR_GO(a, b)                                                                       \
-  if (c.ni == a && c.warps == b)                                                           \
-    return ex ? launch_f64_t<a, b, true>(eps2, c.split, ip, js, ep, st)                    \
-              : launch_f64_t<a, b, false>(eps2, c.split, ip, js, ep, st);
-    NBR_CFG_LIST(NBR_GO)
-#undef NBR_GO
-  }
-  return cudaErrorInvalidValue;
+  return launch_large(precision, eps2, c, ip, js, ep, st);
 }
 
 // Tile ring plus the per-warp reaction staging (floats for FP32C, doubles for
-// FP64).
-size_t n3_smem_bytes(int precision) {
+// FP64); `warps` per CTA.
+size_t n3_smem_bytes(int precision, int warps) {
   return precision == kFP32C
-             ? kSmemHead + (size_t)kStages * kStage32 + (size_t)kN3Warps * 3 * kN3Block * sizeof(float)
+             ? kSmemHead + (size_t)kStages * kStage32 + (size_t)warps * 3 * kN3Block * sizeof(float)
              : kSmemHead + (size_t)kStages * kStage64 + (size_t)kN3F64Warps * 3 * kN3Block * sizeof(double);
 }
 
 cudaError_t configure_kernels() {
   // The Newton-3 kernels need more than the default 48 KB of dynamic shared
   // memory; set once per device, outside any stream capture.
-  const int s32 = (int)n3_smem_bytes(kFP32C), s64 = (int)n3_smem_bytes(kFP64);
+  const int s32 = (int)n3_smem_bytes(kFP32C, kN3Warps), s64 = (int)n3_smem_bytes(kFP64, kN3F64Warps);
+  const int s32w = (int)n3_smem_bytes(kFP32C, kN3F64Warps);
   const cudaFuncAttribute at = cudaFuncAttributeMaxDynamicSharedMemorySize;
   cudaError_t e = cudaFuncSetAttribute((const void*)k_force_n3_f32c<true>, at, s32);
   if (e == cudaSuccess) e = cudaFuncSetAttribute((const void*)k_force_n3_f32c<false>, at, s32);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute((const void*)k_force_n3_f32c_w2<true>, at, s32w);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute((const void*)k_force_n3_f32c_w2<false>, at, s32w);
   if (e == cudaSuccess) e = cudaFuncSetAttribute((const void*)k_force_n3_f64<true>, at, s64);
   if (e == cudaSuccess) e = cudaFuncSetAttribute((const void*)k_force_n3_f64<false>, at, s64);
+  // large kernels: the 256-source FP32C stages need more than the default 48 KB
+  for (int prec = 0; prec < 2 && e == cudaSuccess; ++prec)
+    for (int ni : {4, 8})
+      for (int w : {2, 4, 8})
+        for (int tj : {64, 128, 256})
+          for (int u : {2, 4, 8})
+            for (int ex = 0; ex < 2 && e == cudaSuccess; ++ex)
+              if (const void* fn = large_fn(prec, ni, w, tj, u, ex != 0))
+                e = cudaFuncSetAttribute(fn, at, (int)large_smem(prec, tj));
   return e;
 }
 
-cudaError_t launch_force_n3(int precision, double eps2, const IParticles& ip, const JStream& js,
-                            const Epilogue& ep, double* scratch, long long scratch_len,
-                            cudaStream_t st) {
+cudaError_t launch_force_n3(int precision, int warps, double eps2, const IParticles& ip,
+                            const JStream& js, const Epilogue& ep, double* scratch,
+                            long long scratch_len, cudaStream_t st) {
   (void)scratch_len;
   if (ip.n <= 0 || js.ntiles <= 0) return cudaSuccess;
   N3Params p3;
@@ -1484,9 +1766,16 @@ cudaError_t launch_force_n3(int precision, double eps2, const IParticles& ip, co
   p3.act = scratch;
   p3.rea = scratch + (size_t)ctas * kN3Warps * 3 * kN3Block;
   NBR_CHECKED_ONLY(p3.act_len = scratch_len;)
-  const size_t smem = n3_smem_bytes(precision);
-  const unsigned grid = (unsigned)ctas, block = (precision == kFP32C ? kN3Warps : kN3F64Warps) * 32;
-  if (precision == kFP32C) {
+  const bool w2 = precision == kFP32C && warps == kN3F64Warps;
+  const size_t smem = n3_smem_bytes(precision, precision == kFP32C ? warps : kN3F64Warps);
+  const unsigned grid = (unsigned)ctas,
+                 block = (precision == kFP32C && !w2 ? kN3Warps : kN3F64Warps) * 32;
+  if (w2) {
+    if (eps2 == 0.0)
+      k_force_n3_f32c_w2<true><<<grid, block, smem, st>>>(ip, js, p3, 0.f, ep.err);
+    else
+      k_force_n3_f32c_w2<false><<<grid, block, smem, st>>>(ip, js, p3, (float)eps2, ep.err);
+  } else if (precision == kFP32C) {
     if (eps2 == 0.0)
       k_force_n3_f32c<true><<<grid, block, smem, st>>>(ip, js, p3, 0.f, ep.err);
     else

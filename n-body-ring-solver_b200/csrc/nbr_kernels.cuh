@@ -72,7 +72,17 @@ struct ForceConfig {
   int ni;      // receivers per thread (4 or 8); 1 selects the small-N kernel
   int warps;   // warps per CTA (2, 4 or 8); for the small-N kernel: lane groups F (2, 4, 8)
   int split;   // j-range splits (>= 1)
+  // Large kernels only (ni 4 / 8): sources per stage of the tile ring (the
+  // j-tile: 64, 128 or 256) and the unroll depth of the source loop (2, 4 or
+  // 8); 0 takes the default (128; unroll 4 for FP32C, 2 for FP64).  Other
+  // values than the defaults exist for the default large configurations,
+  // FP32C (8, 2) and FP64 (4, 4).
+  int tile = 0;
+  int unroll = 0;
 };
+// Default j-tile and unroll depth of the large kernels.
+constexpr int kDefaultTileJ = 128;
+inline int default_unroll(int precision) { return precision == kFP32C ? 4 : 2; }
 
 // The small-N kernel: kSmallWarps warps per CTA, kSmallNI receivers per lane,
 // F lane groups per warp sharing each tile's sources: 128 * kSmallNI / F
@@ -123,11 +133,19 @@ inline long long n3_scratch_doubles(long long nb) {
 // same particles in js (FP32C: their records; FP64: their x, y, z, m arrays),
 // with the epilogue ep: the pair kernel, then the per-particle reduction.
 // scratch holds n3_scratch_doubles(ceil(n / kN3Block)) doubles.
-cudaError_t launch_force_n3(int precision, double eps2, const IParticles& ip, const JStream& js,
-                            const Epilogue& ep, double* scratch, long long scratch_len,
-                            cudaStream_t stream);
+// FP32C: warps = kN3Warps (one warp per row block) or kN3F64Warps (two).
+cudaError_t launch_force_n3(int precision, int warps, double eps2, const IParticles& ip,
+                            const JStream& js, const Epilogue& ep, double* scratch,
+                            long long scratch_len, cudaStream_t stream);
 // Kernel attributes that must be set once per device, outside stream capture.
 cudaError_t configure_kernels();
+
+// The persistent small-system run (nbr_persist.cu): the whole nbr_run step
+// loop of an FP64 system of at most kPersistMaxN particles in one cooperative
+// launch.  ForceConfig ni = kPersistNI with warps = lane groups (4, 8, 16)
+// forces it; it is the default for such systems.
+constexpr int kPersistNI = 2;
+constexpr long long kPersistMaxN = 4096;
 
 // Receivers one CTA of a configuration covers.
 inline long long force_chunk(const ForceConfig& c) {

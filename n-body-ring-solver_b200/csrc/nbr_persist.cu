@@ -1,0 +1,369 @@
+// nbr_persist.cu -- the whole leapfrog loop of a small system in one launch.
+//
+// For a few thousand particles one force evaluation is a few microseconds of
+// work, comparable to the gap between two kernel launches even inside a CUDA
+// graph.  This file runs every step of nbr_run (KDK, Yoshida DKD or Euler,
+// the schedules of reduced_solver_omp_lf / reduced_solver_omp,
+// CPU/omp_solver.cpp:16-178, 257-456) inside ONE cooperative launch:
+//
+//  * each CTA owns fixed receiver chunks of RPC particles for the whole run;
+//  * per force evaluation every CTA stages all N positions (masses once) in
+//    shared memory with L2 loads, its 8 warps split the sources 8 ways and the
+//    F lane groups of each warp split them again (k_force_small's layout), and
+//    the partial sums are combined in a fixed order (xor shuffles, then the
+//    warps in order): deterministic;
+//  * the CTA applies the fused kick/drift to its receivers, writing the next
+//    position buffer, and all CTAs meet at one grid barrier before the next
+//    evaluation reads it.
+//
+// The barrier is a counter plus a generation word; its wait is bounded by
+// %globaltimer (the context's wait limit) and gives up, with an error code
+// for the host, if the limit passes or another CTA has already recorded an
+// error.  The cooperative launch guarantees that all CTAs are resident, so no
+// CTA waits on one that cannot run.  Pair arithmetic is k_force_f64's (CUDA's
+// rsqrt(double)): results equal the other FP64 kernels' up to summation order.
+#include "nbr.h"
+#include "nbr_ctx.h"
+#include "nbr_device.cuh"
+#include "nbr_kernels.cuh"
+
+#include <algorithm>
+#include <vector>
+
+namespace nbr {
+
+namespace {
+
+constexpr int kPWarps = 8;
+constexpr int kPThreads = kPWarps * 32;
+constexpr int kPNI = 4;  // receivers per lane
+
+struct PersistArgs {
+  int n;                   // particles (<= kPersistMaxN)
+  int chunks;              // receiver chunks of RPC particles
+  int evals;               // force evaluations
+  const double2* sched;    // (kick, drift) of every evaluation
+  int mode;                // 1: leapfrog (drift with the kicked velocity); 2: Euler
+  int pre;                 // a standalone kick/drift before the first evaluation
+  int pre_use_acc;         // its kick uses the accelerations left by the last run
+  double pre_kick, pre_drift;
+  double G, eps2;
+  double* px[2];
+  double* py[2];
+  double* pz[2];
+  int cur0;                // buffer the first phase reads
+  double* vx; double* vy; double* vz;
+  double* ax; double* ay; double* az;
+  const double* m;
+  unsigned* bar;           // [0] arrivals, [1] generation
+  int* err;
+  unsigned long long wait_ns;
+  int skip_barrier;        // test hook: CTA 0 leaves before this barrier (-1: off)
+};
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Grid-wide barrier with a bounded wait.  Returns false in every thread of the
+// CTA if the barrier did not complete within the limit or an error was
+// already recorded (the CTA then leaves the kernel).
+__device__ bool grid_barrier(unsigned* bar, int* err, unsigned long long limit_ns) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    const unsigned gen = ld_acquire_u32(bar + 1);
+    __threadfence();
+    const unsigned arrived = atomicAdd(bar, 1u);
+    if (arrived == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      st_release_u32(bar + 1, gen + 1);
+    } else {
+      const unsigned long long t0 = global_ns();
+      while (ld_acquire_u32(bar + 1) == gen) {
+        if (*reinterpret_cast<volatile int*>(err) != 0 || global_ns() - t0 > limit_ns) {
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    if (!ok) record_error(err, kErrGridWait);
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+template <int F, bool EXCL>
+__global__ void __launch_bounds__(kPThreads, 1) k_run_small_f64(const PersistArgs A) {
+  constexpr int G = 32 / F;        // receiver columns per warp
+  constexpr int RPC = G * kPNI;    // receivers per chunk
+  constexpr int S = kPWarps * F;   // ways the sources are split
+  extern __shared__ __align__(16) double smem_d[];
+  const int n = A.n;
+  const int ns = (n + 1) & ~1;
+  double* sx = smem_d;
+  double* sy = sx + ns;
+  double* sz = sy + ns;
+  double* sm = sz + ns;
+  double* red = sm + ns;  // [kPWarps][RPC][3]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gl = lane % G, grp = lane / G;
+
+  for (int j = threadIdx.x; j < n; j += kPThreads) sm[j] = A.m[j];
+  int cur = A.cur0;
+
+  if (A.pre) {
+    for (int c = blockIdx.x; c < A.chunks; c += gridDim.x) {
+      for (int t = threadIdx.x; t < RPC; t += kPThreads) {
+        const int i = c * RPC + t;
+        if (i >= n) continue;
+        double ux = A.vx[i], uy = A.vy[i], uz = A.vz[i];
+        if (A.pre_use_acc) {
+          ux += A.pre_kick * A.ax[i]; uy += A.pre_kick * A.ay[i]; uz += A.pre_kick * A.az[i];
+          A.vx[i] = ux; A.vy[i] = uy; A.vz[i] = uz;
+        }
+        A.px[1 - cur][i] = __ldcg(A.px[cur] + i) + A.pre_drift * ux;
+        A.py[1 - cur][i] = __ldcg(A.py[cur] + i) + A.pre_drift * uy;
+        A.pz[1 - cur][i] = __ldcg(A.pz[cur] + i) + A.pre_drift * uz;
+      }
+    }
+    if (!grid_barrier(A.bar, A.err, A.wait_ns)) return;
+    cur ^= 1;
+  }
+
+  for (int e = 0; e < A.evals; ++e) {
+    // all positions of this evaluation, from L2 (other CTAs wrote them)
+    const double* X = A.px[cur];
+    const double* Y = A.py[cur];
+    const double* Z = A.pz[cur];
+    for (int j = threadIdx.x; j < n; j += kPThreads) {
+      sx[j] = __ldcg(X + j);
+      sy[j] = __ldcg(Y + j);
+      sz[j] = __ldcg(Z + j);
+    }
+    __syncthreads();
+    const double2 kd = A.sched[e];
+    for (int c = blockIdx.x; c < A.chunks; c += gridDim.x) {
+      const int base = c * RPC;
+      double xi[kPNI], yi[kPNI], zi[kPNI], ax[kPNI], ay[kPNI], az[kPNI];
+#pragma unroll
+      for (int k = 0; k < kPNI; ++k) {
+        const int i = base + gl + G * k;
+        const bool real = i < n;
+        xi[k] = real ? sx[i] : 0.0;
+        yi[k] = real ? sy[i] : 0.0;
+        zi[k] = real ? sz[i] : 0.0;
+        ax[k] = ay[k] = az[k] = 0.0;
+      }
+#pragma unroll 2
+      for (int j = warp * F + grp; j < n; j += S) {
+        const double xj = sx[j], yj = sy[j], zj = sz[j], mj = sm[j];
+#pragma unroll
+        for (int k = 0; k < kPNI; ++k) {
+          const double dx = xj - xi[k], dy = yj - yi[k], dz = zj - zi[k];
+          double r2 = fma(dx, dx, A.eps2);
+          r2 = fma(dy, dy, r2);
+          r2 = fma(dz, dz, r2);
+          double y = rsqrt(r2);
+          if (EXCL) y = r2 > 0.0 ? y : 0.0;
+          const double s = mj * (y * y * y);
+          ax[k] = fma(s, dx, ax[k]);
+          ay[k] = fma(s, dy, ay[k]);
+          az[k] = fma(s, dz, az[k]);
+        }
+      }
+      // lane groups of the warp, then the warps in order
+#pragma unroll
+      for (int off = G; off < 32; off <<= 1) {
+#pragma unroll
+        for (int k = 0; k < kPNI; ++k) {
+          ax[k] += __shfl_xor_sync(0xffffffffu, ax[k], off);
+          ay[k] += __shfl_xor_sync(0xffffffffu, ay[k], off);
+          az[k] += __shfl_xor_sync(0xffffffffu, az[k], off);
+        }
+      }
+      if (grp == 0) {
+#pragma unroll
+        for (int k = 0; k < kPNI; ++k) {
+          double* r = red + ((size_t)warp * RPC + gl + G * k) * 3;
+          r[0] = ax[k]; r[1] = ay[k]; r[2] = az[k];
+        }
+      }
+      __syncthreads();
+      if (threadIdx.x < RPC) {
+        const int t = threadIdx.x, i = base + t;
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+#pragma unroll
+        for (int w = 0; w < kPWarps; ++w) {
+          const double* r = red + ((size_t)w * RPC + t) * 3;
+          a0 += r[0]; a1 += r[1]; a2 += r[2];
+        }
+        if (i < n) {
+          // the epilogue of the large kernels: a -> acc, v += kick a, x' = x + drift v
+          // (Euler: drift with the old velocity)
+          const double gx = A.G * a0, gy = A.G * a1, gz = A.G * a2;
+          A.ax[i] = gx; A.ay[i] = gy; A.az[i] = gz;
+          const double ux = A.vx[i], uy = A.vy[i], uz = A.vz[i];
+          const double vx = ux + kd.x * gx, vy = uy + kd.x * gy, vz = uz + kd.x * gz;
+          A.vx[i] = vx; A.vy[i] = vy; A.vz[i] = vz;
+          const bool euler = A.mode == 2;
+          A.px[1 - cur][i] = sx[i] + kd.y * (euler ? ux : vx);
+          A.py[1 - cur][i] = sy[i] + kd.y * (euler ? uy : vy);
+          A.pz[1 - cur][i] = sz[i] + kd.y * (euler ? uz : vz);
+        }
+      }
+      __syncthreads();  // red is reused by the next chunk
+    }
+    if (e + 1 < A.evals) {
+      if (e == A.skip_barrier && blockIdx.x == 0) return;  // test hook: never arrives
+      if (!grid_barrier(A.bar, A.err, A.wait_ns)) return;
+    }
+    cur ^= 1;
+  }
+}
+
+const void* persist_fn(int F, bool excl) {
+  switch (F) {
+    case 4: return excl ? (const void*)k_run_small_f64<4, true> : (const void*)k_run_small_f64<4, false>;
+    case 8: return excl ? (const void*)k_run_small_f64<8, true> : (const void*)k_run_small_f64<8, false>;
+    case 16: return excl ? (const void*)k_run_small_f64<16, true> : (const void*)k_run_small_f64<16, false>;
+    default: return nullptr;
+  }
+}
+
+size_t persist_smem(int n, int F) {
+  const int ns = (n + 1) & ~1;
+  return (size_t)4 * ns * sizeof(double) + (size_t)kPWarps * ((32 / F) * kPNI) * 3 * sizeof(double);
+}
+
+// Lane groups per warp: the layout whose receiver chunks fill the SMs best
+// (chunks / (rounds x SMs)), fewer chunks on a tie.
+int persist_groups(int n, int sms) {
+  int best = 8;
+  double best_eff = -1.0;
+  for (int F : {4, 8, 16}) {
+    const int rpc = (32 / F) * kPNI;
+    const int chunks = (n + rpc - 1) / rpc;
+    const int rounds = (chunks + sms - 1) / sms;
+    const double eff = double(chunks) / (double(rounds) * sms);
+    if (eff > best_eff + 1e-9) {
+      best_eff = eff;
+      best = F;
+    }
+  }
+  return best;
+}
+
+}  // namespace
+
+bool persistent_run_applies(nbr_ctx* c, int precision, size_t n) {
+  const ForceConfig& o = c->override_cfg[precision];
+  if (o.ni != 0 && o.ni != kPersistNI) return false;
+  return precision == kFP64 && c->coop && n >= 2 && n <= (size_t)kPersistMaxN;
+}
+
+int run_persistent(nbr_ctx* c, int precision, int scheme, double dt, size_t steps, double G,
+                   double eps2, bool fsal, const double* cc, const double* dd, int lf,
+                   nbr_run_stats* st) {
+  (void)precision;
+  SysState& s = c->sys;
+  const int n = (int)s.n;
+  // the schedule: the launch sequence of nbr_run's graph, one entry per evaluation
+  std::vector<double2> sched;
+  PersistArgs A{};
+  A.mode = scheme == NBR_EULER ? 2 : 1;
+  if (scheme == NBR_KDK) {
+    if (fsal) {
+      A.pre = 1; A.pre_use_acc = 1; A.pre_kick = 0.5 * dt; A.pre_drift = dt;
+    } else {
+      sched.push_back(make_double2(0.5 * dt, dt));
+    }
+    for (size_t k = 1; k < steps; ++k) sched.push_back(make_double2(dt, dt));
+    sched.push_back(make_double2(0.5 * dt, 0.0));
+  } else if (scheme == NBR_EULER) {
+    for (size_t k = 0; k < steps; ++k) sched.push_back(make_double2(dt, dt));
+  } else {
+    A.pre = 1; A.pre_use_acc = 0; A.pre_kick = 0.0; A.pre_drift = cc[0] * dt;
+    for (size_t k = 0; k < steps; ++k)
+      for (int sub = 0; sub < lf - 1; ++sub) {
+        const double drift = sub < lf - 2 ? cc[sub + 1]
+                                          : ((k + 1 < steps) ? cc[lf - 1] + cc[0] : cc[lf - 1]);
+        sched.push_back(make_double2(dd[sub] * dt, drift * dt));
+      }
+  }
+  const int E = (int)sched.size();
+  cudaError_t e = c->scr.need_red((size_t)2 * E + 16);
+  if (e != cudaSuccess) return cuda_fail(c, e, "persistent schedule");
+  e = cudaMemcpyAsync(c->scr.red, sched.data(), sched.size() * sizeof(double2),
+                      cudaMemcpyHostToDevice, c->stream);
+  unsigned* bar = reinterpret_cast<unsigned*>(c->d_err + 2);
+  if (e == cudaSuccess) e = cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "persistent setup");
+
+  const ForceConfig& o = c->override_cfg[kFP64];
+  const int F = (o.ni == kPersistNI) ? o.warps : persist_groups(n, c->sms);
+  const bool excl = eps2 == 0.0;
+  const void* fn = persist_fn(F, excl);
+  if (!fn) return fail(c, NBR_ERR_INVALID_ARG, "persistent run: lane groups must be 4, 8 or 16");
+  const size_t smem = persist_smem(n, F);
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int per_sm = 0;
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kPThreads, smem);
+  if (e != cudaSuccess) return cuda_fail(c, e, "persistent kernel setup");
+  if (per_sm < 1) return fail(c, NBR_ERR_UNSUPPORTED, "persistent kernel does not fit an SM");
+  const int rpc = (32 / F) * kPNI;
+  A.n = n;
+  A.chunks = (n + rpc - 1) / rpc;
+  A.evals = E;
+  A.sched = reinterpret_cast<const double2*>(c->scr.red);
+  A.G = G;
+  A.eps2 = eps2;
+  for (int b = 0; b < 2; ++b) {
+    A.px[b] = s.pos[b][0]; A.py[b] = s.pos[b][1]; A.pz[b] = s.pos[b][2];
+  }
+  A.cur0 = s.cur;
+  A.vx = s.vel[0]; A.vy = s.vel[1]; A.vz = s.vel[2];
+  A.ax = s.acc[0]; A.ay = s.acc[1]; A.az = s.acc[2];
+  A.m = s.mass;
+  A.bar = bar;
+  A.err = c->d_err;
+  JStream probe{};
+  pipeline_params(probe);
+  A.wait_ns = probe.wait_ns;
+  A.skip_barrier = probe.skip_tile;
+  const int grid = std::min(A.chunks, per_sm * c->sms);
+  void* args[] = {&A};
+  e = cudaEventRecord(c->ev0, c->stream);
+  if (e == cudaSuccess)
+    e = cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kPThreads), args, smem, c->stream);
+  if (e == cudaSuccess) e = cudaEventRecord(c->ev1, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) {
+    c->acc_ok = false;
+    return cuda_fail(c, e, "persistent run launch");
+  }
+  s.cur = (s.cur + A.pre + E) & 1;
+  s.rec_ok[0] = s.rec_ok[1] = false;
+  const int rc = check_device_error(c);
+  if (rc) return rc;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+  st->gpu_ms = ms;
+  st->kernels = 1;
+  st->force_evals = E;
+  st->pairs = double(E) * double(n) * double(n - 1);
+  return NBR_OK;
+}
+
+}  // namespace nbr

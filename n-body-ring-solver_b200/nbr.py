@@ -88,6 +88,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "nbr_yoshida_coefficients": ([C.c_int, _D, _D], C.c_int),
         "nbr_set_force_config": ([C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
         "nbr_get_force_config": ([C.c_void_p, C.c_int, C.c_double] + [C.POINTER(C.c_int)] * 3, C.c_int),
+        "nbr_set_force_tiling": ([C.c_void_p, C.c_int, C.c_int, C.c_int], C.c_int),
+        "nbr_get_force_tiling": ([C.c_void_p, C.c_int, C.c_double] + [C.POINTER(C.c_int)] * 2, C.c_int),
         "nbr_autotune": ([C.c_void_p, C.c_int, C.c_double], C.c_int),
         "nbr_tune_cache_path": ([], C.c_char_p),
         "nbr_ic_plummer": ([_SZ, _U64] + [_D] * 7, C.c_int),
@@ -422,6 +424,16 @@ class Context:
         v = [C.c_int() for _ in range(3)]
         self._chk(self.L.nbr_get_force_config(self.h, precision, eps2, *[C.byref(x) for x in v]),
                   "get_force_config")
+        return tuple(x.value for x in v)
+
+    def set_force_tiling(self, precision, tile=0, unroll=0):
+        """j-tile and unroll depth of a forced large-kernel configuration."""
+        self._chk(self.L.nbr_set_force_tiling(self.h, precision, tile, unroll), "set_force_tiling")
+
+    def get_force_tiling(self, precision, eps2=0.0):
+        v = [C.c_int(), C.c_int()]
+        self._chk(self.L.nbr_get_force_tiling(self.h, precision, eps2, *[C.byref(x) for x in v]),
+                  "get_force_tiling")
         return tuple(x.value for x in v)
 
     def autotune(self, precision, eps2):

@@ -101,6 +101,8 @@ def test_every_kernel_configuration_agrees(ctx, nbr, oracle, prec):
     # (1, F): the small-N warp-splitting kernel with F lane groups per warp;
     # (3, 8): the Newton-3 kernel
     cfgs = [(4, 2), (4, 4), (4, 8), (8, 2), (8, 4), (1, 2), (1, 4), (1, 8), (3, 8)]
+    if prec == FP32C:
+        cfgs.append((3, 16))  # Newton-3, two warps per row block
     for ni, warps in cfgs:
         for split in (1, 3, 0, 47):
             ctx.set_force_config(prec, ni, warps, split)
@@ -351,16 +353,18 @@ def test_small_kernel_leapfrog_and_ranges(ctx, nbr, oracle, prec):
         ctx.set_force_config(prec, 0)
 
 
+@pytest.mark.parametrize("warps", [8, 16])
 @pytest.mark.parametrize("n", [300, 4097, 20000, 70000])
-def test_newton3_kernel(ctx, nbr, oracle, n):
-    """The Newton-3 FP32C kernel (each unordered pair once, acting on both
-    particles): accuracy against the extended-precision oracle, bit-for-bit
-    repeatability, near-exact momentum balance, and a leapfrog run (its
-    epilogue runs in the reduction kernel, with the record pack)."""
+def test_newton3_kernel(ctx, nbr, oracle, n, warps):
+    """The Newton-3 FP32C kernels (each unordered pair once, acting on both
+    particles; one warp per 256-particle row block, or two): accuracy against
+    the extended-precision oracle, bit-for-bit repeatability, near-exact
+    momentum balance, and a leapfrog run (its epilogue runs in the reduction
+    kernel, with the record pack)."""
     s = nbr.plummer(n, 23)
     upload(ctx, s)
     eps2 = 1e-6
-    ctx.set_force_config(FP32C, 3, 8, 0)
+    ctx.set_force_config(FP32C, 3, warps, 0)
     try:
         a = ctx.forces(FP32C, eps2=eps2)
         b = ctx.forces(FP32C, eps2=eps2)
