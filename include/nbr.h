@@ -222,6 +222,27 @@ int nbr_yoshida_coefficients(int order, double* c, double* d);
  * (nbr_ctx_synchronize, a download). */
 int nbr_step_range(nbr_ctx* ctx, int precision, int scheme, size_t i0, size_t count, double kick,
                    double drift, double G, double eps2);
+/* Newton-3 across GPUs (the GPU image of hybrid_ring_solver's travelling
+ * partial forces, CPU/hybrid_solver.cpp:52-107, with a fixed reduction order).
+ * The block-pair triangle of the uploaded system is cut into nslices slices
+ * of consecutive row groups with equal pair work; each unordered pair belongs
+ * to exactly one slice.  nbr_n3_slice_accel writes the partial accelerations
+ * (not multiplied by G) that slice `slice` gives EVERY particle, in FP64,
+ * into the device array dst[d * ld + i] (d = x, y, z; ld >= the system size
+ * rounded up to 1024), asynchronous on the context's stream.  A rank computes
+ * its slices, the ranks exchange the columns of their owned ranges (an
+ * all-to-all), and nbr_step_range_sum adds, for the receivers [i0, i0 +
+ * count) (i0 a multiple of 128), the nslices partials in slice order --
+ * src[v * vstride + d * ld + k] for receiver i0 + k, ld >= count rounded up
+ * to 128 -- multiplies by G and applies the fused kick/drift of scheme
+ * (NBR_KDK / NBR_DKD: v += kick a, x' = x + drift v; NBR_EULER: drift with
+ * the old velocity) to them, like nbr_step_range.  With the same nslices the
+ * result does not depend on how the slices are spread over ranks. */
+int nbr_n3_slice_accel(nbr_ctx* ctx, int precision, double eps2, int slice, int nslices, double* dst,
+                       size_t ld);
+int nbr_step_range_sum(nbr_ctx* ctx, int precision, int scheme, size_t i0, size_t count, double kick,
+                       double drift, double G, const double* src, int nslices, size_t vstride,
+                       size_t ld);
 /* Device pointers of the current position and velocity arrays of the
  * uploaded system (any pointer may be NULL) and their allocated length
  * (*len >= n; entries >= n are zero-mass padding).  The position pointers

@@ -349,11 +349,46 @@ ForceConfig choose_config_large(nbr_ctx* c, int precision, double eps2, long lon
 }
 
 // Prepares scratch for a force launch of `cfg` over n_i receivers.
+// Slices of a banded Newton-3 evaluation of nb blocks (1: one launch).
+// Test hook: NBR_TEST_N3_SLICES=k forces k slices on any system, so that the
+// banded path (slice partials accumulated in order, then the epilogue) runs
+// on systems small enough to check against the oracle.
+int n3_bands(long long nb) {
+  if (const char* f = std::getenv("NBR_TEST_N3_SLICES")) {
+    const int k = std::atoi(f);
+    if (k >= 1) return k;
+  }
+  const long long total = n3_scratch_doubles(nb);
+  if (total <= kN3SingleMaxDoubles) return 1;
+  int V = (int)((total + kN3SliceMaxDoubles - 1) / kN3SliceMaxDoubles);
+  // slices are balanced by CTAs: grow V until the largest one fits
+  while (V < (1 << 16)) {
+    long long worst = 0;
+    for (int v = 0; v < V; ++v) worst = std::max(worst, n3_slice_scratch_doubles(nb, v, V));
+    if (worst <= kN3SliceMaxDoubles) break;
+    ++V;
+  }
+  return V;
+}
+
+// Scratch of a banded Newton-3 evaluation: the largest slice's partial sums,
+// then the FP64 accumulator [3][n_pad].
+long long n3_banded_doubles(long long nb, int V, long long n_pad, long long* acc_off) {
+  long long worst = 0;
+  for (int v = 0; v < V; ++v) worst = std::max(worst, n3_slice_scratch_doubles(nb, v, V));
+  *acc_off = (worst + 31) / 32 * 32;
+  return *acc_off + 3 * n_pad;
+}
+
 int prepare_split(nbr_ctx* c, const ForceConfig& cfg, long long n_pad_i) {
   if (cfg.ni == 3) {  // Newton-3 (the context's whole system only): its own partial sums
     (void)n_pad_i;
     const long long nb = ((long long)c->sys.n + kN3Block - 1) / kN3Block;
-    cudaError_t e = c->scr.need_part((size_t)n3_scratch_doubles(nb));
+    const int V = n3_bands(nb);
+    long long acc_off = 0;
+    const long long need =
+        V == 1 ? n3_scratch_doubles(nb) : n3_banded_doubles(nb, V, (long long)c->sys.n_pad, &acc_off);
+    cudaError_t e = c->scr.need_part((size_t)need);
     return e == cudaSuccess ? NBR_OK : cuda_fail(c, e, "Newton-3 scratch");
   }
   if (cfg.split <= 1) return NBR_OK;
@@ -431,7 +466,7 @@ int eval_system(nbr_ctx* c, int precision, double G, double eps2, int mode, doub
   if (precision == kFP32C) e = ensure_records(c, a, kernels);
   if (e != cudaSuccess) return cuda_fail(c, e, "pack");
   ForceConfig cfg = choose_config(c, precision, eps2, rn, s.ntiles);
-  if (cfg.ni == 3 && (ranged || rn > kN3MaxN))  // needs the whole system
+  if (cfg.ni == 3 && ranged)  // needs the whole system
     cfg = choose_config_large(c, precision, eps2, rn, s.ntiles);
   int rc = prepare_split(c, cfg, np_i);
   if (rc) return rc;
@@ -461,9 +496,27 @@ int eval_system(nbr_ctx* c, int precision, double G, double eps2, int mode, doub
       // test hook: under-report the receivers' length so that the check trips
       if (std::getenv("NBR_TEST_SHRINK_BOUNDS")) ip.len = rn - 1;)
   if (cfg.ni == 3) {
-    e = launch_force_n3(precision, cfg.warps, eps2, ip, js, ep, c->scr.part,
-                        (long long)c->scr.part_cap, c->stream);
-    if (kernels) *kernels += 2;
+    const long long nb = (rn + kN3Block - 1) / kN3Block;
+    const int V = n3_bands(nb);
+    if (V == 1) {
+      e = launch_force_n3(precision, cfg.warps, eps2, ip, js, ep, c->scr.part,
+                          (long long)c->scr.part_cap, c->stream);
+      if (kernels) *kernels += 2;
+    } else {
+      // banded: the slices' partial accelerations accumulate in slice order in
+      // an FP64 buffer behind the largest slice's scratch, then the epilogue
+      long long acc_off = 0;
+      n3_banded_doubles(nb, V, (long long)s.n_pad, &acc_off);
+      double* acc = c->scr.part + acc_off;
+      const long long np = (long long)s.n_pad;
+      for (int v = 0; v < V && e == cudaSuccess; ++v) {
+        e = launch_n3_slice(precision, cfg.warps, eps2, ip, js, ep.err, v, V, c->scr.part, acc_off,
+                            acc, np, 3 * np, v > 0, c->stream);
+        if (kernels) *kernels += 2;
+      }
+      if (e == cudaSuccess) e = launch_sum_finish(ip, ep, acc, 1, 0, np, 3 * np, c->stream);
+      if (kernels) *kernels += 1;
+    }
   } else {
     e = launch_force(precision, eps2, cfg, ip, js, ep, c->stream);
     if (kernels) ++*kernels;
@@ -840,6 +893,85 @@ int nbr_step_range(nbr_ctx* c, int precision, int scheme, size_t i0, size_t coun
   return rc;
 }
 
+int nbr_n3_slice_accel(nbr_ctx* c, int precision, double eps2, int slice, int nslices, double* dst,
+                       size_t ld) {
+  TraceRange trace_range("nbr_n3_slice_accel");
+  if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
+  if (precision != NBR_FP64 && precision != NBR_FP32C)
+    return fail(c, NBR_ERR_INVALID_ARG, "unknown precision");
+  if (!(eps2 >= 0.0) || !std::isfinite(eps2))
+    return fail(c, NBR_ERR_INVALID_ARG, "eps2 must be finite and >= 0");
+  if (nslices < 1 || slice < 0 || slice >= nslices)
+    return fail(c, NBR_ERR_INVALID_ARG, "need 0 <= slice < nslices");
+  SysState& s = c->sys;
+  if (s.n == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no system uploaded");
+  if (!dst || ld < s.n_pad)
+    return fail(c, NBR_ERR_INVALID_ARG, "dst is NULL or ld below the padded particle count");
+  cudaSetDevice(c->device);
+  const int a = s.cur;
+  cudaError_t e = precision == kFP32C ? ensure_records(c, a, nullptr) : cudaSuccess;
+  if (e != cudaSuccess) return cuda_fail(c, e, "pack");
+  const long long nb = ((long long)s.n + kN3Block - 1) / kN3Block;
+  const long long need = n3_slice_scratch_doubles(nb, slice, nslices);
+  e = c->scr.need_part((size_t)std::max<long long>(need, 1));
+  if (e != cudaSuccess) return cuda_fail(c, e, "Newton-3 slice scratch");
+  ForceConfig cfg = choose_config(c, precision, eps2, (long long)s.n, s.ntiles);
+  const int warps = cfg.ni == 3 ? cfg.warps : kN3Warps;
+  IParticles ip{s.pos[a][0], s.pos[a][1], s.pos[a][2], s.mass, (long long)s.n};
+  JStream js{s.pos[a][0], s.pos[a][1], s.pos[a][2], s.mass, s.rec[a], s.org[a], s.ntiles, 0, -1};
+  pipeline_params(js);
+  NBR_CHECKED_ONLY(ip.len = (long long)(s.cap + kRangeSlack); js.len = (long long)s.cap;)
+  e = launch_n3_slice(precision, warps, eps2, ip, js, c->d_err, slice, nslices, c->scr.part,
+                      (long long)c->scr.part_cap, dst, (long long)ld, 3 * (long long)ld, false,
+                      c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "Newton-3 slice launch");
+  c->acc_ok = false;
+  return NBR_OK;
+}
+
+int nbr_step_range_sum(nbr_ctx* c, int precision, int scheme, size_t i0, size_t count, double kick,
+                       double drift, double G, const double* src, int nslices, size_t vstride,
+                       size_t ld) {
+  TraceRange trace_range("nbr_step_range_sum");
+  if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
+  if (precision != NBR_FP64 && precision != NBR_FP32C)
+    return fail(c, NBR_ERR_INVALID_ARG, "unknown precision");
+  if (scheme != NBR_KDK && scheme != NBR_DKD && scheme != NBR_EULER)
+    return fail(c, NBR_ERR_INVALID_ARG, "unknown scheme");
+  if (!std::isfinite(kick) || !std::isfinite(drift) || !std::isfinite(G))
+    return fail(c, NBR_ERR_INVALID_ARG, "kick, drift, G must be finite");
+  SysState& s = c->sys;
+  if (s.n == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no system uploaded");
+  if (i0 % kTile != 0) return fail(c, NBR_ERR_INVALID_ARG, "i0 must be a multiple of 128");
+  if (count == 0 || i0 >= s.n) return fail(c, NBR_ERR_INVALID_ARG, "empty receiver range");
+  const size_t rn = std::min(count, s.n - i0);
+  const size_t rpad = (rn + kTile - 1) / kTile * kTile;
+  if (!src || nslices < 1 || ld < rpad || (nslices > 1 && vstride < 3 * ld))
+    return fail(c, NBR_ERR_INVALID_ARG, "src layout: ld >= count rounded up to 128, vstride >= 3 ld");
+  cudaSetDevice(c->device);
+  const int a = s.cur, b = 1 - s.cur;
+  IParticles ip{s.pos[a][0] + i0, s.pos[a][1] + i0, s.pos[a][2] + i0, s.mass + i0, (long long)rn};
+  Epilogue ep{};
+  ep.mode = scheme == NBR_EULER ? 2 : 1;
+  ep.G = G;
+  ep.ax = s.acc[0] + i0; ep.ay = s.acc[1] + i0; ep.az = s.acc[2] + i0;
+  ep.kick = kick;
+  ep.drift = drift;
+  ep.vx = s.vel[0] + i0; ep.vy = s.vel[1] + i0; ep.vz = s.vel[2] + i0;
+  ep.xn = s.pos[b][0] + i0; ep.yn = s.pos[b][1] + i0; ep.zn = s.pos[b][2] + i0;
+  ep.rec_next = nullptr;
+  ep.err = c->d_err;
+  NBR_CHECKED_ONLY(ip.len = (long long)(s.cap + kRangeSlack) - (long long)i0;)
+  const long long src_len = (long long)(nslices - 1) * (long long)vstride + 3 * (long long)ld;
+  cudaError_t e = launch_sum_finish(ip, ep, src, nslices, (long long)vstride, (long long)ld, src_len,
+                                    c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "slice sum launch");
+  s.cur = b;
+  s.rec_ok[0] = s.rec_ok[1] = false;
+  c->acc_ok = false;
+  return NBR_OK;
+}
+
 int nbr_state_pointers(nbr_ctx* c, double** x, double** y, double** z, double** vx, double** vy,
                        double** vz, size_t* len) {
   if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
@@ -1192,8 +1324,6 @@ int nbr_get_force_tiling(nbr_ctx* c, int precision, double eps2, int* tile, int*
   if (s.n == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no system uploaded");
   cudaSetDevice(c->device);
   ForceConfig cfg = choose_config(c, precision, eps2, (long long)s.n, s.ntiles);
-  if (cfg.ni == 3 && (long long)s.n > kN3MaxN)
-    cfg = choose_config_large(c, precision, eps2, (long long)s.n, s.ntiles);
   const bool large = cfg.ni == 4 || cfg.ni == 8;
   if (tile) *tile = large ? (cfg.tile > 0 ? cfg.tile : kDefaultTileJ) : 0;
   if (unroll) *unroll = large ? (cfg.unroll > 0 ? cfg.unroll : default_unroll(precision)) : 0;
@@ -1208,8 +1338,6 @@ int nbr_get_force_config(nbr_ctx* c, int precision, double eps2, int* ni, int* w
   if (s.n == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no system uploaded");
   cudaSetDevice(c->device);
   ForceConfig cfg = choose_config(c, precision, eps2, (long long)s.n, s.ntiles);
-  if (cfg.ni == 3 && (long long)s.n > kN3MaxN)
-    cfg = choose_config_large(c, precision, eps2, (long long)s.n, s.ntiles);
   if (ni) *ni = cfg.ni;
   if (warps) *warps = cfg.warps;
   if (split) *split = cfg.split;
@@ -1237,7 +1365,7 @@ int nbr_autotune(nbr_ctx* c, int precision, double eps2) {
   float best_ms = 1e30f;
   for (auto& cw : cand) {
     if (cw[0] == 1 && s.n > 65536) continue;  // the small-N kernel only competes on small systems
-    if (cw[0] == 3 && (s.n < 8192 || (long long)s.n > kN3MaxN)) continue;
+    if (cw[0] == 3 && s.n < 8192) continue;
     if (cw[0] == 3 && cw[1] == 16 && precision != kFP32C) continue;  // FP64 has one Newton-3 layout
     ForceConfig base{cw[0], cw[1], 1};
     const int s0 = auto_split(precision, eps2, base, (long long)s.n, s.ntiles, c->sms);

@@ -687,8 +687,8 @@ __global__ void __launch_bounds__(kN3Warps * 32)
   unsigned char* stages = smem + kSmemHead;
   float* red = reinterpret_cast<float*>(stages + kStages * kStage32);  // [warp][3][256]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int g = 0, k = blockIdx.x;
-  const int groups = (int)((p3.nb + kN3Warps - 1) / kN3Warps);
+  int g = p3.g0, k = blockIdx.x;
+  const int groups = p3.g1;  // row groups [g0, g1) of this launch
   while (g < groups) {  // the grid has exactly sum_g n3_chunks(nb, cols, g) CTAs
     const int K = n3_chunks(p3.nb, p3.cols, g);
     if (k < K) break;
@@ -913,8 +913,8 @@ __global__ void __launch_bounds__(kN3F64Warps * 32, 1)
   float* red = reinterpret_cast<float*>(stages + kStages * kStage32);  // [warp][3][256]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int rb = warp >> 1, hf = warp & 1;  // row block in the group, its receiver half
-  int g = 0, k = blockIdx.x;
-  const int groups = (int)((p3.nb + kN3Warps - 1) / kN3Warps);
+  int g = p3.g0, k = blockIdx.x;
+  const int groups = p3.g1;  // row groups [g0, g1) of this launch
   while (g < groups) {  // the grid has exactly sum_g n3_chunks(nb, cols, g) CTAs
     const int K = n3_chunks(p3.nb, p3.cols, g);
     if (k < K) break;
@@ -1142,8 +1142,8 @@ __global__ void __launch_bounds__(kN3F64Warps * 32)
   double* red = reinterpret_cast<double*>(stages + kStages * kStage64);  // [warp][3][256]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int rb = warp >> 1, hf = warp & 1;  // row block in the group, its receiver half
-  int g = 0, k = blockIdx.x;
-  const int groups = (int)((p3.nb + kN3Warps - 1) / kN3Warps);
+  int g = p3.g0, k = blockIdx.x;
+  const int groups = p3.g1;  // row groups [g0, g1) of this launch
   while (g < groups) {  // the grid has exactly sum_g n3_chunks(nb, cols, g) CTAs
     const int K = n3_chunks(p3.nb, p3.cols, g);
     if (k < K) break;
@@ -1289,10 +1289,13 @@ __global__ void __launch_bounds__(kN3F64Warps * 32)
 }
 
 // Adds the Newton-3 partial sums of each particle in a fixed order (its row
-// group's chunks, then the reactions from row groups 0 .. its own) and runs the
-// epilogue of the large kernels.  One warp per 128-particle tile.
+// group's chunks, then the reactions from the launch's row groups g0 .. its
+// own) and then, by mode: 0 runs the epilogue of the large kernels; 1 stores
+// the sums into dst[d * ld + i] (zero for particles the row groups do not
+// reach); 2 adds them to dst.  One warp per 128-particle tile.
 __global__ void __launch_bounds__(128)
-    k_n3_reduce(const IParticles ip, const Epilogue ep, const N3Params p3) {
+    k_n3_reduce(const IParticles ip, const Epilogue ep, const N3Params p3, int mode, double* dst,
+                long long ld) {
   const int lane = threadIdx.x & 31;
   const long long tile = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (tile * kTile >= p3.nb * kN3Block) return;
@@ -1300,8 +1303,9 @@ __global__ void __launch_bounds__(128)
   const int g = (int)(b / kN3Warps), w = (int)(b % kN3Warps);
   const int jb0 = (int)(tile & 1) * kTile + lane;  // particle index inside the block (k = 0)
   double ax[4] = {0, 0, 0, 0}, ay[4] = {0, 0, 0, 0}, az[4] = {0, 0, 0, 0};
-  long long prefix = 0;  // CTAs of row groups before g'
-  for (int gp = 0; gp <= g; ++gp) {
+  long long prefix = 0;  // CTAs of the launch's row groups before g'
+  const int glast = min(g, p3.g1 - 1);
+  for (int gp = p3.g0; gp <= glast; ++gp) {
     const int K = n3_chunks(p3.nb, p3.cols, gp);
     if (gp == g) {
       for (int k = 0; k < K; ++k) {
@@ -1330,11 +1334,50 @@ __global__ void __launch_bounds__(128)
     prefix += K;
   }
   const long long ibase = tile * kTile + lane;
+  if (mode != 0) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const long long i = ibase + 32 * q;
+      if (!NBR_IN(2 * ld + i, p3.dst_len, ep.err)) continue;
+      if (mode == 1) {
+        dst[i] = ax[q]; dst[ld + i] = ay[q]; dst[2 * ld + i] = az[q];
+      } else {
+        dst[i] += ax[q]; dst[ld + i] += ay[q]; dst[2 * ld + i] += az[q];
+      }
+    }
+    return;
+  }
   double xi[4], yi[4], zi[4];
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
     const long long i = ibase + 32 * q;
     xi[q] = ip.x[i]; yi[q] = ip.y[i]; zi[q] = ip.z[i];
+  }
+  epilogue<4>(ip, ep, ibase, lane, xi, yi, zi, ax, ay, az);
+}
+
+// Sums V partial accelerations per particle in slice order, src[v * vstride
+// + d * ld + i] (i < ip.n, rounded up to whole tiles), and runs the epilogue
+// of the large kernels on the receivers ip.  One warp per 128-particle tile.
+__global__ void __launch_bounds__(128)
+    k_sum_finish(const IParticles ip, const Epilogue ep, const double* src, int V, long long vstride,
+                 long long ld, long long src_len) {
+  const int lane = threadIdx.x & 31;
+  const long long tile = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (tile * kTile >= ip.n) return;
+  const long long ibase = tile * kTile + lane;
+  double ax[4] = {0, 0, 0, 0}, ay[4] = {0, 0, 0, 0}, az[4] = {0, 0, 0, 0};
+  double xi[4], yi[4], zi[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const long long i = ibase + 32 * q;
+    for (int v = 0; v < V; ++v) {
+      const double* S = src + (size_t)v * vstride;
+      if (!NBR_IN((long long)v * vstride + 2 * ld + i, src_len, ep.err)) continue;
+      ax[q] += S[i]; ay[q] += S[ld + i]; az[q] += S[2 * ld + i];
+    }
+    xi[q] = yi[q] = zi[q] = 0.0;
+    if (NBR_IN(i, ip.len, ep.err)) { xi[q] = ip.x[i]; yi[q] = ip.y[i]; zi[q] = ip.z[i]; }
   }
   epilogue<4>(ip, ep, ibase, lane, xi, yi, zi, ax, ay, az);
 }
@@ -1763,6 +1806,8 @@ cudaError_t launch_force_n3(int precision, int warps, double eps2, const IPartic
   p3.cols = n3_cols(p3.nb);
   const long long ctas = n3_ctas(p3.nb, p3.cols);
   if (ctas > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+  p3.g0 = 0;
+  p3.g1 = (int)((p3.nb + kN3Warps - 1) / kN3Warps);
   p3.act = scratch;
   p3.rea = scratch + (size_t)ctas * kN3Warps * 3 * kN3Block;
   NBR_CHECKED_ONLY(p3.act_len = scratch_len;)
@@ -1789,7 +1834,65 @@ cudaError_t launch_force_n3(int precision, int warps, double eps2, const IPartic
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   const long long threads = p3.nb * 2 * 32;  // a warp per tile
-  k_n3_reduce<<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(ip, ep, p3);
+  k_n3_reduce<<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(ip, ep, p3, 0, nullptr, 0);
+  return cudaGetLastError();
+}
+
+// The pair kernel of a Newton-3 launch over row groups [g0, g1).
+cudaError_t launch_n3_pairs(int precision, int warps, double eps2, const IParticles& ip,
+                            const JStream& js, int* err, N3Params& p3, cudaStream_t st) {
+  const long long ctas = n3_ctas_range(p3.nb, p3.cols, p3.g0, p3.g1);
+  if (ctas <= 0) return cudaSuccess;
+  if (ctas > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+  const bool w2 = precision == kFP32C && warps == kN3F64Warps;
+  const size_t smem = n3_smem_bytes(precision, precision == kFP32C ? warps : kN3F64Warps);
+  const unsigned grid = (unsigned)ctas,
+                 block = (precision == kFP32C && !w2 ? kN3Warps : kN3F64Warps) * 32;
+  const float e32 = (float)eps2;
+  if (w2) {
+    if (eps2 == 0.0) k_force_n3_f32c_w2<true><<<grid, block, smem, st>>>(ip, js, p3, 0.f, err);
+    else k_force_n3_f32c_w2<false><<<grid, block, smem, st>>>(ip, js, p3, e32, err);
+  } else if (precision == kFP32C) {
+    if (eps2 == 0.0) k_force_n3_f32c<true><<<grid, block, smem, st>>>(ip, js, p3, 0.f, err);
+    else k_force_n3_f32c<false><<<grid, block, smem, st>>>(ip, js, p3, e32, err);
+  } else {
+    if (eps2 == 0.0) k_force_n3_f64<true><<<grid, block, smem, st>>>(ip, js, p3, 0.0, err);
+    else k_force_n3_f64<false><<<grid, block, smem, st>>>(ip, js, p3, eps2, err);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_n3_slice(int precision, int warps, double eps2, const IParticles& ip,
+                            const JStream& js, int* err, int slice, int nslices, double* scratch,
+                            long long scratch_len, double* dst, long long ld, long long dst_len,
+                            bool accumulate, cudaStream_t st) {
+  if (ip.n <= 0 || js.ntiles <= 0) return cudaSuccess;
+  N3Params p3{};
+  p3.nb = (ip.n + kN3Block - 1) / kN3Block;
+  p3.cols = n3_cols(p3.nb);
+  n3_slice_groups(p3.nb, p3.cols, slice, nslices, &p3.g0, &p3.g1);
+  const long long ctas = n3_ctas_range(p3.nb, p3.cols, p3.g0, p3.g1);
+  p3.act = scratch;
+  p3.rea = scratch + (size_t)ctas * kN3Warps * 3 * kN3Block;
+  NBR_CHECKED_ONLY(p3.act_len = scratch_len; p3.dst_len = dst_len;)
+  (void)scratch_len;
+  (void)dst_len;
+  cudaError_t e = launch_n3_pairs(precision, warps, eps2, ip, js, err, p3, st);
+  if (e != cudaSuccess) return e;
+  Epilogue ep{};
+  ep.err = err;
+  const long long threads = p3.nb * 2 * 32;  // a warp per tile
+  k_n3_reduce<<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(ip, ep, p3, accumulate ? 2 : 1,
+                                                                  dst, ld);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sum_finish(const IParticles& ip, const Epilogue& ep, const double* src, int V,
+                              long long vstride, long long ld, long long src_len, cudaStream_t st) {
+  if (ip.n <= 0) return cudaSuccess;
+  const long long threads = ((ip.n + kTile - 1) / kTile) * 32;
+  k_sum_finish<<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(ip, ep, src, V, vstride, ld,
+                                                                  src_len);
   return cudaGetLastError();
 }
 

@@ -99,13 +99,21 @@ constexpr int kN3MaxCols = 32;
 struct N3Params {
   long long nb;  // blocks holding real particles: ceil(n / kN3Block)
   int cols;      // column blocks per CTA
+  int g0, g1;    // row groups [g0, g1) of this launch (all: 0, ceil(nb / kN3Warps))
   double* act;   // action partials [cta][row block][3][kN3Block]
   double* rea;   // reaction partials [cta][column block][3][kN3Block]
   NBR_CHECKED_FIELD(long long act_len)  // doubles from act (through rea's end)
+  NBR_CHECKED_FIELD(long long dst_len)  // doubles of a slice reduction's destination
 };
-// Largest system the Newton-3 kernel takes: its partial sums grow as N^2
-// (8.4 GB at 2^20 particles).
-constexpr long long kN3MaxN = 1LL << 20;
+// The Newton-3 partial sums grow as N^2 (8.4 GB at 2^20 particles).  Up to
+// kN3SingleMaxDoubles one launch covers the system; above it the evaluation
+// runs in row-group slices of at most kN3SliceMaxDoubles each, whose partial
+// accelerations accumulate in slice order in an FP64 buffer (3 x 8 B per
+// particle), so the scratch stays bounded at any N.
+constexpr long long kN3SingleMaxDoubles = 9LL << 27;  // 9 GiB
+constexpr long long kN3SliceMaxDoubles = 1LL << 28;   // 2 GiB
+// Largest system the Newton-3 kernel is the default for.
+constexpr long long kN3MaxN = 1LL << 23;
 // Smallest system the default configuration gives the Newton-3 kernel.
 constexpr long long kN3MinN = 16384;
 // Column chunks (CTAs) of row group g.
@@ -129,6 +137,36 @@ inline long long n3_scratch_doubles(long long nb) {
   const int cols = n3_cols(nb);
   return n3_ctas(nb, cols) * (long long)(kN3Warps + cols) * 3 * kN3Block;
 }
+// CTAs of the row groups [g0, g1).
+inline long long n3_ctas_range(long long nb, int cols, int g0, int g1) {
+  long long t = 0;
+  for (int g = g0; g < g1; ++g) t += n3_chunks(nb, cols, g);
+  return t;
+}
+// Row groups [g0, g1) of slice v of V: consecutive groups with about the same
+// number of CTAs (the same pair work) in each slice; slices may be empty.
+inline void n3_slice_groups(long long nb, int cols, int v, int V, int* g0, int* g1) {
+  const int groups = (int)((nb + kN3Warps - 1) / kN3Warps);
+  const long long total = n3_ctas(nb, cols);
+  auto start = [&](int s) {
+    if (s <= 0) return 0;
+    if (s >= V) return groups;
+    const long long target = (total * s + V - 1) / V;  // first CTA of slice s
+    long long acc = 0;
+    int g = 0;
+    while (g < groups && acc < target) acc += n3_chunks(nb, cols, g++);
+    return g;
+  };
+  *g0 = start(v);
+  *g1 = start(v + 1);
+}
+// Doubles of partial-sum scratch of slice v of V.
+inline long long n3_slice_scratch_doubles(long long nb, int v, int V) {
+  const int cols = n3_cols(nb);
+  int g0 = 0, g1 = 0;
+  n3_slice_groups(nb, cols, v, V, &g0, &g1);
+  return n3_ctas_range(nb, cols, g0, g1) * (long long)(kN3Warps + cols) * 3 * kN3Block;
+}
 // One Newton-3 force evaluation over all n_pad receivers of ip against the
 // same particles in js (FP32C: their records; FP64: their x, y, z, m arrays),
 // with the epilogue ep: the pair kernel, then the per-particle reduction.
@@ -137,6 +175,19 @@ inline long long n3_scratch_doubles(long long nb) {
 cudaError_t launch_force_n3(int precision, int warps, double eps2, const IParticles& ip,
                             const JStream& js, const Epilogue& ep, double* scratch,
                             long long scratch_len, cudaStream_t stream);
+// Newton-3 partial accelerations (not G-scaled) of every particle from the
+// pairs of slice `slice` of `nslices` (n3_slice_groups): stored into dst[d *
+// ld + i] (i < n rounded up to 256), or added to it (accumulate); scratch
+// holds n3_slice_scratch_doubles doubles.
+cudaError_t launch_n3_slice(int precision, int warps, double eps2, const IParticles& ip,
+                            const JStream& js, int* err, int slice, int nslices, double* scratch,
+                            long long scratch_len, double* dst, long long ld, long long dst_len,
+                            bool accumulate, cudaStream_t stream);
+// The epilogue of the large kernels on the receivers ip, from V partial
+// accelerations per particle summed in slice order: src[v * vstride + d * ld + i].
+cudaError_t launch_sum_finish(const IParticles& ip, const Epilogue& ep, const double* src, int V,
+                              long long vstride, long long ld, long long src_len,
+                              cudaStream_t stream);
 // Kernel attributes that must be set once per device, outside stream capture.
 cudaError_t configure_kernels();
 

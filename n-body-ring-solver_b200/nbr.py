@@ -109,6 +109,10 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "nbr_batch_autotune": ([C.c_void_p, C.c_int, C.c_double], C.c_int),
         "nbr_step_range": ([C.c_void_p, C.c_int, C.c_int, _SZ, _SZ, C.c_double, C.c_double, C.c_double,
                             C.c_double], C.c_int),
+        "nbr_n3_slice_accel": ([C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int, C.c_void_p, _SZ],
+                               C.c_int),
+        "nbr_step_range_sum": ([C.c_void_p, C.c_int, C.c_int, _SZ, _SZ, C.c_double, C.c_double,
+                                C.c_double, C.c_void_p, C.c_int, _SZ, _SZ], C.c_int),
         "nbr_state_pointers": ([C.c_void_p] + [C.POINTER(C.c_void_p)] * 6 + [C.POINTER(_SZ)], C.c_int),
         "nbr_state_changed": ([C.c_void_p], C.c_int),
         "nbr_snapshot_write_arrays": ([C.c_char_p, _SZ, _SZ, C.c_double] + [_D] * 10, C.c_int),
@@ -263,6 +267,11 @@ class _DeviceArray:
 
 
 # ------------------------------------------------------------------- context --
+def torch_float64():
+    import torch
+    return torch.float64
+
+
 class Context:
     """One GPU context (its own CUDA stream); see include/nbr.h."""
 
@@ -385,6 +394,25 @@ class Context:
         kick/drift, asynchronous on the context's stream."""
         self._chk(self.L.nbr_step_range(self.h, precision, scheme, i0, count, kick, drift, G, eps2),
                   "step_range")
+
+    def n3_slice_accel(self, precision, eps2, slice_, nslices, dst):
+        """Newton-3 partial accelerations of every particle from slice
+        `slice_` of `nslices` into dst, a contiguous device tensor of shape
+        (3, ld) float64 (ld >= the padded size), asynchronous on the context's
+        stream."""
+        assert dst.dtype == torch_float64() and dst.is_contiguous() and dst.dim() == 2
+        self._chk(self.L.nbr_n3_slice_accel(self.h, precision, eps2, slice_, nslices,
+                                            C.c_void_p(dst.data_ptr()), dst.stride(0)),
+                  "n3_slice_accel")
+
+    def step_range_sum(self, precision, scheme, i0, count, kick, drift, G, src):
+        """Kick/drift of receivers [i0, i0 + count) from the partial
+        accelerations src (device tensor (nslices, 3, ld) float64, contiguous,
+        receiver i0 + k at [:, :, k]) summed in slice order."""
+        assert src.dtype == torch_float64() and src.is_contiguous() and src.dim() == 3
+        self._chk(self.L.nbr_step_range_sum(self.h, precision, scheme, i0, count, kick, drift, G,
+                                            C.c_void_p(src.data_ptr()), src.shape[0],
+                                            src.stride(0), src.stride(1)), "step_range_sum")
 
     def state_pointers(self):
         """Device addresses of the current x, y, z, vx, vy, vz arrays and their length."""

@@ -13,9 +13,21 @@ positions (:310), here an NCCL all-gather over NVLink on the context's stream.
 The exchange is the only collective, once per force evaluation, 24 bytes per
 particle.  Velocities stay with their owner until gather_velocities().
 
-The context object only needs upload / step_range / state_tensors /
-state_changed / download and a `stream` attribute (nbr.Context provides
-them), so the host logic here is independent of where the arithmetic runs.
+method="newton3" evaluates each unordered pair once across the ranks, as
+hybrid_ring_solver does by sending partial forces around the ring with the
+positions (CPU/hybrid_solver.cpp:52-107): the block-pair triangle is cut
+into `slices` slices of equal pair work (nbr_n3_slice_accel), rank r
+computes slices [r V / W, (r + 1) V / W) for every particle, an all-to-all
+hands each rank every slice's partials of its own receivers, and the rank
+adds them in slice order and updates its receivers (nbr_step_range_sum);
+then the position all-gather.  The sum order depends only on V, so any
+world size W <= V gives the same bits.  Per step and rank: V/W slice
+launches, (V/W) x 24 B x n out and about 24 B x n in, plus the all-gather.
+
+The context object only needs upload / step_range (n3_slice_accel /
+step_range_sum for newton3) / state_tensors / state_changed / download and a
+`stream` attribute (nbr.Context provides them), so the host logic here is
+independent of where the arithmetic runs.
 """
 from __future__ import annotations
 
@@ -41,6 +53,12 @@ def shard_bounds(n: int, world: int, rank: int) -> Tuple[int, int, int]:
     return i0, count, owned
 
 
+def slice_range(slices: int, world: int, rank: int) -> Tuple[int, int]:
+    """Slices [v0, v1) of the Newton-3 partition computed by rank (ranks in
+    order hold consecutive slices, so receiving in rank order is slice order)."""
+    return rank * slices // world, (rank + 1) * slices // world
+
+
 class ShardedSystem:
     """A system integrated by `world` processes, one context each.
 
@@ -48,13 +66,19 @@ class ShardedSystem:
     (default: the world).  The context's stream orders everything: the
     exchange runs on it (torch.cuda.ExternalStream) for device tensors."""
 
-    def __init__(self, ctx, group=None):
+    def __init__(self, ctx, group=None, method: str = "range", slices: int = 8):
         self.ctx = ctx
         self.group = group
         self.rank = dist.get_rank(group)
         self.world = dist.get_world_size(group)
         self.n = 0
         self.collectives = 0
+        if method not in ("range", "newton3"):
+            raise ValueError("method is 'range' or 'newton3'")
+        if method == "newton3" and slices < self.world:
+            raise ValueError("newton3 needs at least one slice per rank")
+        self.method = method
+        self.slices = slices
 
     # ---------------------------------------------------------------- state --
     def upload(self, system: Dict[str, np.ndarray]):
@@ -64,6 +88,17 @@ class ShardedSystem:
         self.ctx.upload(system)
         self.n = len(system["x"])
         self.i0, self.count, self.owned = shard_bounds(self.n, self.world, self.rank)
+        if self.method == "newton3":
+            V, W, c = self.slices, self.world, self.count
+            dev = self.ctx.state_tensors()["x"].device
+            n_pad = -(-self.n // 1024) * 1024
+            ld = max(n_pad, W * c)
+            self.v0, self.v1 = slice_range(V, W, self.rank)
+            # this rank's slices for every particle; every slice for own receivers
+            self._mine = torch.zeros((self.v1 - self.v0, 3, ld), dtype=torch.float64, device=dev)
+            self._recv = torch.zeros((V, 3, c), dtype=torch.float64, device=dev)
+            if dev.type == "cuda":
+                torch.cuda.synchronize(dev)  # zero fills done before the context's stream uses them
 
     def _stream_ctx(self, t: torch.Tensor):
         if t.is_cuda:
@@ -72,19 +107,16 @@ class ShardedSystem:
 
     def _all_gather(self, arrays):
         """All-gathers the owned slices [i0, i0 + count) of each array in
-        place: after it, every rank's arrays hold every rank's slice."""
+        place (one all-gather per array, no staging copies): after it, every
+        rank's arrays hold every rank's slice."""
         c, w, r = self.count, self.world, self.rank
         t0 = arrays[0]
         if w * c > t0.numel():
             raise RuntimeError(f"shards of {c} x {w} exceed the arrays' {t0.numel()} entries")
         with self._stream_ctx(t0):
-            mine = torch.stack([a[r * c:(r + 1) * c] for a in arrays])          # [k, c]
-            kk = mine.shape[0]
-            out = torch.empty((w * kk, c), dtype=mine.dtype, device=mine.device)
-            dist.all_gather_into_tensor(out, mine, group=self.group)           # [w * k, c]
-            out = out.view(w, kk, c)
-            for k, a in enumerate(arrays):
-                a[:w * c].view(w, c).copy_(out[:, k, :])
+            for a in arrays:
+                # in place: this rank's shard is already where the gather puts it
+                dist.all_gather_into_tensor(a[:w * c], a[r * c:(r + 1) * c], group=self.group)
         self.collectives += 1
 
     def exchange_positions(self):
@@ -104,9 +136,28 @@ class ShardedSystem:
         then the position exchange.  A rank that owns no receivers only takes
         part in the exchange, which overwrites all n positions of its current
         buffer."""
-        if self.owned > 0:
+        if self.method == "newton3":
+            self._step_newton3(precision, scheme, kick, drift, G, eps2)
+        elif self.owned > 0:
             self.ctx.step_range(precision, scheme, self.i0, self.owned, kick, drift, G, eps2)
         self.exchange_positions()
+
+    def _step_newton3(self, precision, scheme, kick, drift, G, eps2):
+        V, W, c = self.slices, self.world, self.count
+        nv = self.v1 - self.v0
+        with self._stream_ctx(self._mine):
+            for v in range(self.v0, self.v1):
+                self.ctx.n3_slice_accel(precision, eps2, v, V, self._mine[v - self.v0])
+            # columns of every rank's receivers: [W][nv][3][c] out, [V][3][c] in
+            send = self._mine[:, :, :W * c].reshape(nv, 3, W, c).permute(2, 0, 1, 3).contiguous()
+            out_splits = [(slice_range(V, W, q)[1] - slice_range(V, W, q)[0]) * 3 * c
+                          for q in range(W)]
+            dist.all_to_all_single(self._recv.view(-1), send.view(-1), out_splits,
+                                   [nv * 3 * c] * W, group=self.group)
+            if self.owned > 0:
+                self.ctx.step_range_sum(precision, scheme, self.i0, self.owned, kick, drift, G,
+                                        self._recv)
+        self.collectives += 1
 
     def run(self, precision: int, scheme: int, dt: float, steps: int, G: float = 1.0,
             eps2: float = 0.0) -> int:

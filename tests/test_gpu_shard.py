@@ -136,3 +136,120 @@ def test_step_range_argument_errors(nbr):
     ptrs, ln = c.state_pointers()
     assert ln >= 1024 + 1024 and all(p for p in ptrs.values())
     c.close()
+
+
+def _slices(ctx, prec, eps2, V, ld):
+    out = torch.zeros((V, 3, ld), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()  # the zero fill runs on torch's stream, the slices on the context's
+    for v in range(V):
+        ctx.n3_slice_accel(prec, eps2, v, V, out[v])
+    ctx.synchronize()
+    return out
+
+
+@pytest.mark.parametrize("prec", [0, 1], ids=["fp64", "fp32c"])
+@pytest.mark.parametrize("n", [300, 5000, 20000])
+def test_newton3_slices_sum_to_the_forces(nbr, oracle, prec, n):
+    """The Newton-3 slices of the multi-GPU partition: for any slice count
+    their sum is every particle's acceleration (each pair once), against the
+    oracle; empty slices (more slices than row groups) hold zeros."""
+    s = nbr.plummer(n, 7)
+    eps2 = 1e-6
+    ref = oracle.accel(s["x"], s["y"], s["z"], s["m"], eps2=eps2, extended=True)
+    ld = -(-n // 1024) * 1024
+    with nbr.Context(0) as c:
+        c.upload(s)
+        for V in (1, 3, 8, 40):
+            P = _slices(c, prec, eps2, V, ld).cpu().numpy()
+            a = P[0].copy()
+            for v in range(1, V):
+                a += P[v]
+            e = np.linalg.norm(a[:, :n] - ref, axis=0) / np.linalg.norm(ref, axis=0)
+            if prec == 0:
+                assert e.max() <= 1e-12, (V, e.max())
+            else:
+                assert np.median(e) <= 1e-6 and e.max() <= 1e-4, (V, np.median(e), e.max())
+            assert not P[:, :, n:].any()
+
+
+def _n3_emulated(nbr, s, prec, scheme, dt, steps, world, eps2, V=8):
+    """Newton-3 across `world` emulated ranks on one GPU: each context
+    computes its slices for every particle, the owned columns are exchanged
+    by device copies (the all-to-all), each rank adds them in slice order for
+    its receivers (nbr_step_range_sum), then positions are exchanged."""
+    n = len(s["x"])
+    ctxs = [nbr.Context(0) for _ in range(world)]
+    for c in ctxs:
+        c.upload(s)
+    ld = max(-(-n // 1024) * 1024, world * nbr_shard.shard_bounds(n, world, 0)[1])
+    if scheme == nbr.KDK:
+        sched = [(0.5 * dt, dt)] + [(dt, dt)] * (steps - 1) + [(0.5 * dt, 0.0)]
+    else:
+        sched = [(dt, dt)] * steps
+    for kick, drift in sched:
+        P = torch.zeros((V, 3, ld), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        for r, c in enumerate(ctxs):
+            v0, v1 = nbr_shard.slice_range(V, world, r)
+            for v in range(v0, v1):
+                c.n3_slice_accel(prec, eps2, v, V, P[v])
+            c.synchronize()
+        for r, c in enumerate(ctxs):
+            i0, cnt, owned = nbr_shard.shard_bounds(n, world, r)
+            if owned:
+                src = P[:, :, i0:i0 + cnt].contiguous()
+                torch.cuda.synchronize()
+                c.step_range_sum(prec, scheme, i0, owned, kick, drift, 1.0, src)
+        _exchange(ctxs, n)
+    _gather_velocities(ctxs, n)
+    out = ctxs[0].download()
+    for c in ctxs:
+        c.synchronize()
+        c.close()
+    return out
+
+
+@pytest.mark.parametrize("prec", [0, 1], ids=["fp64", "fp32c"])
+@pytest.mark.parametrize("scheme", [0, 2], ids=["kdk", "euler"])
+def test_newton3_emulated_ranks(nbr, oracle, prec, scheme):
+    """1, 2 and 3 emulated ranks give the same bits (the sum order depends
+    only on the slice count), and the oracle's trajectory."""
+    n, eps2, dt, steps = 6000, 1e-6, 1e-3, 3
+    s = nbr.plummer(n, 8)
+    one = _n3_emulated(nbr, s, prec, scheme, dt, steps, 1, eps2)
+    for world in (2, 3):
+        got = _n3_emulated(nbr, s, prec, scheme, dt, steps, world, eps2)
+        for k in ("x", "y", "z", "vx", "vy", "vz"):
+            np.testing.assert_array_equal(got[k], one[k], err_msg=k)
+    want = oracle.kdk(s, dt, steps, eps2=eps2) if scheme == nbr.KDK else oracle.euler(s, dt, steps, eps2=eps2)
+    tol = 1e-11 if prec == 0 else 1e-6
+    for k in ("x", "y", "z", "vx", "vy", "vz"):
+        assert np.abs(one[k] - want[k]).max() <= tol, k
+
+
+@pytest.mark.parametrize("prec", [0, 1], ids=["fp64", "fp32c"])
+def test_banded_newton3_evaluation(nbr, oracle, prec):
+    """The banded whole-system Newton-3 evaluation (slices accumulated in
+    order in an FP64 buffer, then the epilogue), forced by a test hook on a
+    system small enough for the oracle: forces and a KDK run."""
+    import os
+    n, eps2 = 20000, 1e-6
+    s = nbr.plummer(n, 12)
+    os.environ["NBR_TEST_N3_SLICES"] = "5"
+    try:
+        with nbr.Context(0) as c:
+            c.set_force_config(prec, 3, 8, 0)
+            c.upload(s)
+            a = c.forces(prec, eps2=eps2)
+            c.upload(s)
+            c.run(prec, 0, 2, 1e-3, 3, eps2=eps2)
+            got = c.download()
+    finally:
+        del os.environ["NBR_TEST_N3_SLICES"]
+    idx = np.arange(0, n, 53)
+    ref = oracle.accel_subset(s["x"], s["y"], s["z"], s["m"], idx, eps2=eps2)
+    e = np.linalg.norm(a[:, idx] - ref, axis=0) / np.linalg.norm(ref, axis=0)
+    assert (e.max() <= 1e-12) if prec == 0 else (np.median(e) <= 1e-6 and e.max() <= 1e-4)
+    want = oracle.kdk(s, 1e-3, 3, eps2=eps2)
+    for k in ("x", "y", "z", "vx", "vy", "vz"):
+        assert np.abs(got[k] - want[k]).max() <= (1e-11 if prec == 0 else 1e-6), k

@@ -54,6 +54,34 @@ class OracleRangeContext:
             self.pos[b][d][r] = self.pos[a][d][r] + drift * v_drift
         self.cur = b
 
+    def n3_slice_accel(self, precision, eps2, v, V, dst):
+        """Stand-in slice: the accelerations from the sources of index block v
+        of V (a different partition of the pairs than the library's, with
+        the same property: the V slices together hold each pair once)."""
+        n = self.n
+        lo, hi = n * v // V, n * (v + 1) // V
+        m = np.zeros(n)
+        m[lo:hi] = self.m[lo:hi]
+        x, y, z = (p[:n].copy() for p in self.pos[self.cur])
+        a = self.orc.accel(x, y, z, m, 1.0, eps2)
+        dst.zero_()
+        dst[:, :n] = torch.from_numpy(a)
+
+    def step_range_sum(self, precision, scheme, i0, count, kick, drift, G, src):
+        n, a, b = self.n, self.cur, 1 - self.cur
+        cnt = min(count, n - i0)
+        acc = np.zeros((3, cnt))
+        for v in range(src.shape[0]):  # slice order
+            acc += src[v, :, :cnt].numpy()
+        acc *= G
+        r = slice(i0, i0 + cnt)
+        for d in range(3):
+            v_old = self.vel[d][r].copy()
+            self.vel[d][r] += kick * acc[d]
+            v_drift = v_old if scheme == 2 else self.vel[d][r]
+            self.pos[b][d][r] = self.pos[a][d][r] + drift * v_drift
+        self.cur = b
+
     def state_tensors(self):
         p = self.pos[self.cur]
         return {"x": torch.from_numpy(p[0]), "y": torch.from_numpy(p[1]), "z": torch.from_numpy(p[2]),
@@ -77,13 +105,13 @@ def _system(n, seed):
     return s
 
 
-def _worker(rank, world, port, outdir, n, scheme, steps):
+def _worker(rank, world, port, outdir, n, scheme, steps, method="range"):
     os.environ["OMP_NUM_THREADS"] = "1"
     dist.init_process_group("gloo", rank=rank, world_size=world,
                             init_method=f"tcp://127.0.0.1:{port}")
     try:
         ctx = OracleRangeContext()
-        sh = nbr_shard.ShardedSystem(ctx)
+        sh = nbr_shard.ShardedSystem(ctx, method=method, slices=8)
         sh.upload(_system(n, 11))
         evals = sh.run(0, scheme, 1e-3, steps, G=1.0, eps2=1e-4)
         out = sh.download()
@@ -99,8 +127,8 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _run(world, tmp_path, n, scheme, steps):
-    mp.start_processes(_worker, args=(world, _free_port(), str(tmp_path), n, scheme, steps),
+def _run(world, tmp_path, n, scheme, steps, method="range"):
+    mp.start_processes(_worker, args=(world, _free_port(), str(tmp_path), n, scheme, steps, method),
                        nprocs=world, join=True, start_method="spawn")
     return [dict(np.load(tmp_path / f"w{world}_r{r}.npz")) for r in range(world)]
 
@@ -155,3 +183,33 @@ def test_ranks_without_receivers_still_exchange(tmp_path):
     for o in outs:
         for k in ("x", "vx", "vz"):
             np.testing.assert_array_equal(o[k], one[k])
+
+
+@pytest.mark.parametrize("scheme", [0, 2], ids=["kdk", "euler"])
+def test_newton3_partition_matches_single_rank_and_oracle(tmp_path, oracle, scheme):
+    """Newton-3 across ranks: 8 slices spread over 1, 2, 3 or 4 ranks, the
+    partials exchanged by an all-to-all and added in slice order.  Every world
+    size gives the single rank's bits, which follow the oracle's trajectory."""
+    n, steps = 1000, 3
+    one = _run(1, tmp_path, n, scheme, steps, "newton3")[0]
+    s0 = _system(n, 11)
+    ref = oracle.kdk(s0, 1e-3, steps, 1.0, 1e-4) if scheme == 0 else oracle.euler(s0, 1e-3, steps, 1.0, 1e-4)
+    for k in ("x", "y", "z", "vx", "vy", "vz"):
+        np.testing.assert_allclose(one[k], ref[k], rtol=1e-12, atol=1e-14)
+    for world in (2, 3, 4):
+        outs = _run(world, tmp_path, n, scheme, steps, "newton3")
+        assert sum(int(o["owned"]) for o in outs) == n
+        for o in outs:
+            # per evaluation: the slice all-to-all and the position all-gather
+            assert int(o["collectives"]) == 2 * int(o["evals"]) + 1
+            for k in ("x", "y", "z", "vx", "vy", "vz"):
+                np.testing.assert_array_equal(o[k], one[k])
+
+
+def test_slice_range_covers_the_slices():
+    for V in (1, 5, 8, 16):
+        for W in range(1, V + 1):
+            got = [nbr_shard.slice_range(V, W, r) for r in range(W)]
+            assert got[0][0] == 0 and got[-1][1] == V
+            assert all(a[1] == b[0] for a, b in zip(got, got[1:]))
+            assert all(v1 > v0 for v0, v1 in got)
