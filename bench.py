@@ -645,10 +645,12 @@ def measure_config_accuracy(ctx):
 
 
 def run_sharded(a, rank, world, local):
-    """--gpus N under torchrun: the one system split by receivers over the N
-    GPUs (nbr_shard.ShardedSystem: owned slice against all sources, then an
-    NCCL all-gather of positions per step, as hybrid_full_solver does with
-    MPI_Allgather).  Strong scaling: N(N-1) pairs per step in total."""
+    """--gpus N under torchrun: the one system over the N GPUs with Newton-3
+    across them (nbr_shard.ShardedSystem, method "newton3": each GPU computes
+    its slices of the pair triangle for every particle, an NCCL all-to-all
+    hands each GPU the partial forces of its own receivers, added in slice
+    order, then an NCCL all-gather of positions per step).  Strong scaling:
+    N(N-1) pairs per step in total."""
     import datetime
     import numpy as np
     import torch
@@ -671,7 +673,7 @@ def run_sharded(a, rank, world, local):
         pairs = float(n) * float(n - 1)
         s = nbr.plummer(n, a.seed)
         ctx = nbr.Context(local)
-        sh = ShardedSystem(ctx)
+        sh = ShardedSystem(ctx, method="newton3", slices=max(8, world))
         sh.upload(s)
         ext = torch.cuda.ExternalStream(ctx.stream)
         flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")
@@ -697,14 +699,11 @@ def run_sharded(a, rank, world, local):
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             return float(t.item())
 
-        # kernel-only: the owned slice's evaluation with kick = drift = 0
-        # (state unchanged), then an exchange to refill the other slices
-        k_s = []
-        for _ in range(3):
-            if sh.owned:
-                k_s.append(timed(lambda: ctx.step_range(prec, nbr.KDK, sh.i0, sh.owned, 0.0, 0.0,
-                                                        1.0, eps2)))
-            sh.exchange_positions()
+        # kernel-only: this GPU's Newton-3 slices (state unchanged)
+        def my_slices():
+            for v in range(sh.v0, sh.v1):
+                ctx.n3_slice_accel(prec, eps2, v, sh.slices, sh._mine[v - sh.v0])
+        k_s = [timed(my_slices) for _ in range(3)]
         for _ in range(a.warmup):
             step()
         ctx.synchronize()
@@ -740,17 +739,20 @@ def run_sharded(a, rank, world, local):
         k_max = max_over_ranks(k_t)
         if rank == 0:
             mhz = (clk or {}).get("sm_mhz") or 1965.0
-            peak = world * SMS * 128 * mhz * 1e6 / FMA_OPS_PER_PAIR / 1e9
+            ops = (FMA_OPS_PER_PAIR + REACTION_OPS) / 2  # Newton-3: per ordered pair
+            peak = world * SMS * 128 * mhz * 1e6 / ops / 1e9
             achieved = pairs / k_max / 1e9 if k_max > 0 else None
             line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
                     "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * t_total / a.steps,
                     "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
                     "dtype": "f32" if prec == nbr.FP32C else "f64", "data": "synthetic",
                     "config": workload_config(a, {"precision": a.precision,
-                                                  "parallelism": f"i-partition x{world}, NCCL "
-                                                                 "all-gather of positions per step",
+                                                  "parallelism": f"Newton-3 slices x{world} GPUs "
+                                                                 f"({sh.slices} slices), NCCL all-to-all "
+                                                                 "of partial forces + all-gather of "
+                                                                 "positions per step",
                                                   "shard": sh.count}),
-                    "gpu_launches": 2 * a.steps,
+                    "gpu_launches": a.steps * (2 * (sh.v1 - sh.v0) + 1),
                     "e2e": {"value": a.steps * pairs / e2e_total / 1e9, "unit": UNIT,
                             "h2d_bytes_per_step": 7 * 8 * n, "d2h_bytes_per_step": 3 * 8 * n,
                             "scheme": "kdk, whole state uploaded and positions downloaded per step"},
@@ -758,9 +760,11 @@ def run_sharded(a, rank, world, local):
                                  "unit": UNIT, "frac": achieved / peak if achieved else None,
                                  "traffic": None,
                                  "peak_source": f"{world} GPUs x {SMS} SMs x 128 FP32 lanes x rank-0 "
-                                                "median SM clock / 16 FMA-pipe ops per pair",
+                                                f"median SM clock / {ops:g} FMA-pipe ops per ordered "
+                                                "pair (Newton-3)",
                                  "kernel_ms_max_over_ranks": 1e3 * k_max},
-                    "clocks": clk, "cpu_baseline": None, "collectives_per_step": 1}
+                    "clocks": clk, "cpu_baseline": None,
+                    "collectives_per_step": "1 all-to-all + 3 in-place all-gathers"}
             print(json.dumps(line))
         ctx.synchronize()
         ctx.close()

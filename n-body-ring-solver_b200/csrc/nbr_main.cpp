@@ -9,7 +9,12 @@
 //   -t gpu-bench     the scaling benchmark's CSV row (CPU/hybrid_solver.cpp:623-645);
 //   -t gpu-accuracy  omp_accuracy (CPU/omp_solver.cpp:899-993);
 //   -t gpu-ratio     omp_ratio_accuracy (CPU/omp_solver.cpp:995-1243);
-//   -t gpu-batch     many independent systems in one persistent launch.
+//   -t gpu-batch     many independent systems in one persistent launch;
+//   -t gpu-multi     one system over -ngpu GPUs from this one process: the
+//                    Newton-3 slices of each GPU, an NCCL all-to-all of the
+//                    partial forces and an NCCL all-gather of the positions
+//                    per force evaluation (hybrid_ring_solver's partition of
+//                    the pair work, CPU/hybrid_solver.cpp:14-224, on NVLink).
 // Added flags: -eps (softening length), -dt (overrides T/s), -ic
 // ring|plummer|ball|twocomp|random, -seed, -scheme dkd|kdk, -G, -nsys, -nmin,
 // -nmax, -autotune, -save K (a record of the reference's snapshot format,
@@ -30,6 +35,9 @@
 #include <random>
 #include <string>
 #include <vector>
+
+#include <cuda_runtime.h>
+#include <nccl.h>
 
 #include "nbr.h"
 
@@ -59,6 +67,9 @@ struct Args {
   int device = 0;
   size_t save_every = 0;  // -save K: snapshot every K steps (NBody_<N>.dat)
   std::string resume;     // -resume PATH: start from the file's last record
+  int ngpu = 1;           // -ngpu W: GPUs of -t gpu-multi
+  int slices = 0;         // -slices V: Newton-3 slices (0: max(8, W))
+  std::string final_snapshot;  // -final PATH: the end state as one snapshot record
 };
 
 bool parse(int argc, char** argv, Args& a) {
@@ -81,7 +92,8 @@ bool parse(int argc, char** argv, Args& a) {
     else if (is("-o")) { a.output = argv[++i]; a.output_given = true; }
     else if (is("-t")) {
       std::string t = argv[++i];
-      static const char* known[] = {"gpu", "gpu-bench", "gpu-accuracy", "gpu-ratio", "gpu-batch"};
+      static const char* known[] = {"gpu", "gpu-bench", "gpu-accuracy", "gpu-ratio", "gpu-batch",
+                                    "gpu-multi"};
       bool ok = false;
       for (auto k : known) ok |= (t == k);
       if (!ok) {
@@ -116,6 +128,9 @@ bool parse(int argc, char** argv, Args& a) {
     else if (is("-device")) a.device = std::atoi(argv[++i]);
     else if (is("-save")) a.save_every = std::strtoull(argv[++i], nullptr, 10);
     else if (is("-resume")) a.resume = argv[++i];
+    else if (is("-ngpu")) a.ngpu = std::atoi(argv[++i]);
+    else if (is("-slices")) a.slices = std::atoi(argv[++i]);
+    else if (is("-final")) a.final_snapshot = argv[++i];
   }
   // Validation and resets of CPU/main.cpp:271-288.
   if (a.N >= 100000000 || a.start_N >= 100000000 ||
@@ -461,11 +476,218 @@ int run_batch(nbr_ctx* ctx, const Args& a) {
   return 0;
 }
 
+// ------------------------------------------------------------ multi-GPU ----
+// One process drives W GPUs (one libnbr context each, one NCCL communicator
+// per GPU from ncclCommInitAll).  Rank r owns the receivers [r c, (r + 1) c),
+// c = n / W rounded up to 128, and computes Newton-3 slices [r V / W,
+// (r + 1) V / W) for every particle; per force evaluation:
+//   1. nbr_n3_slice_accel for its slices (on its context's stream);
+//   2. one NCCL group of point-to-point transfers: the columns of every
+//      rank's receivers of each of its slices go to that rank (its own by a
+//      device copy); rank r receives slice v's columns into recv[v];
+//   3. nbr_step_range_sum: its receivers' V partials added in slice order,
+//      then the fused kick/drift;
+//   4. an in-place NCCL all-gather of x, y, z (MPI_Allgather of
+//      hybrid_full_solver, CPU/hybrid_solver.cpp:310).
+// The sum order depends on V only: any W <= V gives the same bits.
+struct MultiRank {
+  int dev = 0;
+  nbr_ctx* ctx = nullptr;
+  ncclComm_t comm = nullptr;
+  cudaStream_t st = nullptr;
+  size_t i0 = 0, owned = 0;
+  int v0 = 0, v1 = 0;
+  double* mine = nullptr;  // [v1 - v0][3][ld]
+  double* recv = nullptr;  // [V][3][c]
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+};
+
+int multi_fail(const char* what, const char* msg) {
+  std::printf("gpu-multi: %s: %s\n", what, msg);
+  return 1;
+}
+
+int run_multi(const Args& a) {
+  const int W = a.ngpu;
+  if (W < 1 || W > nbr_device_count())
+    return multi_fail("-ngpu", "needs 1 <= W <= the number of visible GPUs");
+  const int V = a.slices > 0 ? a.slices : std::max(8, W);
+  if (V < W) return multi_fail("-slices", "needs at least one slice per GPU");
+  const int scheme = a.integ == "lf" ? NBR_KDK : NBR_EULER;
+  State s;
+  if (make_ic(a, a.N, a.ratio, s) != NBR_OK) return 1;
+  const size_t n = a.N;
+  const size_t c = ((n + W - 1) / W + 127) / 128 * 128;
+  const size_t n_pad = (n + 1023) / 1024 * 1024;
+  const size_t ld = std::max(n_pad, (size_t)W * c);
+  const double dt = a.dt > 0.0 ? a.dt : a.T / double(a.time_steps);
+  const double eps2 = a.eps * a.eps;
+  std::vector<MultiRank> R(W);
+  std::vector<ncclComm_t> comms(W);
+  std::vector<int> devs(W);
+  for (int r = 0; r < W; ++r) devs[r] = r;
+  if (ncclCommInitAll(comms.data(), W, devs.data()) != ncclSuccess)
+    return multi_fail("ncclCommInitAll", "failed");
+  int rc = 0;
+  for (int r = 0; r < W && rc == 0; ++r) {
+    MultiRank& k = R[r];
+    k.dev = r;
+    k.comm = comms[r];
+    if (nbr_ctx_create(r, &k.ctx) != NBR_OK) {
+      rc = multi_fail("context", nbr_last_error_string(nullptr));
+      break;
+    }
+    k.st = static_cast<cudaStream_t>(nbr_ctx_stream(k.ctx));
+    if (nbr_system_upload(k.ctx, n, s.x.data(), s.y.data(), s.z.data(), s.vx.data(), s.vy.data(),
+                          s.vz.data(), s.m.data()) != NBR_OK) {
+      rc = multi_fail("upload", nbr_last_error_string(k.ctx));
+      break;
+    }
+    size_t len = 0;
+    nbr_state_pointers(k.ctx, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, &len);
+    if ((size_t)W * c > len) {
+      rc = multi_fail("-ngpu", "the shards of the in-place all-gather exceed the state arrays");
+      break;
+    }
+    k.i0 = (size_t)r * c;
+    k.owned = k.i0 < n ? std::min(c, n - k.i0) : 0;
+    k.v0 = r * V / W;
+    k.v1 = (r + 1) * V / W;
+    cudaSetDevice(r);
+    const size_t bm = (size_t)(k.v1 - k.v0) * 3 * ld * sizeof(double);
+    const size_t br = (size_t)V * 3 * c * sizeof(double);
+    if (cudaMalloc((void**)&k.mine, bm) != cudaSuccess || cudaMalloc((void**)&k.recv, br) != cudaSuccess ||
+        cudaMemset(k.mine, 0, bm) != cudaSuccess || cudaMemset(k.recv, 0, br) != cudaSuccess ||
+        cudaEventCreate(&k.e0) != cudaSuccess || cudaEventCreate(&k.e1) != cudaSuccess ||
+        cudaDeviceSynchronize() != cudaSuccess)
+      rc = multi_fail("buffers", "device allocation failed");
+  }
+  auto nccl_ok = [&](ncclResult_t e, const char* what) {
+    if (e != ncclSuccess && rc == 0) rc = multi_fail(what, ncclGetErrorString(e));
+    return e == ncclSuccess;
+  };
+  auto evaluate = [&](double kick, double drift) {
+    for (int r = 0; r < W && rc == 0; ++r)
+      for (int v = R[r].v0; v < R[r].v1; ++v)
+        if (nbr_n3_slice_accel(R[r].ctx, a.precision, eps2, v, V,
+                               R[r].mine + (size_t)(v - R[r].v0) * 3 * ld, ld) != NBR_OK)
+          rc = multi_fail("slice", nbr_last_error_string(R[r].ctx));
+    if (rc) return;
+    nccl_ok(ncclGroupStart(), "group");
+    for (int r = 0; r < W; ++r) {
+      MultiRank& k = R[r];
+      cudaSetDevice(k.dev);
+      for (int q = 0; q < W; ++q) {
+        for (int v = k.v0; v < k.v1; ++v)
+          for (int d = 0; d < 3; ++d) {
+            const double* src = k.mine + ((size_t)(v - k.v0) * 3 + d) * ld + (size_t)q * c;
+            if (q == r)
+              cudaMemcpyAsync(k.recv + ((size_t)v * 3 + d) * c, src, c * sizeof(double),
+                              cudaMemcpyDeviceToDevice, k.st);
+            else
+              nccl_ok(ncclSend(src, c, ncclDouble, q, k.comm, k.st), "send");
+          }
+        if (q == r) continue;
+        for (int v = R[q].v0; v < R[q].v1; ++v)
+          for (int d = 0; d < 3; ++d)
+            nccl_ok(ncclRecv(k.recv + ((size_t)v * 3 + d) * c, c, ncclDouble, q, k.comm, k.st), "recv");
+      }
+    }
+    nccl_ok(ncclGroupEnd(), "group");
+    for (int r = 0; r < W && rc == 0; ++r)
+      if (R[r].owned &&
+          nbr_step_range_sum(R[r].ctx, a.precision, scheme, R[r].i0, R[r].owned, kick, drift, a.G,
+                             R[r].recv, V, 3 * c, c) != NBR_OK)
+        rc = multi_fail("update", nbr_last_error_string(R[r].ctx));
+    if (rc) return;
+    std::vector<double*> px(W), py(W), pz(W);
+    for (int r = 0; r < W; ++r)
+      nbr_state_pointers(R[r].ctx, &px[r], &py[r], &pz[r], nullptr, nullptr, nullptr, nullptr);
+    nccl_ok(ncclGroupStart(), "group");
+    for (int r = 0; r < W; ++r)
+      for (double* p : {px[r], py[r], pz[r]})
+        nccl_ok(ncclAllGather(p + R[r].i0, p, c, ncclDouble, R[r].comm, R[r].st), "all-gather");
+    nccl_ok(ncclGroupEnd(), "group");
+    for (int r = 0; r < W; ++r) nbr_state_changed(R[r].ctx);
+  };
+  std::vector<std::pair<double, double>> sched;
+  if (scheme == NBR_KDK) {
+    sched.push_back({0.5 * dt, dt});
+    for (size_t t = 1; t < a.time_steps; ++t) sched.push_back({dt, dt});
+    sched.push_back({0.5 * dt, 0.0});
+  } else {
+    for (size_t t = 0; t < a.time_steps; ++t) sched.push_back({dt, dt});
+  }
+  for (int r = 0; r < W && rc == 0; ++r) cudaEventRecord(R[r].e0, R[r].st);
+  for (auto& kd : sched) {
+    if (rc) break;
+    evaluate(kd.first, kd.second);
+  }
+  float ms_max = 0.f;
+  for (int r = 0; r < W && rc == 0; ++r) {
+    cudaEventRecord(R[r].e1, R[r].st);
+    if (nbr_ctx_synchronize(R[r].ctx) != NBR_OK) {
+      rc = multi_fail("run", nbr_last_error_string(R[r].ctx));
+      break;
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, R[r].e0, R[r].e1);
+    ms_max = std::max(ms_max, ms);
+  }
+  if (rc == 0) {
+    // velocities of every rank's receivers to every rank, then the state out of rank 0
+    std::vector<double*> vx(W), vy(W), vz(W);
+    for (int r = 0; r < W; ++r)
+      nbr_state_pointers(R[r].ctx, nullptr, nullptr, nullptr, &vx[r], &vy[r], &vz[r], nullptr);
+    nccl_ok(ncclGroupStart(), "group");
+    for (int r = 0; r < W; ++r)
+      for (double* p : {vx[r], vy[r], vz[r]})
+        nccl_ok(ncclAllGather(p + R[r].i0, p, c, ncclDouble, R[r].comm, R[r].st), "all-gather");
+    nccl_ok(ncclGroupEnd(), "group");
+    for (int r = 0; r < W; ++r) nbr_ctx_synchronize(R[r].ctx);
+  }
+  if (rc == 0) {
+    const double secs = ms_max * 1e-3;
+    const double pairs = double(sched.size()) * double(n) * double(n - 1);
+    std::printf("GPUs = %d, slices = %d, N = %zu, evaluations = %zu\n", W, V, n, sched.size());
+    std::printf("GPU multi solver took %fs (max over GPUs): %.3f GPairs/s\n", secs, pairs / secs * 1e-9);
+    if (!a.final_snapshot.empty() &&
+        nbr_snapshot_save(R[0].ctx, a.final_snapshot.c_str(), a.time_steps, dt) != NBR_OK)
+      rc = multi_fail("snapshot", nbr_last_error_string(R[0].ctx));
+    if (a.output_given && rc == 0) {
+      const bool exists = file_exists(a.output);
+      FILE* f = std::fopen(a.output.c_str(), exists ? "a" : "w");
+      if (f) {
+        if (!exists)
+          std::fprintf(f, "#Nodes, Cores, N, t_total[s], performance[Mpairs/s], time_steps/s, ms/time_step\n");
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+        std::fprintf(f, "%d,%d,%zu,%f,%f,%f,%f\n", W, W * sms, n, secs, pairs / secs * 1e-6,
+                     double(a.time_steps) / secs, secs * 1000.0 / double(a.time_steps));
+        std::fclose(f);
+      }
+    }
+  }
+  for (auto& k : R) {
+    if (k.ctx) nbr_ctx_synchronize(k.ctx);
+    cudaSetDevice(k.dev);
+    if (k.mine) cudaFree(k.mine);
+    if (k.recv) cudaFree(k.recv);
+    if (k.e0) cudaEventDestroy(k.e0);
+    if (k.e1) cudaEventDestroy(k.e1);
+    if (k.ctx) nbr_ctx_destroy(k.ctx);
+  }
+  for (auto cm : comms)
+    if (cm) ncclCommDestroy(cm);
+  return rc;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
   Args a;
   parse(argc, argv, a);
+  if (a.exec == "gpu-multi") return run_multi(a);
   nbr_ctx* ctx = nullptr;
   if (nbr_ctx_create(a.device, &ctx) != NBR_OK) {
     std::printf("No GPU context: %s\n", nbr_last_error_string(nullptr));

@@ -68,3 +68,23 @@ def test_cli_batch(tmp_path):
     out = run(["-t", "gpu-batch", "-nsys", "64", "-nmin", "64", "-nmax", "512", "-s", "5", "-dt", "1e-3",
                "-eps", "1e-3", "-p", "sp"], tmp_path)
     assert "systems*steps/s" in out
+
+
+@pytest.mark.parametrize("prec,tol", [("dp", 1e-11), ("sp", 1e-6)])
+def test_cli_multi_gpu_newton3(tmp_path, nbr, oracle, prec, tol):
+    """-t gpu-multi: the C++ multi-GPU host (NCCL communicator per GPU,
+    Newton-3 slices, all-to-all of partial forces, all-gather of positions) on
+    the one GPU this runs on; the end state against the oracle's KDK run."""
+    final = tmp_path / "final.dat"
+    csv = tmp_path / "multi.csv"
+    out = run(["-t", "gpu-multi", "-ngpu", "1", "-slices", "5", "-N", "3000", "-ic", "plummer",
+               "-seed", "4", "-eps", "1e-3", "-i", "lf", "-scheme", "kdk", "-s", "3", "-dt", "1e-3",
+               "-p", prec, "-final", str(final), "-o", str(csv)], tmp_path)
+    assert "GPU multi solver" in out
+    got = nbr.snapshot_read(str(final), 3000, 0)
+    s = nbr.plummer(3000, 4)
+    want = oracle.kdk(s, 1e-3, 3, eps2=1e-6)
+    for k in ("x", "y", "z", "vx", "vy", "vz"):
+        assert np.abs(got[k] - want[k]).max() <= tol, k
+    lines = csv.read_text().strip().splitlines()
+    assert lines[0].startswith("#Nodes, Cores, N") and lines[1].startswith("1,")
