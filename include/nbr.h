@@ -289,9 +289,10 @@ int nbr_snapshot_load(nbr_ctx* ctx, const char* path, size_t n, size_t record, d
  * ni = 1: the small-N kernel with warps = 2, 4 or 8 lane groups per warp;
  * ni = 3, warps = 8: the Newton-3 kernel, each unordered pair evaluated once
  * and applied to both particles, for FP32C and for FP64; for FP32C also
- * warps = 16, two warps per 256-particle row block; whole systems of at most
- * 2^20 particles, other calls fall back to the large kernels; ni = 2, FP64
- * only, warps = 4, 8 or 16 lane groups: nbr_run of a system of at most 4096
+ * warps = 16, two warps per 256-particle row block; whole systems only,
+ * receiver ranges and separate receiver and source sets fall back to the large
+ * kernels; ni = 2, FP64 only, warps = 4, 8 or 16 lane groups per warp, split =
+ * 8 or 16 warps per CTA (0: 16): nbr_run of a system of at most 4096
  * particles as one cooperative launch for all steps (the default for such
  * systems), evaluations outside nbr_run use the default kernels).  ni = 0
  * restores the autotuner. */

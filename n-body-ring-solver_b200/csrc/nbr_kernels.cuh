@@ -195,8 +195,10 @@ cudaError_t configure_kernels();
 // loop of an FP64 system of at most kPersistMaxN particles in one cooperative
 // launch.  ForceConfig ni = kPersistNI with warps = lane groups (4, 8, 16)
 // forces it; it is the default for such systems.
+// ForceConfig split = warps per CTA of that launch (8 or 16; 0: default).
 constexpr int kPersistNI = 2;
 constexpr long long kPersistMaxN = 4096;
+constexpr int kPersistDefaultWarps = 16;
 
 // Receivers one CTA of a configuration covers.
 inline long long force_chunk(const ForceConfig& c) {

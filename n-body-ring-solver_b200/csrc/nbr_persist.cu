@@ -34,8 +34,6 @@ namespace nbr {
 
 namespace {
 
-constexpr int kPWarps = 8;
-constexpr int kPThreads = kPWarps * 32;
 constexpr int kPNI = 4;  // receivers per lane
 
 struct PersistArgs {
@@ -92,7 +90,6 @@ __device__ bool grid_barrier(unsigned* bar, int* err, unsigned long long limit_n
           ok = 0;
           break;
         }
-        __nanosleep(64);
       }
     }
     __threadfence();
@@ -103,8 +100,11 @@ __device__ bool grid_barrier(unsigned* bar, int* err, unsigned long long limit_n
   return s_ok != 0;
 }
 
-template <int F, bool EXCL>
-__global__ void __launch_bounds__(kPThreads, 1) k_run_small_f64(const PersistArgs A) {
+// W warps per CTA (8 or 16), F lane groups per warp.
+template <int F, int W, bool EXCL>
+__global__ void __launch_bounds__(W * 32, 1) k_run_small_f64(const PersistArgs A) {
+  constexpr int kPWarps = W;
+  constexpr int kPThreads = W * 32;
   constexpr int G = 32 / F;        // receiver columns per warp
   constexpr int RPC = G * kPNI;    // receivers per chunk
   constexpr int S = kPWarps * F;   // ways the sources are split
@@ -146,10 +146,22 @@ __global__ void __launch_bounds__(kPThreads, 1) k_run_small_f64(const PersistArg
     const double* X = A.px[cur];
     const double* Y = A.py[cur];
     const double* Z = A.pz[cur];
-    for (int j = threadIdx.x; j < n; j += kPThreads) {
-      sx[j] = __ldcg(X + j);
-      sy[j] = __ldcg(Y + j);
-      sz[j] = __ldcg(Z + j);
+    // 16-byte L2 loads, several in flight per thread before the stores (the
+    // arrays hold at least ns entries: n_pad is a multiple of 1024)
+    {
+      const double2* X2 = reinterpret_cast<const double2*>(X);
+      const double2* Y2 = reinterpret_cast<const double2*>(Y);
+      const double2* Z2 = reinterpret_cast<const double2*>(Z);
+      double2* sx2 = reinterpret_cast<double2*>(sx);
+      double2* sy2 = reinterpret_cast<double2*>(sy);
+      double2* sz2 = reinterpret_cast<double2*>(sz);
+#pragma unroll 4
+      for (int j = threadIdx.x; j < ns / 2; j += kPThreads) {
+        const double2 a = __ldcg(X2 + j), b = __ldcg(Y2 + j), c = __ldcg(Z2 + j);
+        sx2[j] = a;
+        sy2[j] = b;
+        sz2[j] = c;
+      }
     }
     __syncthreads();
     const double2 kd = A.sched[e];
@@ -232,18 +244,25 @@ __global__ void __launch_bounds__(kPThreads, 1) k_run_small_f64(const PersistArg
   }
 }
 
-const void* persist_fn(int F, bool excl) {
+template <int F>
+const void* persist_fn_f(int W, bool excl) {
+  if (W == 8) return excl ? (const void*)k_run_small_f64<F, 8, true> : (const void*)k_run_small_f64<F, 8, false>;
+  if (W == 16) return excl ? (const void*)k_run_small_f64<F, 16, true> : (const void*)k_run_small_f64<F, 16, false>;
+  return nullptr;
+}
+
+const void* persist_fn(int F, int W, bool excl) {
   switch (F) {
-    case 4: return excl ? (const void*)k_run_small_f64<4, true> : (const void*)k_run_small_f64<4, false>;
-    case 8: return excl ? (const void*)k_run_small_f64<8, true> : (const void*)k_run_small_f64<8, false>;
-    case 16: return excl ? (const void*)k_run_small_f64<16, true> : (const void*)k_run_small_f64<16, false>;
+    case 4: return persist_fn_f<4>(W, excl);
+    case 8: return persist_fn_f<8>(W, excl);
+    case 16: return persist_fn_f<16>(W, excl);
     default: return nullptr;
   }
 }
 
-size_t persist_smem(int n, int F) {
+size_t persist_smem(int n, int F, int W) {
   const int ns = (n + 1) & ~1;
-  return (size_t)4 * ns * sizeof(double) + (size_t)kPWarps * ((32 / F) * kPNI) * 3 * sizeof(double);
+  return (size_t)4 * ns * sizeof(double) + (size_t)W * ((32 / F) * kPNI) * 3 * sizeof(double);
 }
 
 // Lane groups per warp: the layout whose receiver chunks fill the SMs best
@@ -311,11 +330,18 @@ int run_persistent(nbr_ctx* c, int precision, int scheme, double dt, size_t step
   if (e != cudaSuccess) return cuda_fail(c, e, "persistent setup");
 
   const ForceConfig& o = c->override_cfg[kFP64];
-  const int F = (o.ni == kPersistNI) ? o.warps : persist_groups(n, c->sms);
+  int F = persist_groups(n, c->sms), W = kPersistDefaultWarps;
+  if (o.ni == kPersistNI) {
+    F = o.warps;
+    if (o.split > 1) W = o.split;
+  }
   const bool excl = eps2 == 0.0;
-  const void* fn = persist_fn(F, excl);
-  if (!fn) return fail(c, NBR_ERR_INVALID_ARG, "persistent run: lane groups must be 4, 8 or 16");
-  const size_t smem = persist_smem(n, F);
+  const void* fn = persist_fn(F, W, excl);
+  if (!fn)
+    return fail(c, NBR_ERR_INVALID_ARG,
+                "persistent run: lane groups must be 4, 8 or 16 and warps per CTA 8 or 16");
+  const int kPThreads = W * 32;
+  const size_t smem = persist_smem(n, F, W);
   e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int per_sm = 0;
   if (e == cudaSuccess)

@@ -39,10 +39,11 @@ def _maxdiff(a, b):
 
 @pytest.mark.parametrize("n", [2, 3, 127, 1000, 2048, 4096])
 @pytest.mark.parametrize("groups", [4, 8, 16])
-def test_persistent_matches_launch_per_step(ctx, nbr, n, groups):
+@pytest.mark.parametrize("warps", [8, 16])
+def test_persistent_matches_launch_per_step(ctx, nbr, n, groups, warps):
     s = nbr.plummer(n, 60 + n)
     for scheme, order, eps2 in ((KDK, 2, 1e-6), (DKD, 4, 1e-6), (EULER, 2, 1e-6), (KDK, 2, 0.0)):
-        got, st = _run(ctx, s, (PERSIST, groups, 0), scheme, order, 1e-3, 7, eps2, calls=2)
+        got, st = _run(ctx, s, (PERSIST, groups, warps), scheme, order, 1e-3, 7, eps2, calls=2)
         assert st["kernels"] == 1, st
         want, _ = _run(ctx, s, (1, 8, 0), scheme, order, 1e-3, 7, eps2, calls=2)
         assert _maxdiff(got, want) <= 1e-12, (scheme, order, eps2, _maxdiff(got, want))

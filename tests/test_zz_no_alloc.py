@@ -10,6 +10,7 @@ row, with different sizes, check that the shared scratch is cleared and
 reused correctly.  This file is collected last on purpose.
 """
 import ctypes as C
+import os
 
 import numpy as np
 import pytest
