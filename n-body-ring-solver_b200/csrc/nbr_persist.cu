@@ -16,7 +16,7 @@
 //    position buffer, and all CTAs meet at one grid barrier before the next
 //    evaluation reads it.
 //
-// The barrier is a counter plus a generation word; its wait is bounded by
+// The barrier is a 64-bit arrival counter that only grows; its wait is bounded by
 // %globaltimer (the context's wait limit) and gives up, with an error code
 // for the host, if the limit passes or another CTA has already recorded an
 // error.  The cooperative launch guarantees that all CTAs are resident, so no
@@ -53,39 +53,40 @@ struct PersistArgs {
   double* vx; double* vy; double* vz;
   double* ax; double* ay; double* az;
   const double* m;
-  unsigned* bar;           // [0] arrivals, [1] generation
+  unsigned long long* bar; // arrivals at grid barriers (only grows; zero at launch)
   int* err;
   unsigned long long wait_ns;
   int skip_barrier;        // test hook: CTA 0 leaves before this barrier (-1: off)
 };
 
-__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
-  unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
 }
-__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+
+__device__ __forceinline__ void red_release_add_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-// Grid-wide barrier with a bounded wait.  Returns false in every thread of the
-// CTA if the barrier did not complete within the limit or an error was
-// already recorded (the CTA then leaves the kernel).
-__device__ bool grid_barrier(unsigned* bar, int* err, unsigned long long limit_ns) {
+// Grid-wide barrier number `k` (0, 1, ...) of the launch, with a bounded
+// wait.  The arrival counter only grows (zeroed by the host before the
+// launch): barrier k is complete when it reaches (k + 1) x gridDim.x, so an
+// arrival is one release add and nothing is reset.  Returns false in every
+// thread of the CTA if the barrier did not complete within the limit or an
+// error was already recorded (the CTA then leaves the kernel).
+__device__ bool grid_barrier(unsigned long long* bar, int* err, unsigned long long limit_ns,
+                             unsigned long long k) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
-    const unsigned gen = ld_acquire_u32(bar + 1);
+    const unsigned long long target = (k + 1) * gridDim.x;
     __threadfence();
-    const unsigned arrived = atomicAdd(bar, 1u);
-    if (arrived == gridDim.x - 1) {
-      atomicExch(bar, 0u);
-      __threadfence();
-      st_release_u32(bar + 1, gen + 1);
-    } else {
+    red_release_add_u64(bar, 1ull);
+    if (ld_acquire_u64(bar) < target) {
       const unsigned long long t0 = global_ns();
-      while (ld_acquire_u32(bar + 1) == gen) {
+      while (ld_acquire_u64(bar) < target) {
         if (*reinterpret_cast<volatile int*>(err) != 0 || global_ns() - t0 > limit_ns) {
           ok = 0;
           break;
@@ -116,11 +117,14 @@ __global__ void __launch_bounds__(W * 32, 1) k_run_small_f64(const PersistArgs A
   double* sz = sy + ns;
   double* sm = sz + ns;
   double* red = sm + ns;  // [kPWarps][RPC][3]
+  // velocities of this CTA's receivers for the whole run: [round][RPC][3]
+  double* svel = red + (size_t)kPWarps * RPC * 3;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gl = lane % G, grp = lane / G;
 
   for (int j = threadIdx.x; j < n; j += kPThreads) sm[j] = A.m[j];
   int cur = A.cur0;
+  unsigned long long nbar = 0;  // grid barriers passed
 
   if (A.pre) {
     for (int c = blockIdx.x; c < A.chunks; c += gridDim.x) {
@@ -137,9 +141,19 @@ __global__ void __launch_bounds__(W * 32, 1) k_run_small_f64(const PersistArgs A
         A.pz[1 - cur][i] = __ldcg(A.pz[cur] + i) + A.pre_drift * uz;
       }
     }
-    if (!grid_barrier(A.bar, A.err, A.wait_ns)) return;
+    if (!grid_barrier(A.bar, A.err, A.wait_ns, nbar++)) return;
     cur ^= 1;
   }
+  // the CTA owns its receivers for the whole run: their velocities stay in
+  // shared memory until the end
+  for (int c = blockIdx.x, r = 0; c < A.chunks; c += gridDim.x, ++r)
+    for (int t = threadIdx.x; t < RPC; t += kPThreads) {
+      const int i = c * RPC + t;
+      double* v = svel + ((size_t)r * RPC + t) * 3;
+      v[0] = i < n ? A.vx[i] : 0.0;
+      v[1] = i < n ? A.vy[i] : 0.0;
+      v[2] = i < n ? A.vz[i] : 0.0;
+    }
 
   for (int e = 0; e < A.evals; ++e) {
     // all positions of this evaluation, from L2 (other CTAs wrote them)
@@ -165,7 +179,7 @@ __global__ void __launch_bounds__(W * 32, 1) k_run_small_f64(const PersistArgs A
     }
     __syncthreads();
     const double2 kd = A.sched[e];
-    for (int c = blockIdx.x; c < A.chunks; c += gridDim.x) {
+    for (int c = blockIdx.x, round = 0; c < A.chunks; c += gridDim.x, ++round) {
       const int base = c * RPC;
       double xi[kPNI], yi[kPNI], zi[kPNI], ax[kPNI], ay[kPNI], az[kPNI];
 #pragma unroll
@@ -225,9 +239,10 @@ __global__ void __launch_bounds__(W * 32, 1) k_run_small_f64(const PersistArgs A
           // (Euler: drift with the old velocity)
           const double gx = A.G * a0, gy = A.G * a1, gz = A.G * a2;
           A.ax[i] = gx; A.ay[i] = gy; A.az[i] = gz;
-          const double ux = A.vx[i], uy = A.vy[i], uz = A.vz[i];
+          double* v = svel + ((size_t)round * RPC + t) * 3;
+          const double ux = v[0], uy = v[1], uz = v[2];
           const double vx = ux + kd.x * gx, vy = uy + kd.x * gy, vz = uz + kd.x * gz;
-          A.vx[i] = vx; A.vy[i] = vy; A.vz[i] = vz;
+          v[0] = vx; v[1] = vy; v[2] = vz;
           const bool euler = A.mode == 2;
           A.px[1 - cur][i] = sx[i] + kd.y * (euler ? ux : vx);
           A.py[1 - cur][i] = sy[i] + kd.y * (euler ? uy : vy);
@@ -238,10 +253,17 @@ __global__ void __launch_bounds__(W * 32, 1) k_run_small_f64(const PersistArgs A
     }
     if (e + 1 < A.evals) {
       if (e == A.skip_barrier && blockIdx.x == 0) return;  // test hook: never arrives
-      if (!grid_barrier(A.bar, A.err, A.wait_ns)) return;
+      if (!grid_barrier(A.bar, A.err, A.wait_ns, nbar++)) return;
     }
     cur ^= 1;
   }
+  for (int c = blockIdx.x, r = 0; c < A.chunks; c += gridDim.x, ++r)
+    for (int t = threadIdx.x; t < RPC; t += kPThreads) {
+      const int i = c * RPC + t;
+      if (i >= n) continue;
+      const double* v = svel + ((size_t)r * RPC + t) * 3;
+      A.vx[i] = v[0]; A.vy[i] = v[1]; A.vz[i] = v[2];
+    }
 }
 
 template <int F>
@@ -260,9 +282,12 @@ const void* persist_fn(int F, int W, bool excl) {
   }
 }
 
-size_t persist_smem(int n, int F, int W) {
+// Shared memory of a launch: positions and masses, the warps' partial sums, and
+// the velocities of up to `rounds` receiver chunks per CTA.
+size_t persist_smem(int n, int F, int W, int rounds) {
   const int ns = (n + 1) & ~1;
-  return (size_t)4 * ns * sizeof(double) + (size_t)W * ((32 / F) * kPNI) * 3 * sizeof(double);
+  const size_t rpc = (size_t)(32 / F) * kPNI;
+  return (size_t)4 * ns * sizeof(double) + ((size_t)W + rounds) * rpc * 3 * sizeof(double);
 }
 
 // Lane groups per warp: the layout whose receiver chunks fill the SMs best
@@ -325,8 +350,9 @@ int run_persistent(nbr_ctx* c, int precision, int scheme, double dt, size_t step
   if (e != cudaSuccess) return cuda_fail(c, e, "persistent schedule");
   e = cudaMemcpyAsync(c->scr.red, sched.data(), sched.size() * sizeof(double2),
                       cudaMemcpyHostToDevice, c->stream);
-  unsigned* bar = reinterpret_cast<unsigned*>(c->d_err + 2);
-  if (e == cudaSuccess) e = cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), c->stream);
+  // the arrival counter: the context's error block words 2-3 (8-byte aligned)
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(c->d_err + 2);
+  if (e == cudaSuccess) e = cudaMemsetAsync(bar, 0, sizeof(unsigned long long), c->stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "persistent setup");
 
   const ForceConfig& o = c->override_cfg[kFP64];
@@ -341,16 +367,19 @@ int run_persistent(nbr_ctx* c, int precision, int scheme, double dt, size_t step
     return fail(c, NBR_ERR_INVALID_ARG,
                 "persistent run: lane groups must be 4, 8 or 16 and warps per CTA 8 or 16");
   const int kPThreads = W * 32;
-  const size_t smem = persist_smem(n, F, W);
+  const int rpc = (32 / F) * kPNI;
+  const int chunks = (n + rpc - 1) / rpc;
+  // the grid is at least min(chunks, SMs) CTAs, so no CTA gets more rounds than this
+  const int rounds = (chunks + std::min(chunks, c->sms) - 1) / std::min(chunks, c->sms);
+  const size_t smem = persist_smem(n, F, W, rounds);
   e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int per_sm = 0;
   if (e == cudaSuccess)
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kPThreads, smem);
   if (e != cudaSuccess) return cuda_fail(c, e, "persistent kernel setup");
   if (per_sm < 1) return fail(c, NBR_ERR_UNSUPPORTED, "persistent kernel does not fit an SM");
-  const int rpc = (32 / F) * kPNI;
   A.n = n;
-  A.chunks = (n + rpc - 1) / rpc;
+  A.chunks = chunks;
   A.evals = E;
   A.sched = reinterpret_cast<const double2*>(c->scr.red);
   A.G = G;
