@@ -535,9 +535,13 @@ def measure_config0(ctx, l2_flush, mhz, n=2048, steps=100):
         t = min(times)
         cfg = ctx.get_force_config(prec, eps2)
         gp = r["pairs"] / t / 1e9
+        persistent = r["kernels"] == 1
         out[name] = {"steps_per_s": steps / t, "ms_per_step": 1e3 * t / steps, "gpairs": gp,
                      "force_evals": r["force_evals"], "kernels_per_run": r["kernels"],
-                     "config": list(cfg), "runs_timed": len(times), "time": "best of 3 graph launches"}
+                     "path": ("k_run_small_f64: all steps in one cooperative launch" if persistent
+                              else f"one graph of per-step launches, force config {list(cfg)}"),
+                     "runs_timed": len(times),
+                     "time": "best of 3 runs (events around the launch)"}
     out["fp64"]["frac_of_fp64_16op_roofline"] = out["fp64"]["gpairs"] / fp64_peak(mhz)
     out["fp32c"]["frac_of_fp32_16op_roofline"] = out["fp32c"]["gpairs"] / (
         SMS * 128 * mhz * 1e6 / FMA_OPS_PER_PAIR / 1e9)

@@ -6,7 +6,8 @@
 // the schedules of reduced_solver_omp_lf / reduced_solver_omp,
 // CPU/omp_solver.cpp:16-178, 257-456) inside ONE cooperative launch:
 //
-//  * each CTA owns fixed receiver chunks of RPC particles for the whole run;
+//  * each CTA owns fixed receiver chunks (about n / SMs particles, at most RPC
+//    lane slots) for the whole run;
 //  * per force evaluation every CTA stages all N positions (masses once) in
 //    shared memory with L2 loads, its 8 warps split the sources 8 ways and the
 //    F lane groups of each warp split them again (k_force_small's layout), and
@@ -38,7 +39,8 @@ constexpr int kPNI = 4;  // receivers per lane
 
 struct PersistArgs {
   int n;                   // particles (<= kPersistMaxN)
-  int chunks;              // receiver chunks of RPC particles
+  int chunks;              // receiver chunks of cs particles
+  int cs;                  // receivers per chunk (<= RPC slots of the lane layout)
   int evals;               // force evaluations
   const double2* sched;    // (kick, drift) of every evaluation
   int mode;                // 1: leapfrog (drift with the kicked velocity); 2: Euler
@@ -128,8 +130,8 @@ __global__ void __launch_bounds__(W * 32, 1) k_run_small_f64(const PersistArgs A
 
   if (A.pre) {
     for (int c = blockIdx.x; c < A.chunks; c += gridDim.x) {
-      for (int t = threadIdx.x; t < RPC; t += kPThreads) {
-        const int i = c * RPC + t;
+      for (int t = threadIdx.x; t < A.cs; t += kPThreads) {
+        const int i = c * A.cs + t;
         if (i >= n) continue;
         double ux = A.vx[i], uy = A.vy[i], uz = A.vz[i];
         if (A.pre_use_acc) {
@@ -148,11 +150,12 @@ __global__ void __launch_bounds__(W * 32, 1) k_run_small_f64(const PersistArgs A
   // shared memory until the end
   for (int c = blockIdx.x, r = 0; c < A.chunks; c += gridDim.x, ++r)
     for (int t = threadIdx.x; t < RPC; t += kPThreads) {
-      const int i = c * RPC + t;
+      const int i = c * A.cs + t;
+      const bool own = t < A.cs && i < n;
       double* v = svel + ((size_t)r * RPC + t) * 3;
-      v[0] = i < n ? A.vx[i] : 0.0;
-      v[1] = i < n ? A.vy[i] : 0.0;
-      v[2] = i < n ? A.vz[i] : 0.0;
+      v[0] = own ? A.vx[i] : 0.0;
+      v[1] = own ? A.vy[i] : 0.0;
+      v[2] = own ? A.vz[i] : 0.0;
     }
 
   for (int e = 0; e < A.evals; ++e) {
@@ -180,12 +183,12 @@ __global__ void __launch_bounds__(W * 32, 1) k_run_small_f64(const PersistArgs A
     __syncthreads();
     const double2 kd = A.sched[e];
     for (int c = blockIdx.x, round = 0; c < A.chunks; c += gridDim.x, ++round) {
-      const int base = c * RPC;
+      const int base = c * A.cs;
       double xi[kPNI], yi[kPNI], zi[kPNI], ax[kPNI], ay[kPNI], az[kPNI];
 #pragma unroll
       for (int k = 0; k < kPNI; ++k) {
-        const int i = base + gl + G * k;
-        const bool real = i < n;
+        const int slot = gl + G * k, i = base + slot;
+        const bool real = slot < A.cs && i < n;
         xi[k] = real ? sx[i] : 0.0;
         yi[k] = real ? sy[i] : 0.0;
         zi[k] = real ? sz[i] : 0.0;
@@ -234,7 +237,7 @@ __global__ void __launch_bounds__(W * 32, 1) k_run_small_f64(const PersistArgs A
           const double* r = red + ((size_t)w * RPC + t) * 3;
           a0 += r[0]; a1 += r[1]; a2 += r[2];
         }
-        if (i < n) {
+        if (t < A.cs && i < n) {
           // the epilogue of the large kernels: a -> acc, v += kick a, x' = x + drift v
           // (Euler: drift with the old velocity)
           const double gx = A.G * a0, gy = A.G * a1, gz = A.G * a2;
@@ -258,8 +261,8 @@ __global__ void __launch_bounds__(W * 32, 1) k_run_small_f64(const PersistArgs A
     cur ^= 1;
   }
   for (int c = blockIdx.x, r = 0; c < A.chunks; c += gridDim.x, ++r)
-    for (int t = threadIdx.x; t < RPC; t += kPThreads) {
-      const int i = c * RPC + t;
+    for (int t = threadIdx.x; t < A.cs; t += kPThreads) {
+      const int i = c * A.cs + t;
       if (i >= n) continue;
       const double* v = svel + ((size_t)r * RPC + t) * 3;
       A.vx[i] = v[0]; A.vy[i] = v[1]; A.vz[i] = v[2];
@@ -290,22 +293,14 @@ size_t persist_smem(int n, int F, int W, int rounds) {
   return (size_t)4 * ns * sizeof(double) + ((size_t)W + rounds) * rpc * 3 * sizeof(double);
 }
 
-// Lane groups per warp: the layout whose receiver chunks fill the SMs best
-// (chunks / (rounds x SMs)), fewer chunks on a tie.
+// Lane groups per warp: the most (the finest split of the sources) whose
+// chunk of (32 / F) x 4 receiver slots still holds n / SMs receivers, so that
+// one round of chunks covers the system.
 int persist_groups(int n, int sms) {
-  int best = 8;
-  double best_eff = -1.0;
-  for (int F : {4, 8, 16}) {
-    const int rpc = (32 / F) * kPNI;
-    const int chunks = (n + rpc - 1) / rpc;
-    const int rounds = (chunks + sms - 1) / sms;
-    const double eff = double(chunks) / (double(rounds) * sms);
-    if (eff > best_eff + 1e-9) {
-      best_eff = eff;
-      best = F;
-    }
-  }
-  return best;
+  const int need = (n + sms - 1) / sms;
+  for (int F : {16, 8, 4})
+    if ((32 / F) * kPNI >= need) return F;
+  return 4;
 }
 
 }  // namespace
@@ -368,7 +363,9 @@ int run_persistent(nbr_ctx* c, int precision, int scheme, double dt, size_t step
                 "persistent run: lane groups must be 4, 8 or 16 and warps per CTA 8 or 16");
   const int kPThreads = W * 32;
   const int rpc = (32 / F) * kPNI;
-  const int chunks = (n + rpc - 1) / rpc;
+  // receivers per chunk: n / SMs (one chunk per SM) when the slots allow it
+  const int cs = std::max(1, std::min(rpc, (n + c->sms - 1) / c->sms));
+  const int chunks = (n + cs - 1) / cs;
   // the grid is at least min(chunks, SMs) CTAs, so no CTA gets more rounds than this
   const int rounds = (chunks + std::min(chunks, c->sms) - 1) / std::min(chunks, c->sms);
   const size_t smem = persist_smem(n, F, W, rounds);
@@ -380,6 +377,7 @@ int run_persistent(nbr_ctx* c, int precision, int scheme, double dt, size_t step
   if (per_sm < 1) return fail(c, NBR_ERR_UNSUPPORTED, "persistent kernel does not fit an SM");
   A.n = n;
   A.chunks = chunks;
+  A.cs = cs;
   A.evals = E;
   A.sched = reinterpret_cast<const double2*>(c->scr.red);
   A.G = G;
