@@ -302,7 +302,9 @@ int nbr_set_force_config(nbr_ctx* ctx, int precision, int ni, int warps, int spl
  * for a configuration forced with nbr_set_force_config (ni 4 or 8); 0 takes
  * the default (128; unroll 4 for FP32C, 2 for FP64).  Built for the default
  * large configurations FP32C (8, 2) and FP64 (4, 4); other (tile, unroll)
- * pairs return NBR_ERR_INVALID_ARG. */
+ * pairs return NBR_ERR_INVALID_ARG.  For the persistent small-system run (ni
+ * = 2) tile is its receivers per lane instead: 4 (the default) or 8, the
+ * latter with 8 or 16 lane groups. */
 int nbr_set_force_tiling(nbr_ctx* ctx, int precision, int tile, int unroll);
 /* The j-tile and unroll depth a force evaluation of the uploaded system would
  * use (0 and 0 when the chosen kernel is not a large one). */

@@ -1304,8 +1304,9 @@ int nbr_set_force_tiling(nbr_ctx* c, int precision, int tile, int unroll) {
   if (precision != NBR_FP64 && precision != NBR_FP32C)
     return fail(c, NBR_ERR_INVALID_ARG, "unknown precision");
   ForceConfig cfg = c->override_cfg[precision];
-  if (cfg.ni != 4 && cfg.ni != 8)
-    return fail(c, NBR_ERR_INVALID_ARG, "force a large-kernel configuration (ni 4 or 8) first");
+  if (cfg.ni != 4 && cfg.ni != 8 && cfg.ni != kPersistNI)
+    return fail(c, NBR_ERR_INVALID_ARG,
+                "force a large-kernel (ni 4 or 8) or persistent (ni 2) configuration first");
   cfg.tile = tile;
   cfg.unroll = unroll;
   ForceConfig probe = cfg;

@@ -35,7 +35,7 @@ namespace nbr {
 
 namespace {
 
-constexpr int kPNI = 4;  // receivers per lane
+constexpr int kPNIDefault = 4;  // receivers per lane
 
 struct PersistArgs {
   int n;                   // particles (<= kPersistMaxN)
@@ -103,8 +103,8 @@ __device__ bool grid_barrier(unsigned long long* bar, int* err, unsigned long lo
   return s_ok != 0;
 }
 
-// W warps per CTA (8 or 16), F lane groups per warp.
-template <int F, int W, bool EXCL>
+// W warps per CTA (8 or 16), F lane groups per warp, kPNI receivers per lane.
+template <int F, int W, int kPNI, bool EXCL>
 __global__ void __launch_bounds__(W * 32, 1) k_run_small_f64(const PersistArgs A) {
   constexpr int kPWarps = W;
   constexpr int kPThreads = W * 32;
@@ -269,27 +269,37 @@ __global__ void __launch_bounds__(W * 32, 1) k_run_small_f64(const PersistArgs A
     }
 }
 
-template <int F>
+template <int F, int NI>
 const void* persist_fn_f(int W, bool excl) {
-  if (W == 8) return excl ? (const void*)k_run_small_f64<F, 8, true> : (const void*)k_run_small_f64<F, 8, false>;
-  if (W == 16) return excl ? (const void*)k_run_small_f64<F, 16, true> : (const void*)k_run_small_f64<F, 16, false>;
+  if (W == 8) return excl ? (const void*)k_run_small_f64<F, 8, NI, true> : (const void*)k_run_small_f64<F, 8, NI, false>;
+  if (W == 16) return excl ? (const void*)k_run_small_f64<F, 16, NI, true> : (const void*)k_run_small_f64<F, 16, NI, false>;
   return nullptr;
 }
 
-const void* persist_fn(int F, int W, bool excl) {
-  switch (F) {
-    case 4: return persist_fn_f<4>(W, excl);
-    case 8: return persist_fn_f<8>(W, excl);
-    case 16: return persist_fn_f<16>(W, excl);
-    default: return nullptr;
+const void* persist_fn(int F, int W, int NI, bool excl) {
+  if (NI == 4) {
+    switch (F) {
+      case 4: return persist_fn_f<4, 4>(W, excl);
+      case 8: return persist_fn_f<8, 4>(W, excl);
+      case 16: return persist_fn_f<16, 4>(W, excl);
+      default: return nullptr;
+    }
   }
+  if (NI == 8) {
+    switch (F) {
+      case 8: return persist_fn_f<8, 8>(W, excl);
+      case 16: return persist_fn_f<16, 8>(W, excl);
+      default: return nullptr;
+    }
+  }
+  return nullptr;
 }
 
 // Shared memory of a launch: positions and masses, the warps' partial sums, and
 // the velocities of up to `rounds` receiver chunks per CTA.
-size_t persist_smem(int n, int F, int W, int rounds) {
+size_t persist_smem(int n, int F, int W, int NI, int rounds) {
   const int ns = (n + 1) & ~1;
-  const size_t rpc = (size_t)(32 / F) * kPNI;
+  const size_t rpc = (size_t)(32 / F) * NI;
   return (size_t)4 * ns * sizeof(double) + ((size_t)W + rounds) * rpc * 3 * sizeof(double);
 }
 
@@ -299,7 +309,7 @@ size_t persist_smem(int n, int F, int W, int rounds) {
 int persist_groups(int n, int sms) {
   const int need = (n + sms - 1) / sms;
   for (int F : {16, 8, 4})
-    if ((32 / F) * kPNI >= need) return F;
+    if ((32 / F) * kPNIDefault >= need) return F;
   return 4;
 }
 
@@ -351,24 +361,26 @@ int run_persistent(nbr_ctx* c, int precision, int scheme, double dt, size_t step
   if (e != cudaSuccess) return cuda_fail(c, e, "persistent setup");
 
   const ForceConfig& o = c->override_cfg[kFP64];
-  int F = persist_groups(n, c->sms), W = kPersistDefaultWarps;
+  int F = persist_groups(n, c->sms), W = kPersistDefaultWarps, NI = kPNIDefault;
   if (o.ni == kPersistNI) {
     F = o.warps;
     if (o.split > 1) W = o.split;
+    if (o.tile > 0) NI = o.tile;
   }
   const bool excl = eps2 == 0.0;
-  const void* fn = persist_fn(F, W, excl);
+  const void* fn = persist_fn(F, W, NI, excl);
   if (!fn)
     return fail(c, NBR_ERR_INVALID_ARG,
-                "persistent run: lane groups must be 4, 8 or 16 and warps per CTA 8 or 16");
+                "persistent run: (lane groups, receivers per lane) must be (4|8|16, 4) or "
+                "(8|16, 8) and warps per CTA 8 or 16");
   const int kPThreads = W * 32;
-  const int rpc = (32 / F) * kPNI;
+  const int rpc = (32 / F) * NI;
   // receivers per chunk: n / SMs (one chunk per SM) when the slots allow it
   const int cs = std::max(1, std::min(rpc, (n + c->sms - 1) / c->sms));
   const int chunks = (n + cs - 1) / cs;
   // the grid is at least min(chunks, SMs) CTAs, so no CTA gets more rounds than this
   const int rounds = (chunks + std::min(chunks, c->sms) - 1) / std::min(chunks, c->sms);
-  const size_t smem = persist_smem(n, F, W, rounds);
+  const size_t smem = persist_smem(n, F, W, NI, rounds);
   e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int per_sm = 0;
   if (e == cudaSuccess)

@@ -49,6 +49,25 @@ def test_persistent_matches_launch_per_step(ctx, nbr, n, groups, warps):
         assert _maxdiff(got, want) <= 1e-12, (scheme, order, eps2, _maxdiff(got, want))
 
 
+@pytest.mark.parametrize("n", [3, 1000, 2048, 4096])
+@pytest.mark.parametrize("groups", [8, 16])
+def test_persistent_eight_receivers_per_lane(ctx, nbr, n, groups):
+    """The layout with 8 receivers per lane (nbr_set_force_tiling tile = 8)."""
+    s = nbr.plummer(n, 90 + n)
+    for scheme, eps2 in ((KDK, 1e-6), (EULER, 0.0)):
+        ctx.set_force_config(FP64, PERSIST, groups, 16)
+        ctx.set_force_tiling(FP64, 8, 0)
+        try:
+            ctx.upload(s)
+            st = ctx.run(FP64, scheme, 2, 1e-3, 7, eps2=eps2)
+            got = ctx.download()
+        finally:
+            ctx.set_force_config(FP64, 0)
+        assert st["kernels"] == 1
+        want, _ = _run(ctx, s, (1, 8, 0), scheme, 2, 1e-3, 7, eps2)
+        assert _maxdiff(got, want) <= 1e-12, (scheme, eps2, _maxdiff(got, want))
+
+
 def test_persistent_is_the_default_for_small_fp64_systems(ctx, nbr, oracle):
     """Plummer N = 2048, eps = 1e-3, KDK dt = 1e-3, 100 steps (the small-system
     workload) through the default path: one launch, the oracle's trajectory."""
