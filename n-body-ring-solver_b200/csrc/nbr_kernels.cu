@@ -1701,10 +1701,13 @@ cudaError_t launch_small_t(double eps2, int split, const IParticles& ip, const J
 size_t n3_smem_bytes(int precision, int warps);
 
 bool force_config_supported(int precision, const ForceConfig& c) {
-  if (c.ni == kPersistNI)  // warps = lane groups, split = warps per CTA, tile = receivers
-    return precision == kFP64 && (c.split <= 1 || c.split == 8 || c.split == 16) &&
-           (((c.tile == 0 || c.tile == 4) && (c.warps == 4 || c.warps == 8 || c.warps == 16)) ||
-            (c.tile == 8 && (c.warps == 8 || c.warps == 16)));
+  if (c.ni == kPersistNI) {  // warps = lane groups, split = warps per CTA, tile = receivers
+    const bool f4 = c.warps == 4 || c.warps == 8 || c.warps == 16;
+    if (precision == kFP32C)  // 16 warps, 4 receivers per lane
+      return f4 && (c.split <= 1 || c.split == 16) && (c.tile == 0 || c.tile == 4);
+    return (c.split <= 1 || c.split == 8 || c.split == 16) &&
+           (((c.tile == 0 || c.tile == 4) && f4) || (c.tile == 8 && (c.warps == 8 || c.warps == 16)));
+  }
   if (c.ni == 3)  // Newton-3: FP32C one or two warps per row block; FP64 (two)
     return c.warps == kN3Warps || (precision == kFP32C && c.warps == kN3F64Warps);
   if (c.ni == 1) return (c.warps == 2 || c.warps == 4 || c.warps == 8) && c.split >= 1;

@@ -269,6 +269,251 @@ __global__ void __launch_bounds__(W * 32, 1) k_run_small_f64(const PersistArgs A
     }
 }
 
+// The FP32C form, with the pair arithmetic of k_force_small / k_force_f32c
+// (f32x2 differences, rsqrt.approx with the first-order Newton correction of
+// y^3 folded into the mass terms).  16 warps per CTA, 4 receivers per lane.
+// Per force evaluation every CTA reads all N positions from L2 into registers,
+// takes their FP64 mean as the origin (summed in a fixed order), and writes
+// FP32 source records relative to it into shared memory: (x, x, y, y),
+// (z, z, -1.5 m, -1.5 m), (2.5 m, 2.5 m), the mass terms once per run.  The
+// CTA's own receivers keep their FP64 positions and velocities in shared
+// memory for the whole run.  A thread's FP32 sums cover N / (16 F) sources;
+// lane groups and warps are then added in FP64 in a fixed order.
+constexpr int kPW32 = 16;
+constexpr int kPLoads32 = (int)((kPersistMaxN / 2 + kPW32 * 32 - 1) / (kPW32 * 32));
+
+template <int F, bool EXCL>
+__global__ void __launch_bounds__(kPW32 * 32, 1) k_run_small_f32c(const PersistArgs A) {
+  constexpr int W = kPW32, NT = W * 32, NI = 4, IPAIR = 2;
+  constexpr int G = 32 / F, RPC = G * NI, S = W * F;
+  extern __shared__ __align__(16) unsigned char smem_b[];
+  __shared__ double s_org[W][3];
+  __shared__ double s_o[3];
+  const int n = A.n, ns = (n + 1) & ~1;
+  ulonglong2* rxy = reinterpret_cast<ulonglong2*>(smem_b);  // [ns] (x, x, y, y)
+  ulonglong2* rzm = rxy + ns;                               // [ns] (z, z, -1.5 m, -1.5 m)
+  u64* rb = reinterpret_cast<u64*>(rzm + ns);               // [ns] (2.5 m, 2.5 m)
+  double* red = reinterpret_cast<double*>(rb + ns);         // [W][RPC][3]
+  const int rounds = (A.chunks + gridDim.x - 1) / gridDim.x;
+  double* svel = red + (size_t)W * RPC * 3;                 // [rounds][RPC][3]
+  double* spos = svel + (size_t)rounds * RPC * 3;           // [rounds][RPC][3]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gl = lane % G, grp = lane / G;
+  const float e2f = (float)A.eps2;
+  const u64 EPS2 = pack2(e2f, e2f);
+
+  for (int j = threadIdx.x; j < ns; j += NT) {
+    const double m = j < n ? A.m[j] : 0.0;
+    const float fa = __double2float_rn(-1.5 * m), fb = __double2float_rn(2.5 * m);
+    rzm[j] = make_ulonglong2(0ull, pack2(fa, fa));
+    rb[j] = pack2(fb, fb);
+  }
+  int cur = A.cur0;
+  unsigned long long nbar = 0;
+
+  if (A.pre) {
+    for (int c = blockIdx.x; c < A.chunks; c += gridDim.x) {
+      for (int t = threadIdx.x; t < A.cs; t += NT) {
+        const int i = c * A.cs + t;
+        if (i >= n) continue;
+        double ux = A.vx[i], uy = A.vy[i], uz = A.vz[i];
+        if (A.pre_use_acc) {
+          ux += A.pre_kick * A.ax[i]; uy += A.pre_kick * A.ay[i]; uz += A.pre_kick * A.az[i];
+          A.vx[i] = ux; A.vy[i] = uy; A.vz[i] = uz;
+        }
+        A.px[1 - cur][i] = __ldcg(A.px[cur] + i) + A.pre_drift * ux;
+        A.py[1 - cur][i] = __ldcg(A.py[cur] + i) + A.pre_drift * uy;
+        A.pz[1 - cur][i] = __ldcg(A.pz[cur] + i) + A.pre_drift * uz;
+      }
+    }
+    if (!grid_barrier(A.bar, A.err, A.wait_ns, nbar++)) return;
+    cur ^= 1;
+  }
+  // the CTA's receivers: positions and velocities in shared memory for the run
+  for (int c = blockIdx.x, r = 0; c < A.chunks; c += gridDim.x, ++r)
+    for (int t = threadIdx.x; t < RPC; t += NT) {
+      const int i = c * A.cs + t;
+      const bool own = t < A.cs && i < n;
+      double* v = svel + ((size_t)r * RPC + t) * 3;
+      double* x = spos + ((size_t)r * RPC + t) * 3;
+      v[0] = own ? A.vx[i] : 0.0; v[1] = own ? A.vy[i] : 0.0; v[2] = own ? A.vz[i] : 0.0;
+      x[0] = own ? __ldcg(A.px[cur] + i) : 0.0;
+      x[1] = own ? __ldcg(A.py[cur] + i) : 0.0;
+      x[2] = own ? __ldcg(A.pz[cur] + i) : 0.0;
+    }
+
+  for (int e = 0; e < A.evals; ++e) {
+    // all positions from L2 into registers, and their sum for the origin
+    const double2* X2 = reinterpret_cast<const double2*>(A.px[cur]);
+    const double2* Y2 = reinterpret_cast<const double2*>(A.py[cur]);
+    const double2* Z2 = reinterpret_cast<const double2*>(A.pz[cur]);
+    double2 qx[kPLoads32], qy[kPLoads32], qz[kPLoads32];
+    double ox = 0.0, oy = 0.0, oz = 0.0;
+#pragma unroll
+    for (int k = 0; k < kPLoads32; ++k) {
+      const int j2 = threadIdx.x + k * NT;
+      qx[k] = qy[k] = qz[k] = make_double2(0.0, 0.0);
+      if (j2 < ns / 2) {
+        qx[k] = __ldcg(X2 + j2); qy[k] = __ldcg(Y2 + j2); qz[k] = __ldcg(Z2 + j2);
+        ox += qx[k].x; oy += qy[k].x; oz += qz[k].x;
+        if (2 * j2 + 1 < n) { ox += qx[k].y; oy += qy[k].y; oz += qz[k].y; }
+      }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      ox += __shfl_xor_sync(0xffffffffu, ox, off);
+      oy += __shfl_xor_sync(0xffffffffu, oy, off);
+      oz += __shfl_xor_sync(0xffffffffu, oz, off);
+    }
+    if (lane == 0) { s_org[warp][0] = ox; s_org[warp][1] = oy; s_org[warp][2] = oz; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double a = 0.0, b = 0.0, cc = 0.0;
+      for (int w = 0; w < W; ++w) { a += s_org[w][0]; b += s_org[w][1]; cc += s_org[w][2]; }
+      s_o[0] = a / n; s_o[1] = b / n; s_o[2] = cc / n;
+    }
+    __syncthreads();
+    const double o0 = s_o[0], o1 = s_o[1], o2 = s_o[2];
+#pragma unroll
+    for (int k = 0; k < kPLoads32; ++k) {
+      const int j2 = threadIdx.x + k * NT;
+      if (j2 < ns / 2) {
+        const float x0 = __double2float_rn(qx[k].x - o0), x1 = __double2float_rn(qx[k].y - o0);
+        const float y0 = __double2float_rn(qy[k].x - o1), y1 = __double2float_rn(qy[k].y - o1);
+        const float z0 = __double2float_rn(qz[k].x - o2), z1 = __double2float_rn(qz[k].y - o2);
+        rxy[2 * j2] = make_ulonglong2(pack2(x0, x0), pack2(y0, y0));
+        rxy[2 * j2 + 1] = make_ulonglong2(pack2(x1, x1), pack2(y1, y1));
+        reinterpret_cast<u64*>(rzm + 2 * j2)[0] = pack2(z0, z0);
+        reinterpret_cast<u64*>(rzm + 2 * j2 + 1)[0] = pack2(z1, z1);
+      }
+    }
+    __syncthreads();
+    const double2 kd = A.sched[e];
+    for (int c = blockIdx.x, round = 0; c < A.chunks; c += gridDim.x, ++round) {
+      const int base = c * A.cs;
+      double* sp = spos + (size_t)round * RPC * 3;
+      u64 XI[IPAIR], YI[IPAIR], ZI[IPAIR], AX[IPAIR], AY[IPAIR], AZ[IPAIR];
+#pragma unroll
+      for (int p = 0; p < IPAIR; ++p) {
+        const double* r0 = sp + (gl + G * (2 * p)) * 3;
+        const double* r1 = sp + (gl + G * (2 * p + 1)) * 3;
+        XI[p] = pack2(__double2float_rn(r0[0] - o0), __double2float_rn(r1[0] - o0));
+        YI[p] = pack2(__double2float_rn(r0[1] - o1), __double2float_rn(r1[1] - o1));
+        ZI[p] = pack2(__double2float_rn(r0[2] - o2), __double2float_rn(r1[2] - o2));
+        AX[p] = AY[p] = AZ[p] = 0ull;
+      }
+#pragma unroll 2
+      for (int j = warp * F + grp; j < n; j += S) {
+        const ulonglong2 q0 = rxy[j];
+        const ulonglong2 q1 = rzm[j];
+        const u64 bj = rb[j];
+#pragma unroll
+        for (int p = 0; p < IPAIR; ++p) {
+          const u64 dx = sub2(q0.x, XI[p]);
+          const u64 dy = sub2(q0.y, YI[p]);
+          const u64 dz = sub2(q1.x, ZI[p]);
+          u64 r2 = fma2(dx, dx, EPS2);
+          r2 = fma2(dy, dy, r2);
+          r2 = fma2(dz, dz, r2);
+          u64 y;
+          if (EXCL) {
+            float rl, rh;
+            unpack2(r2, rl, rh);
+            y = pack2(rl > 0.f ? rsqrt_mufu(rl) : 0.f, rh > 0.f ? rsqrt_mufu(rh) : 0.f);
+          } else {
+            y = rsqrt2(r2);
+          }
+          const u64 y2 = mul2(y, y);
+          const u64 pr = mul2(r2, y2);
+          const u64 mg = fma2(q1.y, pr, bj);
+          const u64 y3 = mul2(y2, y);
+          const u64 sv = mul2(y3, mg);
+          AX[p] = fma2(sv, dx, AX[p]);
+          AY[p] = fma2(sv, dy, AY[p]);
+          AZ[p] = fma2(sv, dz, AZ[p]);
+        }
+      }
+      double ax[NI], ay[NI], az[NI];
+#pragma unroll
+      for (int p = 0; p < IPAIR; ++p) {
+        float l, h;
+        unpack2(AX[p], l, h); ax[2 * p] = l; ax[2 * p + 1] = h;
+        unpack2(AY[p], l, h); ay[2 * p] = l; ay[2 * p + 1] = h;
+        unpack2(AZ[p], l, h); az[2 * p] = l; az[2 * p + 1] = h;
+      }
+#pragma unroll
+      for (int off = G; off < 32; off <<= 1) {
+#pragma unroll
+        for (int k = 0; k < NI; ++k) {
+          ax[k] += __shfl_xor_sync(0xffffffffu, ax[k], off);
+          ay[k] += __shfl_xor_sync(0xffffffffu, ay[k], off);
+          az[k] += __shfl_xor_sync(0xffffffffu, az[k], off);
+        }
+      }
+      if (grp == 0) {
+#pragma unroll
+        for (int k = 0; k < NI; ++k) {
+          double* r = red + ((size_t)warp * RPC + gl + G * k) * 3;
+          r[0] = ax[k]; r[1] = ay[k]; r[2] = az[k];
+        }
+      }
+      __syncthreads();
+      if (threadIdx.x < RPC) {
+        const int t = threadIdx.x, i = base + t;
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+          const double* r = red + ((size_t)w * RPC + t) * 3;
+          a0 += r[0]; a1 += r[1]; a2 += r[2];
+        }
+        if (t < A.cs && i < n) {
+          const double gx = A.G * a0, gy = A.G * a1, gz = A.G * a2;
+          A.ax[i] = gx; A.ay[i] = gy; A.az[i] = gz;
+          double* v = svel + ((size_t)round * RPC + t) * 3;
+          double* x = sp + (size_t)t * 3;
+          const double ux = v[0], uy = v[1], uz = v[2];
+          const double vx = ux + kd.x * gx, vy = uy + kd.x * gy, vz = uz + kd.x * gz;
+          v[0] = vx; v[1] = vy; v[2] = vz;
+          const bool euler = A.mode == 2;
+          const double nx = x[0] + kd.y * (euler ? ux : vx);
+          const double ny = x[1] + kd.y * (euler ? uy : vy);
+          const double nz = x[2] + kd.y * (euler ? uz : vz);
+          x[0] = nx; x[1] = ny; x[2] = nz;
+          A.px[1 - cur][i] = nx; A.py[1 - cur][i] = ny; A.pz[1 - cur][i] = nz;
+        }
+      }
+      __syncthreads();  // red and the receivers' positions are read again
+    }
+    if (e + 1 < A.evals) {
+      if (e == A.skip_barrier && blockIdx.x == 0) return;  // test hook: never arrives
+      if (!grid_barrier(A.bar, A.err, A.wait_ns, nbar++)) return;
+    }
+    cur ^= 1;
+  }
+  for (int c = blockIdx.x, r = 0; c < A.chunks; c += gridDim.x, ++r)
+    for (int t = threadIdx.x; t < A.cs; t += NT) {
+      const int i = c * A.cs + t;
+      if (i >= n) continue;
+      const double* v = svel + ((size_t)r * RPC + t) * 3;
+      A.vx[i] = v[0]; A.vy[i] = v[1]; A.vz[i] = v[2];
+    }
+}
+
+const void* persist_fn32(int F, bool excl) {
+  switch (F) {
+    case 4: return excl ? (const void*)k_run_small_f32c<4, true> : (const void*)k_run_small_f32c<4, false>;
+    case 8: return excl ? (const void*)k_run_small_f32c<8, true> : (const void*)k_run_small_f32c<8, false>;
+    case 16: return excl ? (const void*)k_run_small_f32c<16, true> : (const void*)k_run_small_f32c<16, false>;
+    default: return nullptr;
+  }
+}
+
+size_t persist_smem32(int n, int F, int rounds) {
+  const int ns = (n + 1) & ~1;
+  const size_t rpc = (size_t)(32 / F) * 4;
+  return (size_t)40 * ns + ((size_t)kPW32 + 2 * (size_t)rounds) * rpc * 3 * sizeof(double);
+}
+
 template <int F, int NI>
 const void* persist_fn_f(int W, bool excl) {
   if (W == 8) return excl ? (const void*)k_run_small_f64<F, 8, NI, true> : (const void*)k_run_small_f64<F, 8, NI, false>;
@@ -318,13 +563,14 @@ int persist_groups(int n, int sms) {
 bool persistent_run_applies(nbr_ctx* c, int precision, size_t n) {
   const ForceConfig& o = c->override_cfg[precision];
   if (o.ni != 0 && o.ni != kPersistNI) return false;
-  return precision == kFP64 && c->coop && n >= 2 && n <= (size_t)kPersistMaxN;
+  // the default for FP64; the FP32C form when forced (ni = kPersistNI)
+  if (o.ni == 0 && precision != kFP64) return false;
+  return c->coop && n >= 2 && n <= (size_t)kPersistMaxN;
 }
 
 int run_persistent(nbr_ctx* c, int precision, int scheme, double dt, size_t steps, double G,
                    double eps2, bool fsal, const double* cc, const double* dd, int lf,
                    nbr_run_stats* st) {
-  (void)precision;
   SysState& s = c->sys;
   const int n = (int)s.n;
   // the schedule: the launch sequence of nbr_run's graph, one entry per evaluation
@@ -360,7 +606,7 @@ int run_persistent(nbr_ctx* c, int precision, int scheme, double dt, size_t step
   if (e == cudaSuccess) e = cudaMemsetAsync(bar, 0, sizeof(unsigned long long), c->stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "persistent setup");
 
-  const ForceConfig& o = c->override_cfg[kFP64];
+  const ForceConfig& o = c->override_cfg[precision];
   int F = persist_groups(n, c->sms), W = kPersistDefaultWarps, NI = kPNIDefault;
   if (o.ni == kPersistNI) {
     F = o.warps;
@@ -368,7 +614,12 @@ int run_persistent(nbr_ctx* c, int precision, int scheme, double dt, size_t step
     if (o.tile > 0) NI = o.tile;
   }
   const bool excl = eps2 == 0.0;
-  const void* fn = persist_fn(F, W, NI, excl);
+  const bool fp32 = precision == kFP32C;
+  if (fp32) {
+    W = kPW32;
+    NI = kPNIDefault;
+  }
+  const void* fn = fp32 ? persist_fn32(F, excl) : persist_fn(F, W, NI, excl);
   if (!fn)
     return fail(c, NBR_ERR_INVALID_ARG,
                 "persistent run: (lane groups, receivers per lane) must be (4|8|16, 4) or "
@@ -380,7 +631,7 @@ int run_persistent(nbr_ctx* c, int precision, int scheme, double dt, size_t step
   const int chunks = (n + cs - 1) / cs;
   // the grid is at least min(chunks, SMs) CTAs, so no CTA gets more rounds than this
   const int rounds = (chunks + std::min(chunks, c->sms) - 1) / std::min(chunks, c->sms);
-  const size_t smem = persist_smem(n, F, W, NI, rounds);
+  const size_t smem = fp32 ? persist_smem32(n, F, rounds) : persist_smem(n, F, W, NI, rounds);
   e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int per_sm = 0;
   if (e == cudaSuccess)

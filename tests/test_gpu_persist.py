@@ -114,3 +114,48 @@ def test_persistent_grid_barrier_expires_cleanly(nbr, oracle):
     want = oracle.kdk(s, 1e-3, 4, eps2=1e-6)
     for k in ("x", "y", "z", "vx", "vy", "vz"):
         assert np.abs(got[k] - want[k]).max() <= 1e-11, k
+
+
+FP32C = 1
+
+
+@pytest.mark.parametrize("n", [2, 127, 1000, 2048, 4096])
+@pytest.mark.parametrize("groups", [4, 8, 16])
+def test_persistent_fp32c(ctx, nbr, oracle, n, groups):
+    """The FP32C form of the persistent run (forced with ni = 2): the oracle's
+    KDK and Euler trajectories within the FP32C tolerance of the other
+    FP32C trajectory tests, one launch per run, and the FP32C accelerations
+    it leaves against the FP64 ones."""
+    s = nbr.plummer(n, 70 + n)
+    for scheme, eps2 in ((KDK, 1e-6), (EULER, 1e-6), (KDK, 0.0)):
+        ctx.set_force_config(FP32C, PERSIST, groups, 0)
+        try:
+            ctx.upload(s)
+            st = ctx.run(FP32C, scheme, 2, 1e-3, 5, eps2=eps2)
+            got = ctx.download()
+        finally:
+            ctx.set_force_config(FP32C, 0)
+        assert st["kernels"] == 1 and st["force_evals"] == (6 if scheme == KDK else 5)
+        want = oracle.kdk(s, 1e-3, 5, eps2=eps2) if scheme == KDK else oracle.euler(s, 1e-3, 5, eps2=eps2)
+        for k in ("x", "y", "z", "vx", "vy", "vz"):
+            assert np.abs(got[k] - want[k]).max() <= 1e-6, (scheme, eps2, k)
+
+
+def test_persistent_fp32c_far_from_the_origin(ctx, nbr, oracle):
+    """Its records are relative to the system's FP64 mean position, so a
+    system shifted far from the coordinate origin keeps FP32 resolution."""
+    s = nbr.plummer(2048, 5)
+    for k, d in (("x", 1.0e3), ("y", -2.0e3), ("z", 5.0e2)):
+        s[k] = s[k] + d
+    ctx.set_force_config(FP32C, PERSIST, 8, 0)
+    try:
+        ctx.upload(s)
+        ctx.run(FP32C, KDK, 2, 1e-3, 5, eps2=1e-6)
+        got = ctx.download()
+    finally:
+        ctx.set_force_config(FP32C, 0)
+    want = oracle.kdk(s, 1e-3, 5, eps2=1e-6)
+    for k in ("vx", "vy", "vz"):
+        assert np.abs(got[k] - want[k]).max() <= 1e-6, k
+    for k in ("x", "y", "z"):
+        assert np.abs(got[k] - want[k]).max() <= 1e-6 * (1.0 + np.abs(want[k]).max()), k
