@@ -291,11 +291,11 @@ int nbr_snapshot_load(nbr_ctx* ctx, const char* path, size_t n, size_t record, d
  * and applied to both particles, for FP32C and for FP64; for FP32C also
  * warps = 16, two warps per 256-particle row block; whole systems only,
  * receiver ranges and separate receiver and source sets fall back to the large
- * kernels; ni = 2, FP64 only, warps = 4, 8 or 16 lane groups per warp, split =
- * 8 or 16 warps per CTA (0: 16): nbr_run of a system of at most 4096
+ * kernels; ni = 2, warps = 4, 8 or 16 lane groups per warp, split = 8 or 16
+ * warps per CTA (0: 16; FP32C: 16 only): nbr_run of a system of at most 4096
  * particles as one cooperative launch for all steps (the default for such
- * systems), evaluations outside nbr_run use the default kernels).  ni = 0
- * restores the autotuner. */
+ * systems, both precisions), evaluations outside nbr_run use the default
+ * kernels).  ni = 0 restores the autotuner. */
 int nbr_set_force_config(nbr_ctx* ctx, int precision, int ni, int warps, int split);
 /* The j-tile (sources per stage of the shared-memory ring: 64, 128 or 256)
  * and the unroll depth of the source loop (2, 4 or 8) of the large kernels,

@@ -1138,7 +1138,7 @@ int nbr_run(nbr_ctx* c, int precision, int scheme, int order, double dt, size_t 
   }
   nbr_run_stats st{};
   if (steps > 0 && persistent_run_applies(c, precision, s.n)) {
-    // small FP64 systems: every step in one cooperative launch
+    // small systems: every step in one cooperative launch
     const bool fsal = (scheme == NBR_KDK) && c->acc_ok && c->acc_prec == precision &&
                       c->acc_G == G && c->acc_eps2 == eps2;
     rc = run_persistent(c, precision, scheme, dt, steps, G, eps2, fsal, cc, dd, lf, &st);

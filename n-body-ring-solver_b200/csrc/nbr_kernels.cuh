@@ -192,8 +192,8 @@ cudaError_t launch_sum_finish(const IParticles& ip, const Epilogue& ep, const do
 cudaError_t configure_kernels();
 
 // The persistent small-system run (nbr_persist.cu): the whole nbr_run step
-// loop of an FP64 system of at most kPersistMaxN particles in one cooperative
-// launch.  ForceConfig ni = kPersistNI with warps = lane groups (4, 8, 16)
+// loop of a system of at most kPersistMaxN particles (FP64 or FP32C) in one
+// cooperative launch.  ForceConfig ni = kPersistNI with warps = lane groups (4, 8, 16)
 // forces it; it is the default for such systems.
 // ForceConfig split = warps per CTA of that launch (8 or 16; 0: default).
 constexpr int kPersistNI = 2;

@@ -9,20 +9,22 @@
 //  * each CTA owns fixed receiver chunks (about n / SMs particles, at most RPC
 //    lane slots) for the whole run;
 //  * per force evaluation every CTA stages all N positions (masses once) in
-//    shared memory with L2 loads, its 8 warps split the sources 8 ways and the
-//    F lane groups of each warp split them again (k_force_small's layout), and
-//    the partial sums are combined in a fixed order (xor shuffles, then the
-//    warps in order): deterministic;
-//  * the CTA applies the fused kick/drift to its receivers, writing the next
-//    position buffer, and all CTAs meet at one grid barrier before the next
-//    evaluation reads it.
+//    shared memory with L2 loads, its W warps (8 or 16) split the sources W
+//    ways and the F lane groups of each warp split them again
+//    (k_force_small's layout), and the partial sums are combined in a fixed
+//    order (xor shuffles, then the warps in order): deterministic;
+//  * the CTA applies the fused kick/drift to its receivers, whose velocities
+//    (and, FP32C, positions) stay in shared memory for the run, writes their
+//    positions to the next buffer, and all CTAs meet at one grid barrier
+//    before the next evaluation reads it.
 //
-// The barrier is a 64-bit arrival counter that only grows; its wait is bounded by
-// %globaltimer (the context's wait limit) and gives up, with an error code
+// The barrier is a 64-bit arrival counter that only grows; its wait is bounded
+// by %globaltimer (the context's wait limit) and gives up, with an error code
 // for the host, if the limit passes or another CTA has already recorded an
 // error.  The cooperative launch guarantees that all CTAs are resident, so no
-// CTA waits on one that cannot run.  Pair arithmetic is k_force_f64's (CUDA's
-// rsqrt(double)): results equal the other FP64 kernels' up to summation order.
+// CTA waits on one that cannot run.  FP64 pair arithmetic is k_force_f64's
+// (CUDA's rsqrt(double)): results equal the other FP64 kernels' up to
+// summation order; the FP32C form (k_run_small_f32c) is described there.
 #include "nbr.h"
 #include "nbr_ctx.h"
 #include "nbr_device.cuh"
@@ -563,8 +565,6 @@ int persist_groups(int n, int sms) {
 bool persistent_run_applies(nbr_ctx* c, int precision, size_t n) {
   const ForceConfig& o = c->override_cfg[precision];
   if (o.ni != 0 && o.ni != kPersistNI) return false;
-  // the default for FP64; the FP32C form when forced (ni = kPersistNI)
-  if (o.ni == 0 && precision != kFP64) return false;
   return c->coop && n >= 2 && n <= (size_t)kPersistMaxN;
 }
 
