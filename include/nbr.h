@@ -227,9 +227,12 @@ int nbr_step_range(nbr_ctx* ctx, int precision, int scheme, size_t i0, size_t co
  * The block-pair triangle of the uploaded system is cut into nslices slices
  * of consecutive row groups with equal pair work; each unordered pair belongs
  * to exactly one slice.  nbr_n3_slice_accel writes the partial accelerations
- * (not multiplied by G) that slice `slice` gives EVERY particle, in FP64,
- * into the device array dst[d * ld + i] (d = x, y, z; ld >= the system size
- * rounded up to 1024), asynchronous on the context's stream.  A rank computes
+ * (not multiplied by G) that each slice v in [slice_begin, slice_end) gives
+ * EVERY particle, in FP64, into the device array dst[(v - slice_begin) * 3 *
+ * ld + d * ld + i] (d = x, y, z; ld >= the system size rounded up to 1024),
+ * asynchronous on the context's stream; the slices of the range share one
+ * pair-kernel launch (each slice's partials are the same as when computed
+ * alone).  A rank computes
  * its slices, the ranks exchange the columns of their owned ranges (an
  * all-to-all), and nbr_step_range_sum adds, for the receivers [i0, i0 +
  * count) (i0 a multiple of 128), the nslices partials in slice order --
@@ -238,8 +241,8 @@ int nbr_step_range(nbr_ctx* ctx, int precision, int scheme, size_t i0, size_t co
  * (NBR_KDK / NBR_DKD: v += kick a, x' = x + drift v; NBR_EULER: drift with
  * the old velocity) to them, like nbr_step_range.  With the same nslices the
  * result does not depend on how the slices are spread over ranks. */
-int nbr_n3_slice_accel(nbr_ctx* ctx, int precision, double eps2, int slice, int nslices, double* dst,
-                       size_t ld);
+int nbr_n3_slice_accel(nbr_ctx* ctx, int precision, double eps2, int slice_begin, int slice_end,
+                       int nslices, double* dst, size_t ld);
 int nbr_step_range_sum(nbr_ctx* ctx, int precision, int scheme, size_t i0, size_t count, double kick,
                        double drift, double G, const double* src, int nslices, size_t vstride,
                        size_t ld);

@@ -893,16 +893,16 @@ int nbr_step_range(nbr_ctx* c, int precision, int scheme, size_t i0, size_t coun
   return rc;
 }
 
-int nbr_n3_slice_accel(nbr_ctx* c, int precision, double eps2, int slice, int nslices, double* dst,
-                       size_t ld) {
+int nbr_n3_slice_accel(nbr_ctx* c, int precision, double eps2, int slice_begin, int slice_end,
+                       int nslices, double* dst, size_t ld) {
   TraceRange trace_range("nbr_n3_slice_accel");
   if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
   if (precision != NBR_FP64 && precision != NBR_FP32C)
     return fail(c, NBR_ERR_INVALID_ARG, "unknown precision");
   if (!(eps2 >= 0.0) || !std::isfinite(eps2))
     return fail(c, NBR_ERR_INVALID_ARG, "eps2 must be finite and >= 0");
-  if (nslices < 1 || slice < 0 || slice >= nslices)
-    return fail(c, NBR_ERR_INVALID_ARG, "need 0 <= slice < nslices");
+  if (nslices < 1 || slice_begin < 0 || slice_end <= slice_begin || slice_end > nslices)
+    return fail(c, NBR_ERR_INVALID_ARG, "need 0 <= slice_begin < slice_end <= nslices");
   SysState& s = c->sys;
   if (s.n == 0) return fail(c, NBR_ERR_NO_SYSTEM, "no system uploaded");
   if (!dst || ld < s.n_pad)
@@ -912,7 +912,7 @@ int nbr_n3_slice_accel(nbr_ctx* c, int precision, double eps2, int slice, int ns
   cudaError_t e = precision == kFP32C ? ensure_records(c, a, nullptr) : cudaSuccess;
   if (e != cudaSuccess) return cuda_fail(c, e, "pack");
   const long long nb = ((long long)s.n + kN3Block - 1) / kN3Block;
-  const long long need = n3_slice_scratch_doubles(nb, slice, nslices);
+  const long long need = n3_slices_scratch_doubles(nb, slice_begin, slice_end, nslices);
   e = c->scr.need_part((size_t)std::max<long long>(need, 1));
   if (e != cudaSuccess) return cuda_fail(c, e, "Newton-3 slice scratch");
   ForceConfig cfg = choose_config(c, precision, eps2, (long long)s.n, s.ntiles);
@@ -921,9 +921,9 @@ int nbr_n3_slice_accel(nbr_ctx* c, int precision, double eps2, int slice, int ns
   JStream js{s.pos[a][0], s.pos[a][1], s.pos[a][2], s.mass, s.rec[a], s.org[a], s.ntiles, 0, -1};
   pipeline_params(js);
   NBR_CHECKED_ONLY(ip.len = (long long)(s.cap + kRangeSlack); js.len = (long long)s.cap;)
-  e = launch_n3_slice(precision, warps, eps2, ip, js, c->d_err, slice, nslices, c->scr.part,
-                      (long long)c->scr.part_cap, dst, (long long)ld, 3 * (long long)ld, false,
-                      c->stream);
+  e = launch_n3_slices(precision, warps, eps2, ip, js, c->d_err, slice_begin, slice_end, nslices,
+                       c->scr.part, (long long)c->scr.part_cap, dst, (long long)ld,
+                       3 * (long long)ld * (slice_end - slice_begin), false, c->stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "Newton-3 slice launch");
   c->acc_ok = false;
   return NBR_OK;

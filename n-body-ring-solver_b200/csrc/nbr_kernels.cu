@@ -1868,15 +1868,20 @@ cudaError_t launch_n3_pairs(int precision, int warps, double eps2, const IPartic
   return cudaGetLastError();
 }
 
-cudaError_t launch_n3_slice(int precision, int warps, double eps2, const IParticles& ip,
-                            const JStream& js, int* err, int slice, int nslices, double* scratch,
-                            long long scratch_len, double* dst, long long ld, long long dst_len,
-                            bool accumulate, cudaStream_t st) {
-  if (ip.n <= 0 || js.ntiles <= 0) return cudaSuccess;
+cudaError_t launch_n3_slices(int precision, int warps, double eps2, const IParticles& ip,
+                             const JStream& js, int* err, int v0, int v1, int nslices,
+                             double* scratch, long long scratch_len, double* dst, long long ld,
+                             long long dst_len, bool accumulate, cudaStream_t st) {
+  if (ip.n <= 0 || js.ntiles <= 0 || v1 <= v0) return cudaSuccess;
   N3Params p3{};
   p3.nb = (ip.n + kN3Block - 1) / kN3Block;
   p3.cols = n3_cols(p3.nb);
-  n3_slice_groups(p3.nb, p3.cols, slice, nslices, &p3.g0, &p3.g1);
+  // one pair launch over the slices' consecutive row groups: a CTA's partial
+  // sums depend on its (row group, chunk) only, so they equal those of
+  // per-slice launches, with fewer partly filled waves
+  int g_last = 0;
+  n3_slice_groups(p3.nb, p3.cols, v0, nslices, &p3.g0, &g_last);
+  n3_slice_groups(p3.nb, p3.cols, v1 - 1, nslices, &g_last, &p3.g1);
   const long long ctas = n3_ctas_range(p3.nb, p3.cols, p3.g0, p3.g1);
   p3.act = scratch;
   p3.rea = scratch + (size_t)ctas * kN3Warps * 3 * kN3Block;
@@ -1888,9 +1893,29 @@ cudaError_t launch_n3_slice(int precision, int warps, double eps2, const IPartic
   Epilogue ep{};
   ep.err = err;
   const long long threads = p3.nb * 2 * 32;  // a warp per tile
-  k_n3_reduce<<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(ip, ep, p3, accumulate ? 2 : 1,
-                                                                  dst, ld);
-  return cudaGetLastError();
+  for (int v = v0; v < v1; ++v) {
+    // slice v's row groups and the offset of their CTAs inside the launch
+    N3Params pv = p3;
+    n3_slice_groups(p3.nb, p3.cols, v, nslices, &pv.g0, &pv.g1);
+    const long long before = n3_ctas_range(p3.nb, p3.cols, p3.g0, pv.g0);
+    pv.act = p3.act + (size_t)before * kN3Warps * 3 * kN3Block;
+    pv.rea = p3.rea + (size_t)before * p3.cols * 3 * kN3Block;
+    NBR_CHECKED_ONLY(pv.act_len = scratch_len - (pv.act - scratch);
+                     pv.dst_len = dst_len - (long long)(v - v0) * 3 * ld;)
+    k_n3_reduce<<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(
+        ip, ep, pv, accumulate ? 2 : 1, dst + (size_t)(v - v0) * 3 * ld, ld);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t launch_n3_slice(int precision, int warps, double eps2, const IParticles& ip,
+                            const JStream& js, int* err, int slice, int nslices, double* scratch,
+                            long long scratch_len, double* dst, long long ld, long long dst_len,
+                            bool accumulate, cudaStream_t st) {
+  return launch_n3_slices(precision, warps, eps2, ip, js, err, slice, slice + 1, nslices, scratch,
+                          scratch_len, dst, ld, dst_len, accumulate, st);
 }
 
 cudaError_t launch_sum_finish(const IParticles& ip, const Epilogue& ep, const double* src, int V,

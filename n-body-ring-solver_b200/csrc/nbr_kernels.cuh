@@ -160,12 +160,16 @@ inline void n3_slice_groups(long long nb, int cols, int v, int V, int* g0, int* 
   *g0 = start(v);
   *g1 = start(v + 1);
 }
-// Doubles of partial-sum scratch of slice v of V.
-inline long long n3_slice_scratch_doubles(long long nb, int v, int V) {
+// Doubles of partial-sum scratch of slices [v0, v1) of V (one launch).
+inline long long n3_slices_scratch_doubles(long long nb, int v0, int v1, int V) {
   const int cols = n3_cols(nb);
-  int g0 = 0, g1 = 0;
-  n3_slice_groups(nb, cols, v, V, &g0, &g1);
+  int g0 = 0, g1 = 0, g = 0;
+  n3_slice_groups(nb, cols, v0, V, &g0, &g);
+  n3_slice_groups(nb, cols, v1 - 1, V, &g, &g1);
   return n3_ctas_range(nb, cols, g0, g1) * (long long)(kN3Warps + cols) * 3 * kN3Block;
+}
+inline long long n3_slice_scratch_doubles(long long nb, int v, int V) {
+  return n3_slices_scratch_doubles(nb, v, v + 1, V);
 }
 // One Newton-3 force evaluation over all n_pad receivers of ip against the
 // same particles in js (FP32C: their records; FP64: their x, y, z, m arrays),
@@ -183,6 +187,13 @@ cudaError_t launch_n3_slice(int precision, int warps, double eps2, const IPartic
                             const JStream& js, int* err, int slice, int nslices, double* scratch,
                             long long scratch_len, double* dst, long long ld, long long dst_len,
                             bool accumulate, cudaStream_t stream);
+// Slices [v0, v1) in one pair launch (the same partial sums as one launch per
+// slice): slice v's partials into dst + (v - v0) 3 ld; scratch holds
+// n3_slices_scratch_doubles doubles.
+cudaError_t launch_n3_slices(int precision, int warps, double eps2, const IParticles& ip,
+                             const JStream& js, int* err, int v0, int v1, int nslices,
+                             double* scratch, long long scratch_len, double* dst, long long ld,
+                             long long dst_len, bool accumulate, cudaStream_t stream);
 // The epilogue of the large kernels on the receivers ip, from V partial
 // accelerations per particle summed in slice order: src[v * vstride + d * ld + i].
 cudaError_t launch_sum_finish(const IParticles& ip, const Epilogue& ep, const double* src, int V,

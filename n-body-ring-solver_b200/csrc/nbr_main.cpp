@@ -568,10 +568,9 @@ int run_multi(const Args& a) {
   };
   auto evaluate = [&](double kick, double drift) {
     for (int r = 0; r < W && rc == 0; ++r)
-      for (int v = R[r].v0; v < R[r].v1; ++v)
-        if (nbr_n3_slice_accel(R[r].ctx, a.precision, eps2, v, V,
-                               R[r].mine + (size_t)(v - R[r].v0) * 3 * ld, ld) != NBR_OK)
-          rc = multi_fail("slice", nbr_last_error_string(R[r].ctx));
+      if (nbr_n3_slice_accel(R[r].ctx, a.precision, eps2, R[r].v0, R[r].v1, V, R[r].mine, ld) !=
+          NBR_OK)
+        rc = multi_fail("slice", nbr_last_error_string(R[r].ctx));
     if (rc) return;
     nccl_ok(ncclGroupStart(), "group");
     for (int r = 0; r < W; ++r) {

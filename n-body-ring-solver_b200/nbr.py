@@ -109,8 +109,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         "nbr_batch_autotune": ([C.c_void_p, C.c_int, C.c_double], C.c_int),
         "nbr_step_range": ([C.c_void_p, C.c_int, C.c_int, _SZ, _SZ, C.c_double, C.c_double, C.c_double,
                             C.c_double], C.c_int),
-        "nbr_n3_slice_accel": ([C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int, C.c_void_p, _SZ],
-                               C.c_int),
+        "nbr_n3_slice_accel": ([C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int,
+                                C.c_void_p, _SZ], C.c_int),
         "nbr_step_range_sum": ([C.c_void_p, C.c_int, C.c_int, _SZ, _SZ, C.c_double, C.c_double,
                                 C.c_double, C.c_void_p, C.c_int, _SZ, _SZ], C.c_int),
         "nbr_state_pointers": ([C.c_void_p] + [C.POINTER(C.c_void_p)] * 6 + [C.POINTER(_SZ)], C.c_int),
@@ -395,15 +395,21 @@ class Context:
         self._chk(self.L.nbr_step_range(self.h, precision, scheme, i0, count, kick, drift, G, eps2),
                   "step_range")
 
-    def n3_slice_accel(self, precision, eps2, slice_, nslices, dst):
-        """Newton-3 partial accelerations of every particle from slice
-        `slice_` of `nslices` into dst, a contiguous device tensor of shape
-        (3, ld) float64 (ld >= the padded size), asynchronous on the context's
-        stream."""
-        assert dst.dtype == torch_float64() and dst.is_contiguous() and dst.dim() == 2
-        self._chk(self.L.nbr_n3_slice_accel(self.h, precision, eps2, slice_, nslices,
-                                            C.c_void_p(dst.data_ptr()), dst.stride(0)),
-                  "n3_slice_accel")
+    def n3_slice_accel(self, precision, eps2, slice_, nslices, dst, slice_end=None):
+        """Newton-3 partial accelerations of every particle from slices
+        [slice_, slice_end) of `nslices` (slice_end: slice_ + 1 by default)
+        into dst, a contiguous device tensor of shape (3, ld) for one slice or
+        (slices, 3, ld) float64 (ld >= the padded size), asynchronous on the
+        context's stream; the slices share one pair-kernel launch."""
+        end = slice_ + 1 if slice_end is None else slice_end
+        assert dst.dtype == torch_float64() and dst.is_contiguous()
+        if dst.dim() == 2:
+            assert end == slice_ + 1 and dst.shape[0] == 3
+        else:
+            assert dst.dim() == 3 and dst.shape[0] == end - slice_ and dst.shape[1] == 3
+        ld = dst.stride(-2)
+        self._chk(self.L.nbr_n3_slice_accel(self.h, precision, eps2, slice_, end, nslices,
+                                            C.c_void_p(dst.data_ptr()), ld), "n3_slice_accel")
 
     def step_range_sum(self, precision, scheme, i0, count, kick, drift, G, src):
         """Kick/drift of receivers [i0, i0 + count) from the partial

@@ -146,8 +146,7 @@ class ShardedSystem:
         V, W, c = self.slices, self.world, self.count
         nv = self.v1 - self.v0
         with self._stream_ctx(self._mine):
-            for v in range(self.v0, self.v1):
-                self.ctx.n3_slice_accel(precision, eps2, v, V, self._mine[v - self.v0])
+            self.ctx.n3_slice_accel(precision, eps2, self.v0, V, self._mine, slice_end=self.v1)
             # columns of every rank's receivers: [W][nv][3][c] out, [V][3][c] in
             send = self._mine[:, :, :W * c].reshape(nv, 3, W, c).permute(2, 0, 1, 3).contiguous()
             out_splits = [(slice_range(V, W, q)[1] - slice_range(V, W, q)[0]) * 3 * c

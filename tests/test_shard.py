@@ -54,18 +54,22 @@ class OracleRangeContext:
             self.pos[b][d][r] = self.pos[a][d][r] + drift * v_drift
         self.cur = b
 
-    def n3_slice_accel(self, precision, eps2, v, V, dst):
-        """Stand-in slice: the accelerations from the sources of index block v
-        of V (a different partition of the pairs than the library's, with
-        the same property: the V slices together hold each pair once)."""
+    def n3_slice_accel(self, precision, eps2, v0, V, dst, slice_end=None):
+        """Stand-in slices [v0, slice_end): the accelerations from the sources
+        of index block v of V (a different partition of the pairs than the
+        library's, with the same property: the V slices together hold each
+        pair once)."""
         n = self.n
-        lo, hi = n * v // V, n * (v + 1) // V
-        m = np.zeros(n)
-        m[lo:hi] = self.m[lo:hi]
-        x, y, z = (p[:n].copy() for p in self.pos[self.cur])
-        a = self.orc.accel(x, y, z, m, 1.0, eps2)
-        dst.zero_()
-        dst[:, :n] = torch.from_numpy(a)
+        v1 = v0 + 1 if slice_end is None else slice_end
+        out = dst.view(v1 - v0, 3, -1)
+        for v in range(v0, v1):
+            lo, hi = n * v // V, n * (v + 1) // V
+            m = np.zeros(n)
+            m[lo:hi] = self.m[lo:hi]
+            x, y, z = (p[:n].copy() for p in self.pos[self.cur])
+            a = self.orc.accel(x, y, z, m, 1.0, eps2)
+            out[v - v0].zero_()
+            out[v - v0, :, :n] = torch.from_numpy(a)
 
     def step_range_sum(self, precision, scheme, i0, count, kick, drift, G, src):
         n, a, b = self.n, self.cur, 1 - self.cur
