@@ -265,3 +265,26 @@ def test_banded_newton3_evaluation(nbr, oracle, prec):
     want = oracle.kdk(s, 1e-3, 3, eps2=eps2)
     for k in ("x", "y", "z", "vx", "vy", "vz"):
         assert np.abs(got[k] - want[k]).max() <= (1e-11 if prec == 0 else 1e-6), k
+
+
+def test_banded_newton3_at_two_million(nbr, oracle):
+    """N = 2^21: past the single-launch scratch limit, the default Newton-3
+    evaluation runs in slices of bounded scratch; sampled receivers against
+    the extended-precision oracle (FP64 to 1e-12, FP32C median 1e-6) and
+    Newton's third law over all particles."""
+    n, eps2 = 1 << 21, 1e-6
+    s = nbr.plummer(n, 2)
+    with nbr.Context(0) as c:
+        c.upload(s)
+        assert c.get_force_config(0, eps2)[0] == 3 and c.get_force_config(1, eps2)[0] == 3
+        a64 = c.forces(0, eps2=eps2)
+        a32 = c.forces(1, eps2=eps2)
+    idx = np.random.default_rng(1).choice(n, 128, replace=False)
+    ref = oracle.accel_subset(s["x"], s["y"], s["z"], s["m"], idx, eps2=eps2)
+    e64 = np.linalg.norm(a64[:, idx] - ref, axis=0) / np.linalg.norm(ref, axis=0)
+    e32 = np.linalg.norm(a32[:, idx] - ref, axis=0) / np.linalg.norm(ref, axis=0)
+    assert e64.max() <= 1e-12, e64.max()
+    assert np.median(e32) <= 1e-6, np.median(e32)
+    for a in (a64, a32):
+        net = np.abs((a * s["m"]).sum(axis=1)).max()
+        assert net <= 1e-6 * (np.linalg.norm(a, axis=0) * s["m"]).sum()
