@@ -376,17 +376,24 @@ int nbr_batch_download(nbr_ctx* ctx, double* x, double* y, double* z, double* vx
 int nbr_batch_forces(nbr_ctx* ctx, int precision, double G, double eps2, int want_force,
                      double* ax, double* ay, double* az);
 /* KDK leapfrog of every system for `steps` steps: one persistent launch per
- * step walking a device work queue of (system, receiver tile) items, the whole
- * step loop captured in one CUDA graph. */
+ * step walking a device work queue of (system, receiver tile) items (FP32C
+ * Newton-3 row blocks: one more launch, the epilogue that sums each
+ * particle's action and reactions in a fixed order), the whole step loop
+ * captured in one CUDA graph. */
 int nbr_batch_run(nbr_ctx* ctx, int precision, double dt, size_t steps, double G, double eps2,
                   nbr_run_stats* stats);
 /* Forces the batched kernel's configuration for a precision: wide = 1 pairs a
  * system's receiver tiles into two-tile work items (8 receivers per lane),
- * wide = 0 keeps one-tile items (4 per lane); ctas_per_sm = resident CTAs per
- * SM of the persistent grid (0: the occupancy limit).  wide = -1 restores the
- * autotune cache or the default (occupancy limit; two-tile items for FP32C,
- * one-tile items for FP64).  Applies to
- * the uploaded batch; an upload starts from the autotune cache again. */
+ * wide = 0 keeps one-tile items (4 per lane), wide = 2 (FP32C only; else
+ * NBR_ERR_INVALID_ARG) evaluates every system of three tiles (257 particles)
+ * or more by Newton-3 row blocks -- two receiver tiles against the later
+ * column tiles, each pair once -- and the others as for wide = 1;
+ * ctas_per_sm = resident CTAs per SM of the persistent grid (0: the
+ * occupancy limit).  wide = -1 restores the autotune cache or the default
+ * (occupancy limit; Newton-3 row blocks for FP32C, one-tile items for FP64).
+ * Applies to the uploaded batch; an upload starts from the autotune cache
+ * again.  The Newton-3 scratch (3 doubles per particle and 3 x 128 doubles
+ * per (row block, later column tile)) is allocated at its first use. */
 int nbr_batch_set_config(nbr_ctx* ctx, int precision, int wide, int ctas_per_sm);
 /* Times every (item width, CTAs per SM) on the uploaded batch and stores the
  * fastest in the autotune cache under the batch's (precision, log2 system

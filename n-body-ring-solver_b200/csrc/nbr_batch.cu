@@ -47,6 +47,7 @@ constexpr int kStageB32 = kRec32 + 32;        // + origin
 constexpr int kStageB64 = 4 * kTile * 8;      // FP64 x, y, z, m
 constexpr int kBHead = 128;                   // barriers: kBWarps * kBStages * 8 <= 128
 constexpr int kWideItem = 1 << 30;            // item flag: two receiver tiles
+constexpr int kN3Item = 1 << 29;              // item flag: a Newton-3 row block (FP32C)
 
 struct BatchParams {
   const double* x; const double* y; const double* z; const double* m;  // current buffer
@@ -65,9 +66,23 @@ struct BatchParams {
   int* err;
   unsigned long long wait_ns;
   int skip_tile;
+  // Newton-3 items: the action of every particle [3][n_pad], the reaction
+  // partials (one 3 x 128 slot per (row block, later column tile) of a
+  // system), and each system's first slot (-1: the system has no N3 items)
+  double* act;
+  double* rea;
+  const long long* rea_off;
+  long long n_pad;
   NBR_CHECKED_FIELD(long long len)  // entries allocated in the particle arrays
   NBR_CHECKED_FIELD(int nsys)
+  NBR_CHECKED_FIELD(long long rea_len)  // doubles allocated in rea
 };
+
+// Reaction slots before row block b of a system of T tiles: row block b' has
+// T - 2 b' - 2 later column tiles (every b' < b has at least one).
+__host__ __device__ inline long long n3b_prefix(int T, int b) {
+  return (long long)b * (T - 2) - (long long)b * (b - 1);
+}
 
 template <int P>
 struct Stage;
@@ -377,10 +392,235 @@ __device__ __forceinline__ bool run_item(const BatchParams& p, double eps2, u64 
   return true;
 }
 
-// The persistent kernel.  WIDE = false: every item is narrow (4 receivers per
-// lane); WIDE = true: items flagged kWideItem cover two tiles (8 receivers per
-// lane: twice the pair work per source read, four independent f32x2 chains).
-template <int PREC, bool EXCL, bool WIDE>
+// One Newton-3 item (FP32C): row block `blk` of system s -- its tiles 2 blk and
+// 2 blk + 1, 256 receivers, 8 per lane (lane + 32 q) -- against the system's
+// column tiles c >= 2 blk.  Its own two tiles: every ordered pair, action only.
+// Each later tile c: every pair once, the tile's 128 sources in 4 batches of
+// 32, one per lane, rotating through the warp by shuffles with their reaction
+// sums (the scheme of k_force_n3_f32c); the reaction of tile c from this block
+// goes to its slot, the action of the block's receivers to p.act.  The epilogue
+// runs later, in k_batch_n3_reduce.  Returns false if a tile wait gave up.
+template <bool EXCL>
+__device__ __forceinline__ bool run_item_n3(const BatchParams& p, u64 EPS2, Ring& ring, int lane,
+                                            int s, int blk) {
+  constexpr int SB = kStageB32;
+  const long long poff = p.poff[s];
+  const int ns = p.nreal[s];
+  const int T = (ns + kTile - 1) / kTile;
+  const int t_first = (int)(poff / kTile);
+  const int c0 = 2 * blk;
+  const int ntl = T - c0;                          // column tiles c0 .. T - 1
+  const int rloc = c0 * kTile + lane;              // receiver q = 0 inside the system
+  const long long slot0 = p.rea_off[s] + n3b_prefix(T, blk);
+
+  double xi[8], yi[8], zi[8];
+  u64 AI[4], BI[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    float m0 = 0.f, m1 = 0.f;
+    const int l0 = rloc + 64 * q, l1 = l0 + 32;  // receivers 2q and 2q + 1 of the lane
+    xi[2 * q] = yi[2 * q] = zi[2 * q] = xi[2 * q + 1] = yi[2 * q + 1] = zi[2 * q + 1] = 0.0;
+    if (l0 < ns && NBR_IN(poff + l0, p.len, p.err)) {
+      xi[2 * q] = p.x[poff + l0]; yi[2 * q] = p.y[poff + l0]; zi[2 * q] = p.z[poff + l0];
+      m0 = (float)p.m[poff + l0];
+    }
+    if (l1 < ns && NBR_IN(poff + l1, p.len, p.err)) {
+      xi[2 * q + 1] = p.x[poff + l1]; yi[2 * q + 1] = p.y[poff + l1]; zi[2 * q + 1] = p.z[poff + l1];
+      m1 = (float)p.m[poff + l1];
+    }
+    AI[q] = pack2(-1.5f * m0, -1.5f * m1);
+    BI[q] = pack2(2.5f * m0, 2.5f * m1);
+  }
+  u64 hx[4], hy[4], hz[4], lx[4], ly[4], lz[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) hx[q] = hy[q] = hz[q] = lx[q] = ly[q] = lz[q] = 0ull;
+
+  uint32_t pending = 0;
+  auto issue = [&](int t) {  // lane 0 only
+    if (t == p.skip_tile) return;
+    const unsigned pos = ring.tcount + t;
+    const int st = pos % kBStages;
+    unsigned char* dst = ring.stages + st * SB;
+    const uint32_t bar = smem_u32(&ring.bars[st]);
+    const size_t tile = (size_t)(t_first + c0 + t);
+    if (!NBR_IN((long long)(tile + 1) * kTile - 1, p.len, p.err)) return;  // the wait expires
+    mbar_expect_tx(bar, kStageB32);
+    bulk_g2s(dst, p.rec + tile * kTile * 3, kRec32, bar);
+    bulk_g2s(dst + kRec32, p.org + tile, 32, bar);
+    pending |= 1u << st;
+  };
+  if (lane == 0)
+    for (int t = 0; t < kBStages && t < ntl; ++t) issue(t);
+  bool aborted = false;
+  int t = 0;
+  for (; t < ntl; ++t) {
+    const unsigned pos = ring.tcount + t;
+    const int st = pos % kBStages;
+    const bool ok = mbar_wait_bounded(smem_u32(&ring.bars[st]), (pos / kBStages) & 1u, p.wait_ns);
+    const unsigned char* base = ring.stages + st * SB;
+    const double4 o = *reinterpret_cast<const double4*>(base + kRec32);
+    u64 XI[4], YI[4], ZI[4], AX[4], AY[4], AZ[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      XI[q] = pack2(__double2float_rn(xi[2 * q] - o.x), __double2float_rn(xi[2 * q + 1] - o.x));
+      YI[q] = pack2(__double2float_rn(yi[2 * q] - o.y), __double2float_rn(yi[2 * q + 1] - o.y));
+      ZI[q] = pack2(__double2float_rn(zi[2 * q] - o.z), __double2float_rn(zi[2 * q + 1] - o.z));
+      AX[q] = AY[q] = AZ[q] = 0ull;
+    }
+    if (t < 2) {
+      // the block's own tiles: every ordered pair, action only
+      const ulonglong2* R = reinterpret_cast<const ulonglong2*>(base);
+#pragma unroll 4
+      for (int j = 0; j < kTile; ++j) {
+        const ulonglong2 q0 = R[3 * j];
+        const ulonglong2 q1 = R[3 * j + 1];
+        const u64 bj = R[3 * j + 2].x;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const u64 dx = sub2(q0.x, XI[q]);
+          const u64 dy = sub2(q0.y, YI[q]);
+          const u64 dz = sub2(q1.x, ZI[q]);
+          u64 r2 = fma2(dx, dx, EPS2);
+          r2 = fma2(dy, dy, r2);
+          r2 = fma2(dz, dz, r2);
+          u64 y;
+          if (EXCL) {
+            float rl, rh;
+            unpack2(r2, rl, rh);
+            y = pack2(rl > 0.f ? rsqrt_mufu(rl) : 0.f, rh > 0.f ? rsqrt_mufu(rh) : 0.f);
+          } else {
+            y = rsqrt2(r2);
+          }
+          const u64 y2 = mul2(y, y);
+          const u64 pr = mul2(r2, y2);
+          const u64 mg = fma2(q1.y, pr, bj);
+          const u64 y3 = mul2(y2, y);
+          const u64 sv = mul2(y3, mg);
+          AX[q] = fma2(sv, dx, AX[q]);
+          AY[q] = fma2(sv, dy, AY[q]);
+          AZ[q] = fma2(sv, dz, AZ[q]);
+        }
+      }
+    } else {
+      // a later tile: every pair once; reaction of source j (bt 32 + lane)
+      const float4* R4 = reinterpret_cast<const float4*>(base);
+      const int from = (lane + 31) & 31;
+      double* slot = p.rea + (size_t)(slot0 + (t - 2)) * 3 * kTile;
+#pragma unroll 1
+      for (int bt = 0; bt < 4; ++bt) {
+        const int j = bt * 32 + lane;
+        const float4 q0 = R4[3 * j], q1 = R4[3 * j + 1], q2 = R4[3 * j + 2];
+        float sx = q0.x, sy = q0.z, sz = q1.x, sa = q1.z, sb = q2.x;
+        u64 RX = 0ull, RY = 0ull, RZ = 0ull;
+#pragma unroll 2
+        for (int step = 0; step < 32; ++step) {
+          const u64 SX = pack2(sx, sx), SY = pack2(sy, sy), SZ = pack2(sz, sz);
+          const u64 SA = pack2(sa, sa), SBv = pack2(sb, sb);
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const u64 dx = sub2(SX, XI[q]);
+            const u64 dy = sub2(SY, YI[q]);
+            const u64 dz = sub2(SZ, ZI[q]);
+            u64 r2 = fma2(dx, dx, EPS2);
+            r2 = fma2(dy, dy, r2);
+            r2 = fma2(dz, dz, r2);
+            u64 y;
+            if (EXCL) {
+              float rl, rh;
+              unpack2(r2, rl, rh);
+              y = pack2(rl > 0.f ? rsqrt_mufu(rl) : 0.f, rh > 0.f ? rsqrt_mufu(rh) : 0.f);
+            } else {
+              y = rsqrt2(r2);
+            }
+            const u64 y2 = mul2(y, y);
+            const u64 pr = mul2(r2, y2);
+            const u64 y3 = mul2(y2, y);
+            const u64 sj = mul2(y3, fma2(SA, pr, SBv));       // m_j (1 + 3e/2) y^3
+            const u64 si = mul2(y3, fma2(AI[q], pr, BI[q]));  // m_i (1 + 3e/2) y^3
+            AX[q] = fma2(sj, dx, AX[q]);
+            AY[q] = fma2(sj, dy, AY[q]);
+            AZ[q] = fma2(sj, dz, AZ[q]);
+            RX = fma2(si, dx, RX);
+            RY = fma2(si, dy, RY);
+            RZ = fma2(si, dz, RZ);
+          }
+          sx = __shfl_sync(0xffffffffu, sx, from);
+          sy = __shfl_sync(0xffffffffu, sy, from);
+          sz = __shfl_sync(0xffffffffu, sz, from);
+          sa = __shfl_sync(0xffffffffu, sa, from);
+          sb = __shfl_sync(0xffffffffu, sb, from);
+          RX = __shfl_sync(0xffffffffu, RX, from);
+          RY = __shfl_sync(0xffffffffu, RY, from);
+          RZ = __shfl_sync(0xffffffffu, RZ, from);
+        }
+        // back at its own lane: the acceleration of source j is -sum m_i y^3 d
+        if (NBR_IN((slot - p.rea) + 2 * kTile + j, p.rea_len, p.err)) {
+          float u0, u1;
+          unpack2(RX, u0, u1); slot[j] = -((double)u0 + (double)u1);
+          unpack2(RY, u0, u1); slot[kTile + j] = -((double)u0 + (double)u1);
+          unpack2(RZ, u0, u1); slot[2 * kTile + j] = -((double)u0 + (double)u1);
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      two_sum2(hx[q], lx[q], AX[q]);
+      two_sum2(hy[q], ly[q], AY[q]);
+      two_sum2(hz[q], lz[q], AZ[q]);
+    }
+    __syncwarp();
+    if (__any_sync(0xffffffffu, !ok)) {
+      aborted = true;
+      break;
+    }
+    if (lane == 0) {
+      pending &= ~(1u << st);
+      if (t + kBStages < ntl) issue(t + kBStages);
+    }
+  }
+  if (aborted) {
+    if (lane == 0) {
+      record_error(p.err, kErrTileWait);
+      for (int u = t; u < ntl && u < t + kBStages; ++u) {
+        const unsigned pos = ring.tcount + u;
+        const int st = pos % kBStages;
+        if (!(pending & (1u << st))) continue;
+        if (!mbar_wait_bounded(smem_u32(&ring.bars[st]), (pos / kBStages) & 1u, p.wait_ns)) {
+          record_error(p.err, kErrDrainWait);
+          break;
+        }
+      }
+    }
+    return false;
+  }
+  ring.tcount += ntl;
+  // the block's action, compensated sum hi + lo formed in FP64
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    float h0, h1, l0, l1;
+    const long long i0 = poff + rloc + 64 * q, i1 = i0 + 32;
+    double a0[3], a1[3];
+    unpack2(hx[q], h0, h1); unpack2(lx[q], l0, l1);
+    a0[0] = (double)h0 + (double)l0; a1[0] = (double)h1 + (double)l1;
+    unpack2(hy[q], h0, h1); unpack2(ly[q], l0, l1);
+    a0[1] = (double)h0 + (double)l0; a1[1] = (double)h1 + (double)l1;
+    unpack2(hz[q], h0, h1); unpack2(lz[q], l0, l1);
+    a0[2] = (double)h0 + (double)l0; a1[2] = (double)h1 + (double)l1;
+    if (rloc + 64 * q < ns && NBR_IN(i0, p.len, p.err))
+      for (int d = 0; d < 3; ++d) p.act[(size_t)d * p.n_pad + i0] = a0[d];
+    if (rloc + 64 * q + 32 < ns && NBR_IN(i1, p.len, p.err))
+      for (int d = 0; d < 3; ++d) p.act[(size_t)d * p.n_pad + i1] = a1[d];
+  }
+  __syncwarp();
+  return true;
+}
+// The persistent kernel.  WIDE = 0: every item is narrow (4 receivers per
+// lane); WIDE = 1: items flagged kWideItem cover two tiles (8 receivers per
+// lane: twice the pair work per source read, four independent f32x2 chains);
+// WIDE = 2 (FP32C): items flagged kN3Item are Newton-3 row blocks of systems
+// of three tiles or more (their epilogue runs in k_batch_n3_reduce), the
+// other systems' items as for WIDE = 1.
+template <int PREC, bool EXCL, int WIDE>
 __global__ void __launch_bounds__(kBWarps * 32) k_batch_force(const BatchParams p, const double eps2) {
   constexpr int SB = Stage<PREC>::bytes;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -402,12 +642,97 @@ __global__ void __launch_bounds__(kBWarps * 32) k_batch_force(const BatchParams 
     item = __shfl_sync(0xffffffffu, item, 0);
     if (item >= p.n_items) break;
     const int2 it = p.items[item];
-    const int s = it.x & ~kWideItem;
+    const int s = it.x & ~(kWideItem | kN3Item);
     if (!NBR_IN(s, p.nsys, p.err)) return;
     bool ok;
-    if (WIDE && (it.x & kWideItem)) ok = run_item<PREC, EXCL, 8>(p, eps2, EPS2, ring, lane, s, it.y);
+    if (PREC == kFP32C && WIDE == 2 && (it.x & kN3Item)) ok = run_item_n3<EXCL>(p, EPS2, ring, lane, s, it.y);
+    else if (WIDE >= 1 && (it.x & kWideItem)) ok = run_item<PREC, EXCL, 8>(p, eps2, EPS2, ring, lane, s, it.y);
     else ok = run_item<PREC, EXCL, 4>(p, eps2, EPS2, ring, lane, s, it.y);
     if (!ok) return;
+  }
+}
+
+// The epilogue of the Newton-3 systems: one warp per tile (system, local tile
+// c); each particle's acceleration is its action plus the reactions from the
+// system's row blocks before its own (b = 0 .. c / 2 - 1) in that order:
+// deterministic.  Then the kick/drift and, FP32C, the tile's record pack, as
+// in run_item.
+__global__ void __launch_bounds__(128) k_batch_n3_reduce(const BatchParams p, const int2* tiles,
+                                                         int ntiles) {
+  const int lane = threadIdx.x & 31;
+  const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= ntiles) return;
+  const int2 tc = tiles[w];
+  const int s = tc.x, c = tc.y;
+  const long long poff = p.poff[s];
+  const int ns = p.nreal[s];
+  const int T = (ns + kTile - 1) / kTile;
+  const int B = c / 2;
+  const long long rbase = poff + (long long)c * kTile;
+  const int R = min(kTile, ns - c * kTile);  // real particles of the tile
+  double ax[4], ay[4], az[4], xi[4], yi[4], zi[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int loc = lane + 32 * k;
+    const long long i = rbase + loc;
+    ax[k] = ay[k] = az[k] = xi[k] = yi[k] = zi[k] = 0.0;
+    if (loc >= R || !NBR_IN(i, p.len, p.err)) continue;
+    ax[k] = p.act[i]; ay[k] = p.act[p.n_pad + i]; az[k] = p.act[2 * p.n_pad + i];
+    for (int b = 0; b < B; ++b) {
+      const long long sl = p.rea_off[s] + n3b_prefix(T, b) + (c - 2 * b - 2);
+      const double* r = p.rea + (size_t)sl * 3 * kTile;
+      if (!NBR_IN(sl * 3 * kTile + 2 * kTile + loc, p.rea_len, p.err)) continue;
+      ax[k] += r[loc]; ay[k] += r[kTile + loc]; az[k] += r[2 * kTile + loc];
+    }
+    xi[k] = p.x[i]; yi[k] = p.y[i]; zi[k] = p.z[i];
+  }
+  double px[4], py[4], pz[4];
+  double sx = 0.0, sy = 0.0, sz = 0.0, cnt = 0.0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int loc = lane + 32 * k;
+    const long long i = rbase + loc;
+    px[k] = py[k] = pz[k] = 0.0;
+    if (loc >= R || !NBR_IN(i, p.len, p.err)) continue;
+    const double gx = p.G * ax[k], gy = p.G * ay[k], gz = p.G * az[k];
+    p.ax[i] = gx; p.ay[i] = gy; p.az[i] = gz;
+    if (p.mode == 1) {
+      const double vx = p.vx[i] + p.kick * gx;
+      const double vy = p.vy[i] + p.kick * gy;
+      const double vz = p.vz[i] + p.kick * gz;
+      p.vx[i] = vx; p.vy[i] = vy; p.vz[i] = vz;
+      px[k] = xi[k] + p.drift * vx;
+      py[k] = yi[k] + p.drift * vy;
+      pz[k] = zi[k] + p.drift * vz;
+      p.xn[i] = px[k]; p.yn[i] = py[k]; p.zn[i] = pz[k];
+      sx += px[k]; sy += py[k]; sz += pz[k]; cnt += 1.0;
+    }
+  }
+  if (p.mode != 1 || !p.rec_next || !NBR_IN(rbase + kTile - 1, p.len, p.err)) return;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    sx += __shfl_xor_sync(0xffffffffu, sx, off);
+    sy += __shfl_xor_sync(0xffffffffu, sy, off);
+    sz += __shfl_xor_sync(0xffffffffu, sz, off);
+    cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
+  }
+  const double ox = sx / cnt, oy = sy / cnt, oz = sz / cnt;  // cnt >= 1
+  if (lane == 0) p.org_next[rbase / kTile] = make_double4(ox, oy, oz, 0.0);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int loc = lane + 32 * k;
+    const long long i = rbase + loc;
+    float fx = 0.f, fy = 0.f, fz = 0.f, fa = 0.f, fb = 0.f;
+    if (loc < R) {
+      fx = __double2float_rn(px[k] - ox);
+      fy = __double2float_rn(py[k] - oy);
+      fz = __double2float_rn(pz[k] - oz);
+      fa = __double2float_rn(-1.5 * p.m[i]);
+      fb = __double2float_rn(2.5 * p.m[i]);
+    }
+    p.rec_next[3 * i + 0] = make_float4(fx, fx, fy, fy);
+    p.rec_next[3 * i + 1] = make_float4(fz, fz, fa, fa);
+    p.rec_next[3 * i + 2] = make_float4(fb, fb, 0.f, 0.f);
   }
 }
 
@@ -469,25 +794,31 @@ __global__ void __launch_bounds__(256)
     for (int c = 0; c < 9; ++c) out[(size_t)s * 9 + c] = red[c][0];
 }
 
-template <int PREC, bool EXCL, bool WIDE>
+template <int PREC, bool EXCL, int WIDE>
 const void* batch_fn() {
   return (const void*)k_batch_force<PREC, EXCL, WIDE>;
 }
 
-const void* batch_kernel(int prec, bool excl, bool wide) {
+// wide: 0, 1 or (FP32C) 2 -- the work list the kernel variant takes.
+const void* batch_kernel(int prec, bool excl, int wide) {
   if (prec == kFP32C) {
-    if (excl) return wide ? batch_fn<kFP32C, true, true>() : batch_fn<kFP32C, true, false>();
-    return wide ? batch_fn<kFP32C, false, true>() : batch_fn<kFP32C, false, false>();
+    if (excl)
+      return wide == 2 ? batch_fn<kFP32C, true, 2>()
+             : wide   ? batch_fn<kFP32C, true, 1>()
+                      : batch_fn<kFP32C, true, 0>();
+    return wide == 2 ? batch_fn<kFP32C, false, 2>()
+           : wide   ? batch_fn<kFP32C, false, 1>()
+                    : batch_fn<kFP32C, false, 0>();
   }
-  if (excl) return wide ? batch_fn<kFP64, true, true>() : batch_fn<kFP64, true, false>();
-  return wide ? batch_fn<kFP64, false, true>() : batch_fn<kFP64, false, false>();
+  if (excl) return wide ? batch_fn<kFP64, true, 1>() : batch_fn<kFP64, true, 0>();
+  return wide ? batch_fn<kFP64, false, 1>() : batch_fn<kFP64, false, 0>();
 }
 
 size_t batch_smem(int prec) {
   return kBHead + (size_t)kBWarps * kBStages * (prec == kFP32C ? kStageB32 : kStageB64);
 }
 
-cudaError_t launch_batch(int prec, bool wide, const BatchParams& p, double eps2, int grid,
+cudaError_t launch_batch(int prec, int wide, const BatchParams& p, double eps2, int grid,
                          cudaStream_t st) {
   const void* fn = batch_kernel(prec, eps2 == 0.0, wide);
   const size_t smem = batch_smem(prec);
@@ -507,35 +838,51 @@ std::string batch_key(int prec, size_t nsys, int max_ns, bool excl) {
 
 // The kernel configuration of the batch for a precision: from the autotune
 // cache when it holds this batch's key, else the default (occupancy-limited
-// grid; two-tile items for FP32C, one-tile items for FP64).
+// grid; two-tile items for FP32C, one-tile items for FP64).  The cache stores
+// the work list as ni: 4 one-tile items, 8 two-tile items, 3 Newton-3 row
+// blocks (FP32C).
 void batch_config(nbr_ctx* c, int prec, double eps2) {
   BatchState& b = c->bat;
   const int pi = prec == kFP32C ? 1 : 0;
   if (b.cfg_ok[pi]) return;
   ForceConfig t{0, 0, 0};
-  if (tune_get(batch_key(prec, b.nsys, b.max_ns, eps2 == 0.0), &t) && (t.ni == 4 || t.ni == 8)) {
-    b.wide[pi] = t.ni == 8 ? 1 : 0;
+  if (tune_get(batch_key(prec, b.nsys, b.max_ns, eps2 == 0.0), &t) &&
+      (t.ni == 4 || t.ni == 8 || (t.ni == 3 && prec == kFP32C))) {
+    b.wide[pi] = t.ni == 8 ? 1 : t.ni == 3 ? 2 : 0;
     b.per_sm[pi] = t.split;
   } else {
-    // Defaults from the 4096-system workload on B200: two-tile items lift
-    // FP32C from 1868 to 2029 GPairs/s; FP64 (twice the registers per
-    // receiver) is faster with one-tile items (834 vs 784).
-    b.wide[pi] = prec == kFP32C ? 1 : 0;
+    // Defaults from the 4096-system workload on B200: FP32C 1888 GPairs/s
+    // with one-tile items, 2047 with two-tile items, 2325 with Newton-3 row
+    // blocks for the systems of three tiles or more; FP64 (twice the
+    // registers per receiver) is faster with one-tile items (834 vs 784).
+    b.wide[pi] = prec == kFP32C ? 2 : 0;
     b.per_sm[pi] = 0;
   }
   b.cfg_ok[pi] = true;
 }
 
-// Sets the kernel's shared-memory attribute (once per kernel variant) and
-// returns the persistent grid: resident CTAs per SM (the configured count,
-// at most the occupancy limit) x SMs.  Called before any stream capture.
+// Sets the kernel's shared-memory attribute (once per kernel variant),
+// allocates the Newton-3 scratch at its first use, and returns the
+// persistent grid: resident CTAs per SM (the configured count, at most the
+// occupancy limit) x SMs, or 0 if the scratch allocation failed.  Called
+// before any stream capture.
 int batch_grid(nbr_ctx* c, int prec, double eps2) {
   BatchState& b = c->bat;
   batch_config(c, prec, eps2);
   const int pi = prec == kFP32C ? 1 : 0, ei = eps2 == 0.0 ? 1 : 0, wi = b.wide[pi];
+  if (wi == 2 && b.rea_slots > 0 && !b.d_act) {
+    cudaError_t e = dalloc((void**)&b.d_act, 3 * b.s.n_pad * sizeof(double));
+    if (e == cudaSuccess) e = dalloc((void**)&b.d_rea, (size_t)b.rea_slots * 3 * kTile * sizeof(double));
+    if (e != cudaSuccess) {
+      dfree(b.d_act);
+      dfree(b.d_rea);
+      b.d_act = b.d_rea = nullptr;
+      return 0;
+    }
+  }
   int& occ = b.occ[pi][ei][wi];
   if (occ == 0) {
-    const void* fn = batch_kernel(prec, eps2 == 0.0, wi == 1);
+    const void* fn = batch_kernel(prec, eps2 == 0.0, wi);
     const size_t smem = batch_smem(prec);
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per = 0;
@@ -570,8 +917,10 @@ int batch_eval(nbr_ctx* c, int prec, double G, double eps2, int mode, double kic
   p.x = s.pos[a][0]; p.y = s.pos[a][1]; p.z = s.pos[a][2]; p.m = s.mass;
   p.rec = s.rec[a]; p.org = s.org[a];
   const int grid = batch_grid(c, prec, eps2);  // also settles the configuration
+  if (grid == 0) return fail(c, NBR_ERR_CUDA, "batch Newton-3 scratch allocation");
   const int wi = b.wide[prec == kFP32C ? 1 : 0];
   p.poff = b.d_poff; p.nreal = b.d_nreal; p.items = b.d_items[wi]; p.n_items = b.n_items[wi];
+  p.act = b.d_act; p.rea = b.d_rea; p.rea_off = b.d_rea_off; p.n_pad = (long long)s.n_pad;
   p.head = b.d_head;
   p.mode = mode; p.G = G; p.kick = kick; p.drift = drift;
   p.ax = s.acc[0]; p.ay = s.acc[1]; p.az = s.acc[2];
@@ -584,10 +933,18 @@ int batch_eval(nbr_ctx* c, int prec, double G, double eps2, int mode, double kic
   pipeline_params(js);
   p.wait_ns = js.wait_ns;
   p.skip_tile = js.skip_tile;
-  NBR_CHECKED_ONLY(p.len = (long long)s.cap; p.nsys = (int)b.nsys;)
-  e = launch_batch(prec, wi == 1, p, eps2, grid, c->stream);
+  NBR_CHECKED_ONLY(p.len = (long long)s.cap; p.nsys = (int)b.nsys;
+                   p.rea_len = b.d_rea ? b.rea_slots * 3 * kTile : 0;)
+  e = launch_batch(prec, wi, p, eps2, grid, c->stream);
   if (kernels) ++*kernels;
   if (e != cudaSuccess) return cuda_fail(c, e, "batch force launch");
+  if (wi == 2 && b.n_n3_tiles > 0) {
+    const unsigned blocks = (unsigned)((b.n_n3_tiles + 3) / 4);
+    k_batch_n3_reduce<<<blocks, 128, 0, c->stream>>>(p, b.d_n3_tiles, b.n_n3_tiles);
+    e = cudaGetLastError();
+    if (kernels) ++*kernels;
+    if (e != cudaSuccess) return cuda_fail(c, e, "batch Newton-3 epilogue launch");
+  }
   if (mode == 1) {
     s.cur = o;
     s.rec_ok[o] = (prec == kFP32C);
@@ -605,6 +962,11 @@ void nbr::BatchState::release() {
   dfree(d_sys_of_tile);
   dfree(d_items[0]);
   dfree(d_items[1]);
+  dfree(d_items[2]);
+  dfree(d_n3_tiles);
+  dfree(d_rea_off);
+  dfree(d_act);
+  dfree(d_rea);
   dfree(d_head);
   dfree(d_red);
   *this = BatchState();
@@ -622,7 +984,7 @@ int nbr_batch_upload(nbr_ctx* c, size_t nsys, const size_t* offsets, const doubl
   if ((vx || vy || vz) && !(vx && vy && vz))
     return fail(c, NBR_ERR_INVALID_ARG, "velocities must be all given or all NULL");
   if (offsets[0] != 0) return fail(c, NBR_ERR_INVALID_ARG, "offsets[0] must be 0");
-  if (nsys >= (size_t)kWideItem) return fail(c, NBR_ERR_INVALID_ARG, "too many systems");
+  if (nsys >= (size_t)kN3Item) return fail(c, NBR_ERR_INVALID_ARG, "too many systems");
   for (size_t s = 0; s < nsys; ++s) {
     if (offsets[s + 1] <= offsets[s]) return fail(c, NBR_ERR_INVALID_ARG, "every system needs >= 1 particle");
     if (offsets[s + 1] - offsets[s] > (size_t)1 << 30) return fail(c, NBR_ERR_INVALID_ARG, "system too large");
@@ -677,17 +1039,34 @@ int nbr_batch_upload(nbr_ctx* c, size_t nsys, const size_t* offsets, const doubl
   }
   // Work items ordered by cost (receiver slots x system size), largest first:
   // list 0 with one-tile items only, list 1 pairing a system's tiles into
-  // two-tile items (a system's odd last tile stays a one-tile item).
-  std::vector<int2> lists[2];
-  for (int wl = 0; wl < 2; ++wl) {
+  // two-tile items (a system's odd last tile stays a one-tile item), list 2
+  // with Newton-3 row blocks for the systems of three tiles or more (cost: the
+  // own two tiles' ordered pairs, and each later tile's pairs at the
+  // rotation's ~1.5x the work per pair) and list 1's items for the rest.
+  std::vector<int2> lists[3];
+  std::vector<int2> n3_tiles;
+  std::vector<long long> rea_off(nsys, -1);
+  long long slots = 0;
+  for (int wl = 0; wl < 3; ++wl) {
     std::vector<int2> items;
     std::vector<double> cost;
     for (size_t s = 0; s < nsys; ++s) {
       const long long ns = (long long)(offsets[s + 1] - offsets[s]);
       const long long nt = (ns + kTile - 1) / kTile;
+      if (wl == 2 && nt >= 3) {
+        rea_off[s] = slots;
+        for (long long blk = 0; 2 * blk < nt; ++blk) {
+          const long long later = std::max<long long>(0, nt - 2 * blk - 2);
+          slots += later;
+          items.push_back(make_int2((int)s | kN3Item, (int)blk));
+          cost.push_back(2.0 * kTile * (std::min<long long>(2, nt - 2 * blk) + 1.5 * later) * kTile);
+        }
+        for (long long t = 0; t < nt; ++t) n3_tiles.push_back(make_int2((int)s, (int)t));
+        continue;
+      }
       for (long long t = 0; t < nt;) {
         const int tile = (int)(b.poff[s] / kTile + t);
-        if (wl == 1 && t + 1 < nt) {
+        if (wl >= 1 && t + 1 < nt) {
           items.push_back(make_int2((int)s | kWideItem, tile));
           cost.push_back(2.0 * kTile * double(ns));
           t += 2;
@@ -714,8 +1093,13 @@ int nbr_batch_upload(nbr_ctx* c, size_t nsys, const size_t* offsets, const doubl
   }
   e = dalloc((void**)&b.d_poff, (nsys + 1) * sizeof(long long));
   if (e == cudaSuccess) e = dalloc((void**)&b.d_nreal, nsys * sizeof(int));
-  for (int wl = 0; wl < 2 && e == cudaSuccess; ++wl)
+  for (int wl = 0; wl < 3 && e == cudaSuccess; ++wl)
     e = dalloc((void**)&b.d_items[wl], lists[wl].size() * sizeof(int2));
+  b.n_n3_tiles = (int)n3_tiles.size();
+  b.rea_slots = slots;
+  if (e == cudaSuccess && !n3_tiles.empty())
+    e = dalloc((void**)&b.d_n3_tiles, n3_tiles.size() * sizeof(int2));
+  if (e == cudaSuccess) e = dalloc((void**)&b.d_rea_off, nsys * sizeof(long long));
   if (e == cudaSuccess) e = dalloc((void**)&b.d_head, 256);
   if (e == cudaSuccess) e = dalloc((void**)&b.d_red, nsys * 9 * sizeof(double));
   if (e == cudaSuccess)
@@ -723,8 +1107,14 @@ int nbr_batch_upload(nbr_ctx* c, size_t nsys, const size_t* offsets, const doubl
                         cudaMemcpyHostToDevice, c->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(b.d_nreal, nreal.data(), nsys * sizeof(int), cudaMemcpyHostToDevice, c->stream);
-  for (int wl = 0; wl < 2 && e == cudaSuccess; ++wl)
+  for (int wl = 0; wl < 3 && e == cudaSuccess; ++wl)
     e = cudaMemcpyAsync(b.d_items[wl], lists[wl].data(), lists[wl].size() * sizeof(int2),
+                        cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess && !n3_tiles.empty())
+    e = cudaMemcpyAsync(b.d_n3_tiles, n3_tiles.data(), n3_tiles.size() * sizeof(int2),
+                        cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b.d_rea_off, rea_off.data(), nsys * sizeof(long long),
                         cudaMemcpyHostToDevice, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) {
@@ -900,8 +1290,10 @@ int nbr_batch_set_config(nbr_ctx* c, int precision, int wide, int ctas_per_sm) {
   if (!c) return fail(nullptr, NBR_ERR_INVALID_ARG, "ctx is NULL");
   if (precision != NBR_FP64 && precision != NBR_FP32C)
     return fail(c, NBR_ERR_INVALID_ARG, "unknown precision");
-  if (wide < -1 || wide > 1 || ctas_per_sm < 0)
-    return fail(c, NBR_ERR_INVALID_ARG, "wide must be -1, 0 or 1 and ctas_per_sm >= 0");
+  if (wide < -1 || wide > 2 || ctas_per_sm < 0)
+    return fail(c, NBR_ERR_INVALID_ARG, "wide must be -1, 0, 1 or 2 and ctas_per_sm >= 0");
+  if (wide == 2 && precision != NBR_FP32C)
+    return fail(c, NBR_ERR_INVALID_ARG, "Newton-3 row blocks (wide = 2) are FP32C only");
   BatchState& b = c->bat;
   const int pi = precision == kFP32C ? 1 : 0;
   if (wide < 0) {
@@ -926,11 +1318,11 @@ int nbr_batch_autotune(nbr_ctx* c, int precision, double eps2) {
   const int pi = precision == kFP32C ? 1 : 0;
   int best_w = -1, best_p = 0;
   float best_ms = 1e30f;
-  for (int w = 0; w < 2; ++w) {
+  for (int w = 0; w < (precision == kFP32C ? 3 : 2); ++w) {
     b.wide[pi] = w;
     b.per_sm[pi] = 0;
     b.cfg_ok[pi] = true;
-    batch_grid(c, precision, eps2);
+    if (batch_grid(c, precision, eps2) == 0) continue;
     const int occ = b.occ[pi][eps2 == 0.0 ? 1 : 0][w];
     for (int per = 1; per <= occ; ++per) {
       b.per_sm[pi] = per;
@@ -961,7 +1353,7 @@ int nbr_batch_autotune(nbr_ctx* c, int precision, double eps2) {
   b.per_sm[pi] = best_p;
   b.cfg_ok[pi] = true;
   tune_put(batch_key(precision, b.nsys, b.max_ns, eps2 == 0.0),
-           ForceConfig{best_w ? 8 : 4, kBWarps, best_p});
+           ForceConfig{best_w == 2 ? 3 : best_w ? 8 : 4, kBWarps, best_p});
   return NBR_OK;
 }
 

@@ -67,9 +67,20 @@ struct BatchState {
   int* d_sys_of_tile = nullptr;      // system index of every padded tile
   // Work queues of (system | kWideItem flag, first receiver tile), cost
   // ordered: [0] one-tile items only, [1] two-tile items where a system has
-  // two tiles left.
-  int2* d_items[2] = {nullptr, nullptr};
-  int n_items[2] = {0, 0};
+  // two tiles left, [2] (FP32C) Newton-3 row blocks (system | kN3Item, block)
+  // of the systems of three tiles or more, the others' items as in [1].
+  int2* d_items[3] = {nullptr, nullptr, nullptr};
+  int n_items[3] = {0, 0, 0};
+  // Newton-3 systems: their tiles (system, local tile) for the epilogue
+  // kernel, each system's first reaction slot (-1: none), the slot count, and
+  // the scratch (allocated at first use): action [3][n_pad], reactions
+  // [slots][3][128].
+  int2* d_n3_tiles = nullptr;
+  int n_n3_tiles = 0;
+  long long* d_rea_off = nullptr;
+  long long rea_slots = 0;
+  double* d_act = nullptr;
+  double* d_rea = nullptr;
   int max_ns = 0;                    // largest system
   unsigned* d_head = nullptr;        // work-queue heads
   double* d_red = nullptr;           // per-system diagnostic sums
@@ -83,7 +94,7 @@ struct BatchState {
   bool cfg_ok[2] = {false, false};
   int wide[2] = {1, 1};
   int per_sm[2] = {0, 0};
-  int occ[2][2][2] = {};              // occupancy limit per (precision, eps == 0, wide)
+  int occ[2][2][3] = {};              // occupancy limit per (precision, eps == 0, wide)
 
   void release();
 };

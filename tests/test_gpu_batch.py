@@ -33,8 +33,12 @@ def system(st, off, s):
     return {k: st[k][off[s]:off[s + 1]] for k in st}
 
 
-@pytest.mark.parametrize("wide", [0, 1], ids=["one-tile", "two-tile"])
-@pytest.mark.parametrize("prec", [FP64, FP32C])
+# work lists: one-tile items, two-tile items, Newton-3 row blocks (FP32C)
+WORK = [(FP64, 0), (FP64, 1), (FP32C, 0), (FP32C, 1), (FP32C, 2)]
+WORK_IDS = ["fp64-one-tile", "fp64-two-tile", "fp32c-one-tile", "fp32c-two-tile", "fp32c-newton3"]
+
+
+@pytest.mark.parametrize("prec,wide", WORK, ids=WORK_IDS)
 def test_batch_forces_match_oracle(ctx, nbr, oracle, prec, wide):
     off, st = make_batch(nbr, SIZES)
     ctx.batch_upload(off, st)
@@ -58,6 +62,40 @@ def test_batch_forces_match_oracle(ctx, nbr, oracle, prec, wide):
         assert np.median(allerr) <= 1e-6 and allerr.max() <= 1e-4
 
 
+@pytest.mark.parametrize("eps2", [1e-6, 0.0])
+def test_batch_newton3_row_blocks(ctx, nbr, oracle, eps2):
+    """The Newton-3 work list on systems of 3 to 17 tiles (odd and even tile
+    counts, ragged last tiles) beside small systems that keep two-tile items:
+    every particle against the oracle, the run repeated bit for bit (the
+    reactions are summed in a fixed order), and equal to the two-tile list
+    to FP32C accuracy."""
+    sizes = [5, 129, 257, 300, 384, 385, 640, 1000, 2049, 2100]
+    off, st = make_batch(nbr, sizes, seed=21)
+    ctx.batch_upload(off, st)
+    ctx.batch_set_config(FP32C, 2, 0)
+    a = ctx.batch_forces(FP32C, eps2=eps2)
+    b = ctx.batch_forces(FP32C, eps2=eps2)
+    np.testing.assert_array_equal(a, b)
+    errs = []
+    for s, n in enumerate(sizes):
+        sub = system(st, off, s)
+        ref = oracle.accel(sub["x"], sub["y"], sub["z"], sub["m"], eps2=eps2, extended=True)
+        e = rel_err(a[:, off[s]:off[s + 1]], ref)
+        assert np.median(e) <= 1e-6, (n, np.median(e))
+        errs.append(e)
+    assert np.concatenate(errs).max() <= 1e-4
+    ctx.batch_set_config(FP32C, 1, 0)
+    w = ctx.batch_forces(FP32C, eps2=eps2)
+    assert rel_err(a, w).max() <= 1e-4
+
+
+def test_batch_newton3_is_fp32c_only(ctx, nbr):
+    off, st = make_batch(nbr, [300, 400])
+    ctx.batch_upload(off, st)
+    with pytest.raises(nbr.NbrError):
+        ctx.batch_set_config(FP64, 2, 0)
+
+
 def test_batch_systems_do_not_interact(ctx, nbr):
     """Two copies of one system at the same place: each feels only itself."""
     s1 = nbr.plummer(300, 1)
@@ -71,8 +109,7 @@ def test_batch_systems_do_not_interact(ctx, nbr):
     assert rel_err(a[:, :300], single).max() <= 1e-13
 
 
-@pytest.mark.parametrize("wide", [0, 1], ids=["one-tile", "two-tile"])
-@pytest.mark.parametrize("prec", [FP64, FP32C])
+@pytest.mark.parametrize("prec,wide", WORK, ids=WORK_IDS)
 def test_batch_kdk_matches_oracle(ctx, nbr, oracle, prec, wide):
     sizes = [64, 130, 513, 1000]
     off, st = make_batch(nbr, sizes, seed=9)
@@ -117,11 +154,13 @@ def test_batch_diagnostics(ctx, nbr, oracle):
         assert abs(d[s]["M"] - e["M"]) <= 1e-14
 
 
-def test_batch_full_workload(ctx, nbr, oracle):
+@pytest.mark.parametrize("wide", [1, 2], ids=["two-tile", "newton3"])
+def test_batch_full_workload(ctx, nbr, oracle, wide):
     """The 4096-system log-uniform workload: two FP32C steps; sampled systems
     checked against the oracle; pair count as the workload defines it."""
     off, st = nbr.batch_plummer(4096, 3)
     ctx.batch_upload(off, st)
+    ctx.batch_set_config(FP32C, wide, 0)
     eps2 = 1e-6
     a = ctx.batch_forces(FP32C, eps2=eps2)
     rng = np.random.default_rng(1)
@@ -134,10 +173,15 @@ def test_batch_full_workload(ctx, nbr, oracle):
     assert stats["pairs"] == 2 * float((sizes * (sizes - 1)).sum())
 
 
-def test_batch_bounded_wait_expires_cleanly(nbr):
+@pytest.mark.parametrize("wide", [1, 2], ids=["two-tile", "newton3"])
+def test_batch_bounded_wait_expires_cleanly(nbr, wide):
+    """Tile 2 of every item never arrives (a test hook; for a Newton-3 row
+    block, its first later column tile): the wait gives up, the call reports
+    NBR_ERR_TIMEOUT and the context keeps working."""
     off, st = make_batch(nbr, [700, 900], seed=2)
     with nbr.Context(0) as c:
         c.batch_upload(off, st)
+        c.batch_set_config(FP32C, wide, 0)
         os.environ["NBR_WAIT_LIMIT_MS"] = "100"
         os.environ["NBR_TEST_SKIP_TILE"] = "2"
         try:
