@@ -678,13 +678,25 @@ __global__ void __launch_bounds__(128) k_batch_n3_reduce(const BatchParams p, co
     ax[k] = ay[k] = az[k] = xi[k] = yi[k] = zi[k] = 0.0;
     if (loc >= R || !NBR_IN(i, p.len, p.err)) continue;
     ax[k] = p.act[i]; ay[k] = p.act[p.n_pad + i]; az[k] = p.act[2 * p.n_pad + i];
-    for (int b = 0; b < B; ++b) {
-      const long long sl = p.rea_off[s] + n3b_prefix(T, b) + (c - 2 * b - 2);
-      const double* r = p.rea + (size_t)sl * 3 * kTile;
-      if (!NBR_IN(sl * 3 * kTile + 2 * kTile + loc, p.rea_len, p.err)) continue;
-      ax[k] += r[loc]; ay[k] += r[kTile + loc]; az[k] += r[2 * kTile + loc];
-    }
     xi[k] = p.x[i]; yi[k] = p.y[i]; zi[k] = p.z[i];
+  }
+  // The reaction slots in block order; the 12 loads of a slot (every slot
+  // entry is written, padding included) are issued before its adds.
+  const long long slot_b0 = p.rea_off[s] + (c - 2);
+#pragma unroll 2
+  for (int b = 0; b < B; ++b) {
+    const long long sl = slot_b0 + n3b_prefix(T, b) - 2 * b;
+    if (!NBR_IN((sl + 1) * 3 * kTile - 1, p.rea_len, p.err)) break;
+    const double* r = p.rea + (size_t)sl * 3 * kTile + lane;
+    double tx[4], ty[4], tz[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      tx[k] = r[32 * k]; ty[k] = r[kTile + 32 * k]; tz[k] = r[2 * kTile + 32 * k];
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      ax[k] += tx[k]; ay[k] += ty[k]; az[k] += tz[k];
+    }
   }
   double px[4], py[4], pz[4];
   double sx = 0.0, sy = 0.0, sz = 0.0, cnt = 0.0;

@@ -676,8 +676,10 @@ __global__ void __launch_bounds__(kSmallWarps * 32)
 // Results leave as FP64 partial sums: per (CTA, row block) the action, per
 // (CTA, column block) the reaction (summed over the CTA's warps in warp
 // order); k_n3_reduce adds them per particle in a fixed order and runs the
-// epilogue.  Deterministic.
-template <bool EXCL>
+// epilogue.  Deterministic.  RANGED: the launch covers the row groups
+// [p3.g0, p3.g1) (a slice); otherwise all of them (a separate instantiation,
+// the whole-system launch keeps its own code).
+template <bool EXCL, bool RANGED>
 __global__ void __launch_bounds__(kN3Warps * 32)
     k_force_n3_f32c(const IParticles ip, const JStream js, const N3Params p3, const float eps2f,
                     int* err) {
@@ -687,8 +689,9 @@ __global__ void __launch_bounds__(kN3Warps * 32)
   unsigned char* stages = smem + kSmemHead;
   float* red = reinterpret_cast<float*>(stages + kStages * kStage32);  // [warp][3][256]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int g = p3.g0, k = blockIdx.x;
-  const int groups = p3.g1;  // row groups [g0, g1) of this launch
+  int g = RANGED ? p3.g0 : 0, k = blockIdx.x;
+  // row groups [g0, g1) of this launch
+  const int groups = RANGED ? p3.g1 : (int)((p3.nb + kN3Warps - 1) / kN3Warps);
   while (g < groups) {  // the grid has exactly sum_g n3_chunks(nb, cols, g) CTAs
     const int K = n3_chunks(p3.nb, p3.cols, g);
     if (k < K) break;
@@ -1722,7 +1725,7 @@ int force_blocks_per_sm(int precision, double eps2, const ForceConfig& c) {
     const bool w2 = precision == kFP32C && c.warps == kN3F64Warps;
     const void* fn = precision == kFP32C
                          ? (w2 ? (ex ? (const void*)k_force_n3_f32c_w2<true> : (const void*)k_force_n3_f32c_w2<false>)
-                               : (ex ? (const void*)k_force_n3_f32c<true> : (const void*)k_force_n3_f32c<false>))
+                               : (ex ? (const void*)k_force_n3_f32c<true, false> : (const void*)k_force_n3_f32c<false, false>))
                          : (ex ? (const void*)k_force_n3_f64<true> : (const void*)k_force_n3_f64<false>);
     const int threads = (precision == kFP32C && !w2 ? kN3Warps : kN3F64Warps) * 32;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, threads, n3_smem_bytes(precision, c.warps)) !=
@@ -1784,8 +1787,10 @@ cudaError_t configure_kernels() {
   const int s32 = (int)n3_smem_bytes(kFP32C, kN3Warps), s64 = (int)n3_smem_bytes(kFP64, kN3F64Warps);
   const int s32w = (int)n3_smem_bytes(kFP32C, kN3F64Warps);
   const cudaFuncAttribute at = cudaFuncAttributeMaxDynamicSharedMemorySize;
-  cudaError_t e = cudaFuncSetAttribute((const void*)k_force_n3_f32c<true>, at, s32);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute((const void*)k_force_n3_f32c<false>, at, s32);
+  cudaError_t e = cudaFuncSetAttribute((const void*)k_force_n3_f32c<true, false>, at, s32);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute((const void*)k_force_n3_f32c<false, false>, at, s32);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute((const void*)k_force_n3_f32c<true, true>, at, s32);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute((const void*)k_force_n3_f32c<false, true>, at, s32);
   if (e == cudaSuccess) e = cudaFuncSetAttribute((const void*)k_force_n3_f32c_w2<true>, at, s32w);
   if (e == cudaSuccess) e = cudaFuncSetAttribute((const void*)k_force_n3_f32c_w2<false>, at, s32w);
   if (e == cudaSuccess) e = cudaFuncSetAttribute((const void*)k_force_n3_f64<true>, at, s64);
@@ -1828,9 +1833,9 @@ cudaError_t launch_force_n3(int precision, int warps, double eps2, const IPartic
       k_force_n3_f32c_w2<false><<<grid, block, smem, st>>>(ip, js, p3, (float)eps2, ep.err);
   } else if (precision == kFP32C) {
     if (eps2 == 0.0)
-      k_force_n3_f32c<true><<<grid, block, smem, st>>>(ip, js, p3, 0.f, ep.err);
+      k_force_n3_f32c<true, false><<<grid, block, smem, st>>>(ip, js, p3, 0.f, ep.err);
     else
-      k_force_n3_f32c<false><<<grid, block, smem, st>>>(ip, js, p3, (float)eps2, ep.err);
+      k_force_n3_f32c<false, false><<<grid, block, smem, st>>>(ip, js, p3, (float)eps2, ep.err);
   } else {
     if (eps2 == 0.0)
       k_force_n3_f64<true><<<grid, block, smem, st>>>(ip, js, p3, 0.0, ep.err);
@@ -1859,8 +1864,8 @@ cudaError_t launch_n3_pairs(int precision, int warps, double eps2, const IPartic
     if (eps2 == 0.0) k_force_n3_f32c_w2<true><<<grid, block, smem, st>>>(ip, js, p3, 0.f, err);
     else k_force_n3_f32c_w2<false><<<grid, block, smem, st>>>(ip, js, p3, e32, err);
   } else if (precision == kFP32C) {
-    if (eps2 == 0.0) k_force_n3_f32c<true><<<grid, block, smem, st>>>(ip, js, p3, 0.f, err);
-    else k_force_n3_f32c<false><<<grid, block, smem, st>>>(ip, js, p3, e32, err);
+    if (eps2 == 0.0) k_force_n3_f32c<true, true><<<grid, block, smem, st>>>(ip, js, p3, 0.f, err);
+    else k_force_n3_f32c<false, true><<<grid, block, smem, st>>>(ip, js, p3, e32, err);
   } else {
     if (eps2 == 0.0) k_force_n3_f64<true><<<grid, block, smem, st>>>(ip, js, p3, 0.0, err);
     else k_force_n3_f64<false><<<grid, block, smem, st>>>(ip, js, p3, eps2, err);
