@@ -384,16 +384,17 @@ int nbr_batch_run(nbr_ctx* ctx, int precision, double dt, size_t steps, double G
                   nbr_run_stats* stats);
 /* Forces the batched kernel's configuration for a precision: wide = 1 pairs a
  * system's receiver tiles into two-tile work items (8 receivers per lane),
- * wide = 0 keeps one-tile items (4 per lane), wide = 2 (FP32C only; else
- * NBR_ERR_INVALID_ARG) evaluates every system of three tiles (257 particles)
- * or more by Newton-3 row blocks -- two receiver tiles against the later
- * column tiles, each pair once -- and the others as for wide = 1;
- * ctas_per_sm = resident CTAs per SM of the persistent grid (0: the
+ * wide = 0 keeps one-tile items (4 per lane), wide = 2 evaluates the larger
+ * systems by Newton-3 row blocks -- receiver tiles against the later column
+ * tiles, each pair once: FP32C two-tile blocks for systems of three tiles
+ * (257 particles) or more, the others as for wide = 1; FP64 one-tile blocks
+ * for systems of two tiles (129 particles) or more, the others as for
+ * wide = 0; ctas_per_sm = resident CTAs per SM of the persistent grid (0: the
  * occupancy limit).  wide = -1 restores the autotune cache or the default
- * (occupancy limit; Newton-3 row blocks for FP32C, one-tile items for FP64).
- * Applies to the uploaded batch; an upload starts from the autotune cache
- * again.  The Newton-3 scratch (3 doubles per particle and 3 x 128 doubles
- * per (row block, later column tile)) is allocated at its first use. */
+ * (occupancy limit; Newton-3 row blocks).  Applies to the uploaded batch; an
+ * upload starts from the autotune cache again.  The Newton-3 scratch (3
+ * doubles per particle and 3 x 128 doubles per (row block, later column
+ * tile)) is allocated at its first use.  Other values: NBR_ERR_INVALID_ARG. */
 int nbr_batch_set_config(nbr_ctx* ctx, int precision, int wide, int ctas_per_sm);
 /* Times every (item width, CTAs per SM) on the uploaded batch and stores the
  * fastest in the autotune cache under the batch's (precision, log2 system

@@ -21,6 +21,16 @@
 // last tile are skipped (the loop stops at the tile's real count rounded up to
 // 4), so padding costs ~1 % of the pair work on the log-uniform workload.
 //
+// Newton-3 row blocks (the default work list): a system large enough is
+// split into row blocks of R receiver tiles (FP32C R = 2, 8 receivers per
+// lane; FP64 R = 1, 4 per lane), each an item that walks the column tiles
+// from its own: its own tiles with every ordered pair, every later tile with
+// each pair once, the sources rotating through the warp by shuffles with
+// their reaction sums.  The action goes to a per-particle array, each
+// (row block, later tile) reaction to its own slot; k_batch_n3_reduce then
+// adds every particle's action and reactions in a fixed order and runs the
+// epilogue: deterministic, no atomics.
+//
 // Pair arithmetic and accumulation are those of the single-system kernels
 // (nbr_kernels.cu): FP32C f32x2 pairs with TwoSum-compensated tile sums, or
 // FP64.  The epilogue applies the KDK kick/drift and packs the FP32C records of
@@ -47,7 +57,7 @@ constexpr int kStageB32 = kRec32 + 32;        // + origin
 constexpr int kStageB64 = 4 * kTile * 8;      // FP64 x, y, z, m
 constexpr int kBHead = 128;                   // barriers: kBWarps * kBStages * 8 <= 128
 constexpr int kWideItem = 1 << 30;            // item flag: two receiver tiles
-constexpr int kN3Item = 1 << 29;              // item flag: a Newton-3 row block (FP32C)
+constexpr int kN3Item = 1 << 29;              // item flag: a Newton-3 row block
 
 struct BatchParams {
   const double* x; const double* y; const double* z; const double* m;  // current buffer
@@ -68,20 +78,23 @@ struct BatchParams {
   int skip_tile;
   // Newton-3 items: the action of every particle [3][n_pad], the reaction
   // partials (one 3 x 128 slot per (row block, later column tile) of a
-  // system), and each system's first slot (-1: the system has no N3 items)
+  // system), each system's first slot (-1: the system has no N3 items), and
+  // the tiles per row block (FP32C 2, FP64 1)
   double* act;
   double* rea;
   const long long* rea_off;
   long long n_pad;
+  int n3_rows;
   NBR_CHECKED_FIELD(long long len)  // entries allocated in the particle arrays
   NBR_CHECKED_FIELD(int nsys)
   NBR_CHECKED_FIELD(long long rea_len)  // doubles allocated in rea
 };
 
-// Reaction slots before row block b of a system of T tiles: row block b' has
-// T - 2 b' - 2 later column tiles (every b' < b has at least one).
-__host__ __device__ inline long long n3b_prefix(int T, int b) {
-  return (long long)b * (T - 2) - (long long)b * (b - 1);
+// Reaction slots before row block b of a system of T tiles, with `rows` tiles
+// per row block: row block b' has T - rows (b' + 1) later column tiles (every
+// b' < b has at least one).
+__host__ __device__ inline long long n3b_prefix(int T, int b, int rows) {
+  return (long long)b * (T - rows) - (long long)rows * b * (b - 1) / 2;
 }
 
 template <int P>
@@ -411,7 +424,7 @@ __device__ __forceinline__ bool run_item_n3(const BatchParams& p, u64 EPS2, Ring
   const int c0 = 2 * blk;
   const int ntl = T - c0;                          // column tiles c0 .. T - 1
   const int rloc = c0 * kTile + lane;              // receiver q = 0 inside the system
-  const long long slot0 = p.rea_off[s] + n3b_prefix(T, blk);
+  const long long slot0 = p.rea_off[s] + n3b_prefix(T, blk, 2);
 
   double xi[8], yi[8], zi[8];
   u64 AI[4], BI[4];
@@ -506,9 +519,15 @@ __device__ __forceinline__ bool run_item_n3(const BatchParams& p, u64 EPS2, Ring
       const float4* R4 = reinterpret_cast<const float4*>(base);
       const int from = (lane + 31) & 31;
       double* slot = p.rea + (size_t)(slot0 + (t - 2)) * 3 * kTile;
+      const int nsrc = min(kTile, ns - (c0 + t) * kTile);  // real sources of the tile
 #pragma unroll 1
       for (int bt = 0; bt < 4; ++bt) {
         const int j = bt * 32 + lane;
+        if (bt * 32 >= nsrc) {  // a batch of padding: no pairs, zero reactions
+          if (NBR_IN((slot - p.rea) + 2 * kTile + j, p.rea_len, p.err))
+            slot[j] = slot[kTile + j] = slot[2 * kTile + j] = 0.0;
+          continue;
+        }
         const float4 q0 = R4[3 * j], q1 = R4[3 * j + 1], q2 = R4[3 * j + 2];
         float sx = q0.x, sy = q0.z, sz = q1.x, sa = q1.z, sb = q2.x;
         u64 RX = 0ull, RY = 0ull, RZ = 0ull;
@@ -614,12 +633,168 @@ __device__ __forceinline__ bool run_item_n3(const BatchParams& p, u64 EPS2, Ring
   __syncwarp();
   return true;
 }
+// One Newton-3 item (FP64): row tile r of system s -- 128 receivers, 4 per
+// lane (lane + 32 k) -- against the system's column tiles c >= r.  Its own
+// tile: every ordered pair, action only (tile_f64).  Each later tile c: every
+// pair once, the tile's sources in batches of 32, one per lane, rotating
+// through the warp by shuffles with their reaction sums (the scheme of
+// k_force_n3_f64); batches of padding are skipped.  The reaction of tile c
+// goes to its slot, the action to p.act; the epilogue runs in
+// k_batch_n3_reduce.  Returns false if a tile wait gave up.
+template <bool EXCL>
+__device__ __forceinline__ bool run_item_n3_f64(const BatchParams& p, double eps2, Ring& ring,
+                                                int lane, int s, int r) {
+  constexpr int SB = kStageB64;
+  const long long poff = p.poff[s];
+  const int ns = p.nreal[s];
+  const int T = (ns + kTile - 1) / kTile;
+  const int t_first = (int)(poff / kTile);
+  const int ntl = T - r;                 // column tiles r .. T - 1
+  const int rloc = r * kTile + lane;     // receiver k = 0 inside the system
+  const long long slot0 = p.rea_off[s] + n3b_prefix(T, r, 1);
+  const int last_cnt = ((ns - (T - 1) * kTile) + 3) & ~3;  // real sources of the last tile, to 4
+
+  double xi[4], yi[4], zi[4], mi[4], ax[4], ay[4], az[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int l = rloc + 32 * k;
+    xi[k] = yi[k] = zi[k] = mi[k] = ax[k] = ay[k] = az[k] = 0.0;
+    if (l < ns && NBR_IN(poff + l, p.len, p.err)) {
+      xi[k] = p.x[poff + l]; yi[k] = p.y[poff + l]; zi[k] = p.z[poff + l]; mi[k] = p.m[poff + l];
+    }
+  }
+
+  uint32_t pending = 0;
+  auto issue = [&](int t) {  // lane 0 only
+    if (t == p.skip_tile) return;
+    const unsigned pos = ring.tcount + t;
+    const int st = pos % kBStages;
+    unsigned char* dst = ring.stages + st * SB;
+    const uint32_t bar = smem_u32(&ring.bars[st]);
+    const size_t tile = (size_t)(t_first + r + t);
+    if (!NBR_IN((long long)(tile + 1) * kTile - 1, p.len, p.err)) return;  // the wait expires
+    mbar_expect_tx(bar, kStageB64);
+    const size_t off = tile * kTile;
+    bulk_g2s(dst, p.x + off, kTile * 8, bar);
+    bulk_g2s(dst + kTile * 8, p.y + off, kTile * 8, bar);
+    bulk_g2s(dst + 2 * kTile * 8, p.z + off, kTile * 8, bar);
+    bulk_g2s(dst + 3 * kTile * 8, p.m + off, kTile * 8, bar);
+    pending |= 1u << st;
+  };
+  if (lane == 0)
+    for (int t = 0; t < kBStages && t < ntl; ++t) issue(t);
+  bool aborted = false;
+  int t = 0;
+  for (; t < ntl; ++t) {
+    const unsigned pos = ring.tcount + t;
+    const int st = pos % kBStages;
+    const bool ok = mbar_wait_bounded(smem_u32(&ring.bars[st]), (pos / kBStages) & 1u, p.wait_ns);
+    const unsigned char* base = ring.stages + st * SB;
+    const int c = r + t;
+    if (t == 0) {
+      // the own tile: every ordered pair, action only
+      const int jend = (c == T - 1) ? last_cnt : kTile;
+      if (jend == kTile) tile_f64<EXCL, true, 4>(base, 0, 1, kTile, xi, yi, zi, eps2, ax, ay, az);
+      else tile_f64<EXCL, false, 4>(base, 0, 1, jend, xi, yi, zi, eps2, ax, ay, az);
+    } else {
+      const double* SX = reinterpret_cast<const double*>(base);
+      const double* SY = SX + kTile;
+      const double* SZ = SY + kTile;
+      const double* SM = SZ + kTile;
+      const int from = (lane + 31) & 31;
+      double* slot = p.rea + (size_t)(slot0 + (t - 1)) * 3 * kTile;
+      const int nsrc = min(kTile, ns - c * kTile);  // real sources of the tile
+#pragma unroll 1
+      for (int bt = 0; bt < 4; ++bt) {
+        const int j = bt * 32 + lane;
+        const bool in = NBR_IN((slot - p.rea) + 2 * kTile + j, p.rea_len, p.err);
+        if (bt * 32 >= nsrc) {  // a batch of padding: no pairs, zero reactions
+          if (in) slot[j] = slot[kTile + j] = slot[2 * kTile + j] = 0.0;
+          continue;
+        }
+        double sx = SX[j], sy = SY[j], sz = SZ[j], sm = SM[j];
+        double RX = 0.0, RY = 0.0, RZ = 0.0;
+#pragma unroll 2
+        for (int step = 0; step < 32; ++step) {
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const double dx = sx - xi[k], dy = sy - yi[k], dz = sz - zi[k];
+            double r2 = fma(dx, dx, eps2);
+            r2 = fma(dy, dy, r2);
+            r2 = fma(dz, dz, r2);
+            double y = rsqrt(r2);
+            if (EXCL) y = r2 > 0.0 ? y : 0.0;
+            const double y3 = y * y * y;
+            const double sj = sm * y3, si = mi[k] * y3;
+            ax[k] = fma(sj, dx, ax[k]);
+            ay[k] = fma(sj, dy, ay[k]);
+            az[k] = fma(sj, dz, az[k]);
+            RX = fma(si, dx, RX);
+            RY = fma(si, dy, RY);
+            RZ = fma(si, dz, RZ);
+          }
+          sx = __shfl_sync(0xffffffffu, sx, from);
+          sy = __shfl_sync(0xffffffffu, sy, from);
+          sz = __shfl_sync(0xffffffffu, sz, from);
+          sm = __shfl_sync(0xffffffffu, sm, from);
+          RX = __shfl_sync(0xffffffffu, RX, from);
+          RY = __shfl_sync(0xffffffffu, RY, from);
+          RZ = __shfl_sync(0xffffffffu, RZ, from);
+        }
+        // back at its own lane: the acceleration of source j is -sum m_i y^3 d
+        if (in) {
+          slot[j] = -RX;
+          slot[kTile + j] = -RY;
+          slot[2 * kTile + j] = -RZ;
+        }
+      }
+    }
+    __syncwarp();
+    if (__any_sync(0xffffffffu, !ok)) {
+      aborted = true;
+      break;
+    }
+    if (lane == 0) {
+      pending &= ~(1u << st);
+      if (t + kBStages < ntl) issue(t + kBStages);
+    }
+  }
+  if (aborted) {
+    if (lane == 0) {
+      record_error(p.err, kErrTileWait);
+      for (int u = t; u < ntl && u < t + kBStages; ++u) {
+        const unsigned pos = ring.tcount + u;
+        const int st = pos % kBStages;
+        if (!(pending & (1u << st))) continue;
+        if (!mbar_wait_bounded(smem_u32(&ring.bars[st]), (pos / kBStages) & 1u, p.wait_ns)) {
+          record_error(p.err, kErrDrainWait);
+          break;
+        }
+      }
+    }
+    return false;
+  }
+  ring.tcount += ntl;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const long long i = poff + rloc + 32 * k;
+    if (rloc + 32 * k < ns && NBR_IN(i, p.len, p.err)) {
+      p.act[i] = ax[k];
+      p.act[p.n_pad + i] = ay[k];
+      p.act[2 * p.n_pad + i] = az[k];
+    }
+  }
+  __syncwarp();
+  return true;
+}
+
 // The persistent kernel.  WIDE = 0: every item is narrow (4 receivers per
 // lane); WIDE = 1: items flagged kWideItem cover two tiles (8 receivers per
 // lane: twice the pair work per source read, four independent f32x2 chains);
-// WIDE = 2 (FP32C): items flagged kN3Item are Newton-3 row blocks of systems
-// of three tiles or more (their epilogue runs in k_batch_n3_reduce), the
-// other systems' items as for WIDE = 1.
+// WIDE = 2: items flagged kN3Item are Newton-3 row blocks (FP32C: two tiles,
+// systems of three tiles or more; FP64: one tile, systems of two tiles or
+// more; their epilogue runs in k_batch_n3_reduce), the other systems' items
+// as for WIDE = 1 (FP32C) or 0 (FP64).
 template <int PREC, bool EXCL, int WIDE>
 __global__ void __launch_bounds__(kBWarps * 32) k_batch_force(const BatchParams p, const double eps2) {
   constexpr int SB = Stage<PREC>::bytes;
@@ -645,17 +820,25 @@ __global__ void __launch_bounds__(kBWarps * 32) k_batch_force(const BatchParams 
     const int s = it.x & ~(kWideItem | kN3Item);
     if (!NBR_IN(s, p.nsys, p.err)) return;
     bool ok;
-    if (PREC == kFP32C && WIDE == 2 && (it.x & kN3Item)) ok = run_item_n3<EXCL>(p, EPS2, ring, lane, s, it.y);
-    else if (WIDE >= 1 && (it.x & kWideItem)) ok = run_item<PREC, EXCL, 8>(p, eps2, EPS2, ring, lane, s, it.y);
-    else ok = run_item<PREC, EXCL, 4>(p, eps2, EPS2, ring, lane, s, it.y);
+    if (WIDE == 2 && (it.x & kN3Item)) {
+      if constexpr (PREC == kFP32C) ok = run_item_n3<EXCL>(p, EPS2, ring, lane, s, it.y);
+      else ok = run_item_n3_f64<EXCL>(p, eps2, ring, lane, s, it.y);
+    } else if (WIDE == 1 && (it.x & kWideItem)) {
+      ok = run_item<PREC, EXCL, 8>(p, eps2, EPS2, ring, lane, s, it.y);
+    } else if (WIDE == 2 && PREC == kFP32C && (it.x & kWideItem)) {
+      // (the FP64 Newton-3 list has no two-tile items: not compiled in)
+      if constexpr (PREC == kFP32C) ok = run_item<PREC, EXCL, 8>(p, eps2, EPS2, ring, lane, s, it.y);
+    } else {
+      ok = run_item<PREC, EXCL, 4>(p, eps2, EPS2, ring, lane, s, it.y);
+    }
     if (!ok) return;
   }
 }
 
 // The epilogue of the Newton-3 systems: one warp per tile (system, local tile
 // c); each particle's acceleration is its action plus the reactions from the
-// system's row blocks before its own (b = 0 .. c / 2 - 1) in that order:
-// deterministic.  Then the kick/drift and, FP32C, the tile's record pack, as
+// system's row blocks before its own (b = 0 .. c / rows - 1, rows = tiles per
+// row block) in that order: deterministic.  Then the kick/drift and, FP32C, the tile's record pack, as
 // in run_item.
 __global__ void __launch_bounds__(128) k_batch_n3_reduce(const BatchParams p, const int2* tiles,
                                                          int ntiles) {
@@ -667,7 +850,8 @@ __global__ void __launch_bounds__(128) k_batch_n3_reduce(const BatchParams p, co
   const long long poff = p.poff[s];
   const int ns = p.nreal[s];
   const int T = (ns + kTile - 1) / kTile;
-  const int B = c / 2;
+  const int rows = p.n3_rows;
+  const int B = c / rows;
   const long long rbase = poff + (long long)c * kTile;
   const int R = min(kTile, ns - c * kTile);  // real particles of the tile
   double ax[4], ay[4], az[4], xi[4], yi[4], zi[4];
@@ -682,10 +866,10 @@ __global__ void __launch_bounds__(128) k_batch_n3_reduce(const BatchParams p, co
   }
   // The reaction slots in block order; the 12 loads of a slot (every slot
   // entry is written, padding included) are issued before its adds.
-  const long long slot_b0 = p.rea_off[s] + (c - 2);
+  const long long slot_b0 = p.rea_off[s] + (c - rows);
 #pragma unroll 2
   for (int b = 0; b < B; ++b) {
-    const long long sl = slot_b0 + n3b_prefix(T, b) - 2 * b;
+    const long long sl = slot_b0 + n3b_prefix(T, b, rows) - (long long)rows * b;
     if (!NBR_IN((sl + 1) * 3 * kTile - 1, p.rea_len, p.err)) break;
     const double* r = p.rea + (size_t)sl * 3 * kTile + lane;
     double tx[4], ty[4], tz[4];
@@ -811,7 +995,7 @@ const void* batch_fn() {
   return (const void*)k_batch_force<PREC, EXCL, WIDE>;
 }
 
-// wide: 0, 1 or (FP32C) 2 -- the work list the kernel variant takes.
+// wide: 0, 1 or 2 -- the work list the kernel variant takes.
 const void* batch_kernel(int prec, bool excl, int wide) {
   if (prec == kFP32C) {
     if (excl)
@@ -822,8 +1006,13 @@ const void* batch_kernel(int prec, bool excl, int wide) {
            : wide   ? batch_fn<kFP32C, false, 1>()
                     : batch_fn<kFP32C, false, 0>();
   }
-  if (excl) return wide ? batch_fn<kFP64, true, 1>() : batch_fn<kFP64, true, 0>();
-  return wide ? batch_fn<kFP64, false, 1>() : batch_fn<kFP64, false, 0>();
+  if (excl)
+    return wide == 2 ? batch_fn<kFP64, true, 2>()
+           : wide   ? batch_fn<kFP64, true, 1>()
+                    : batch_fn<kFP64, true, 0>();
+  return wide == 2 ? batch_fn<kFP64, false, 2>()
+         : wide   ? batch_fn<kFP64, false, 1>()
+                  : batch_fn<kFP64, false, 0>();
 }
 
 size_t batch_smem(int prec) {
@@ -850,24 +1039,24 @@ std::string batch_key(int prec, size_t nsys, int max_ns, bool excl) {
 
 // The kernel configuration of the batch for a precision: from the autotune
 // cache when it holds this batch's key, else the default (occupancy-limited
-// grid; two-tile items for FP32C, one-tile items for FP64).  The cache stores
+// grid; Newton-3 row blocks).  The cache stores
 // the work list as ni: 4 one-tile items, 8 two-tile items, 3 Newton-3 row
-// blocks (FP32C).
+// blocks.
 void batch_config(nbr_ctx* c, int prec, double eps2) {
   BatchState& b = c->bat;
   const int pi = prec == kFP32C ? 1 : 0;
   if (b.cfg_ok[pi]) return;
   ForceConfig t{0, 0, 0};
   if (tune_get(batch_key(prec, b.nsys, b.max_ns, eps2 == 0.0), &t) &&
-      (t.ni == 4 || t.ni == 8 || (t.ni == 3 && prec == kFP32C))) {
+      (t.ni == 4 || t.ni == 8 || t.ni == 3)) {
     b.wide[pi] = t.ni == 8 ? 1 : t.ni == 3 ? 2 : 0;
     b.per_sm[pi] = t.split;
   } else {
     // Defaults from the 4096-system workload on B200: FP32C 1888 GPairs/s
-    // with one-tile items, 2047 with two-tile items, 2325 with Newton-3 row
-    // blocks for the systems of three tiles or more; FP64 (twice the
-    // registers per receiver) is faster with one-tile items (834 vs 784).
-    b.wide[pi] = prec == kFP32C ? 2 : 0;
+    // with one-tile items, 2045 with two-tile items, 2471 with Newton-3 row
+    // blocks; FP64 837 with one-tile items, 787 with two-tile items, 1153
+    // with Newton-3 row blocks.
+    b.wide[pi] = 2;
     b.per_sm[pi] = 0;
   }
   b.cfg_ok[pi] = true;
@@ -882,13 +1071,14 @@ int batch_grid(nbr_ctx* c, int prec, double eps2) {
   BatchState& b = c->bat;
   batch_config(c, prec, eps2);
   const int pi = prec == kFP32C ? 1 : 0, ei = eps2 == 0.0 ? 1 : 0, wi = b.wide[pi];
-  if (wi == 2 && b.rea_slots > 0 && !b.d_act) {
-    cudaError_t e = dalloc((void**)&b.d_act, 3 * b.s.n_pad * sizeof(double));
-    if (e == cudaSuccess) e = dalloc((void**)&b.d_rea, (size_t)b.rea_slots * 3 * kTile * sizeof(double));
+  BatchState::N3List& l3 = b.n3[pi];
+  if (wi == 2 && l3.slots > 0 && !l3.d_rea) {
+    cudaError_t e = cudaSuccess;
+    if (!b.d_act) e = dalloc((void**)&b.d_act, 3 * b.s.n_pad * sizeof(double));
+    if (e == cudaSuccess) e = dalloc((void**)&l3.d_rea, (size_t)l3.slots * 3 * kTile * sizeof(double));
     if (e != cudaSuccess) {
-      dfree(b.d_act);
-      dfree(b.d_rea);
-      b.d_act = b.d_rea = nullptr;
+      dfree(l3.d_rea);
+      l3.d_rea = nullptr;
       return 0;
     }
   }
@@ -930,9 +1120,13 @@ int batch_eval(nbr_ctx* c, int prec, double G, double eps2, int mode, double kic
   p.rec = s.rec[a]; p.org = s.org[a];
   const int grid = batch_grid(c, prec, eps2);  // also settles the configuration
   if (grid == 0) return fail(c, NBR_ERR_CUDA, "batch Newton-3 scratch allocation");
-  const int wi = b.wide[prec == kFP32C ? 1 : 0];
-  p.poff = b.d_poff; p.nreal = b.d_nreal; p.items = b.d_items[wi]; p.n_items = b.n_items[wi];
-  p.act = b.d_act; p.rea = b.d_rea; p.rea_off = b.d_rea_off; p.n_pad = (long long)s.n_pad;
+  const int pi = prec == kFP32C ? 1 : 0, wi = b.wide[pi];
+  const BatchState::N3List& l3 = b.n3[pi];
+  p.poff = b.d_poff; p.nreal = b.d_nreal;
+  p.items = wi == 2 ? l3.d_items : b.d_items[wi];
+  p.n_items = wi == 2 ? l3.n_items : b.n_items[wi];
+  p.act = b.d_act; p.rea = l3.d_rea; p.rea_off = l3.d_rea_off; p.n_pad = (long long)s.n_pad;
+  p.n3_rows = prec == kFP32C ? 2 : 1;
   p.head = b.d_head;
   p.mode = mode; p.G = G; p.kick = kick; p.drift = drift;
   p.ax = s.acc[0]; p.ay = s.acc[1]; p.az = s.acc[2];
@@ -946,13 +1140,13 @@ int batch_eval(nbr_ctx* c, int prec, double G, double eps2, int mode, double kic
   p.wait_ns = js.wait_ns;
   p.skip_tile = js.skip_tile;
   NBR_CHECKED_ONLY(p.len = (long long)s.cap; p.nsys = (int)b.nsys;
-                   p.rea_len = b.d_rea ? b.rea_slots * 3 * kTile : 0;)
+                   p.rea_len = l3.d_rea ? l3.slots * 3 * kTile : 0;)
   e = launch_batch(prec, wi, p, eps2, grid, c->stream);
   if (kernels) ++*kernels;
   if (e != cudaSuccess) return cuda_fail(c, e, "batch force launch");
-  if (wi == 2 && b.n_n3_tiles > 0) {
-    const unsigned blocks = (unsigned)((b.n_n3_tiles + 3) / 4);
-    k_batch_n3_reduce<<<blocks, 128, 0, c->stream>>>(p, b.d_n3_tiles, b.n_n3_tiles);
+  if (wi == 2 && l3.n_tiles > 0) {
+    const unsigned blocks = (unsigned)((l3.n_tiles + 3) / 4);
+    k_batch_n3_reduce<<<blocks, 128, 0, c->stream>>>(p, l3.d_tiles, l3.n_tiles);
     e = cudaGetLastError();
     if (kernels) ++*kernels;
     if (e != cudaSuccess) return cuda_fail(c, e, "batch Newton-3 epilogue launch");
@@ -974,11 +1168,13 @@ void nbr::BatchState::release() {
   dfree(d_sys_of_tile);
   dfree(d_items[0]);
   dfree(d_items[1]);
-  dfree(d_items[2]);
-  dfree(d_n3_tiles);
-  dfree(d_rea_off);
+  for (N3List& l : n3) {
+    dfree(l.d_items);
+    dfree(l.d_tiles);
+    dfree(l.d_rea_off);
+    dfree(l.d_rea);
+  }
   dfree(d_act);
-  dfree(d_rea);
   dfree(d_head);
   dfree(d_red);
   *this = BatchState();
@@ -1051,34 +1247,40 @@ int nbr_batch_upload(nbr_ctx* c, size_t nsys, const size_t* offsets, const doubl
   }
   // Work items ordered by cost (receiver slots x system size), largest first:
   // list 0 with one-tile items only, list 1 pairing a system's tiles into
-  // two-tile items (a system's odd last tile stays a one-tile item), list 2
-  // with Newton-3 row blocks for the systems of three tiles or more (cost: the
-  // own two tiles' ordered pairs, and each later tile's pairs at the
-  // rotation's ~1.5x the work per pair) and list 1's items for the rest.
-  std::vector<int2> lists[3];
-  std::vector<int2> n3_tiles;
-  std::vector<long long> rea_off(nsys, -1);
-  long long slots = 0;
-  for (int wl = 0; wl < 3; ++wl) {
+  // two-tile items (a system's odd last tile stays a one-tile item); lists 2
+  // (FP64) and 3 (FP32C) with Newton-3 row blocks of R = 1 or 2 tiles for the
+  // systems of R + 1 tiles or more (cost: the own tiles' ordered pairs, and
+  // each later tile's pairs at the rotation's ~1.5x the work per pair), and
+  // list 0's (FP64) or list 1's (FP32C) items for the rest.
+  std::vector<int2> lists[4];
+  std::vector<int2> n3_tiles[2];
+  std::vector<long long> rea_off[2] = {std::vector<long long>(nsys, -1),
+                                       std::vector<long long>(nsys, -1)};
+  long long slots[2] = {0, 0};
+  for (int wl = 0; wl < 4; ++wl) {
     std::vector<int2> items;
     std::vector<double> cost;
+    const int q = wl - 2;                 // Newton-3 list of precision index q
+    const int rows = wl == 3 ? 2 : 1;     // tiles per row block
+    const bool pairs = wl == 1 || wl == 3;  // two-tile items for the other systems
     for (size_t s = 0; s < nsys; ++s) {
       const long long ns = (long long)(offsets[s + 1] - offsets[s]);
       const long long nt = (ns + kTile - 1) / kTile;
-      if (wl == 2 && nt >= 3) {
-        rea_off[s] = slots;
-        for (long long blk = 0; 2 * blk < nt; ++blk) {
-          const long long later = std::max<long long>(0, nt - 2 * blk - 2);
-          slots += later;
+      if (q >= 0 && nt >= rows + 1) {
+        rea_off[q][s] = slots[q];
+        for (long long blk = 0; rows * blk < nt; ++blk) {
+          const long long own = std::min<long long>(rows, nt - rows * blk);
+          const long long later = std::max<long long>(0, nt - rows * blk - rows);
+          slots[q] += later;
           items.push_back(make_int2((int)s | kN3Item, (int)blk));
-          cost.push_back(2.0 * kTile * (std::min<long long>(2, nt - 2 * blk) + 1.5 * later) * kTile);
+          cost.push_back(double(rows) * kTile * (double(own) + 1.5 * double(later)) * kTile);
         }
-        for (long long t = 0; t < nt; ++t) n3_tiles.push_back(make_int2((int)s, (int)t));
+        for (long long t = 0; t < nt; ++t) n3_tiles[q].push_back(make_int2((int)s, (int)t));
         continue;
       }
       for (long long t = 0; t < nt;) {
         const int tile = (int)(b.poff[s] / kTile + t);
-        if (wl >= 1 && t + 1 < nt) {
+        if (pairs && t + 1 < nt) {
           items.push_back(make_int2((int)s | kWideItem, tile));
           cost.push_back(2.0 * kTile * double(ns));
           t += 2;
@@ -1095,7 +1297,6 @@ int nbr_batch_upload(nbr_ctx* c, size_t nsys, const size_t* offsets, const doubl
     std::stable_sort(order.begin(), order.end(), [&](int a, int bb) { return cost[a] > cost[bb]; });
     lists[wl].resize(items.size());
     for (size_t k = 0; k < order.size(); ++k) lists[wl][k] = items[order[k]];
-    b.n_items[wl] = (int)lists[wl].size();
   }
   std::vector<int> nreal(nsys);
   b.max_ns = 0;
@@ -1103,15 +1304,22 @@ int nbr_batch_upload(nbr_ctx* c, size_t nsys, const size_t* offsets, const doubl
     nreal[s] = (int)(offsets[s + 1] - offsets[s]);
     b.max_ns = std::max(b.max_ns, nreal[s]);
   }
+  int2** dl[4] = {&b.d_items[0], &b.d_items[1], &b.n3[0].d_items, &b.n3[1].d_items};
+  b.n_items[0] = (int)lists[0].size();
+  b.n_items[1] = (int)lists[1].size();
+  for (int q = 0; q < 2; ++q) {
+    b.n3[q].n_items = (int)lists[2 + q].size();
+    b.n3[q].n_tiles = (int)n3_tiles[q].size();
+    b.n3[q].slots = slots[q];
+  }
   e = dalloc((void**)&b.d_poff, (nsys + 1) * sizeof(long long));
   if (e == cudaSuccess) e = dalloc((void**)&b.d_nreal, nsys * sizeof(int));
-  for (int wl = 0; wl < 3 && e == cudaSuccess; ++wl)
-    e = dalloc((void**)&b.d_items[wl], lists[wl].size() * sizeof(int2));
-  b.n_n3_tiles = (int)n3_tiles.size();
-  b.rea_slots = slots;
-  if (e == cudaSuccess && !n3_tiles.empty())
-    e = dalloc((void**)&b.d_n3_tiles, n3_tiles.size() * sizeof(int2));
-  if (e == cudaSuccess) e = dalloc((void**)&b.d_rea_off, nsys * sizeof(long long));
+  for (int wl = 0; wl < 4 && e == cudaSuccess; ++wl)
+    e = dalloc((void**)dl[wl], lists[wl].size() * sizeof(int2));
+  for (int q = 0; q < 2 && e == cudaSuccess; ++q) {
+    if (!n3_tiles[q].empty()) e = dalloc((void**)&b.n3[q].d_tiles, n3_tiles[q].size() * sizeof(int2));
+    if (e == cudaSuccess) e = dalloc((void**)&b.n3[q].d_rea_off, nsys * sizeof(long long));
+  }
   if (e == cudaSuccess) e = dalloc((void**)&b.d_head, 256);
   if (e == cudaSuccess) e = dalloc((void**)&b.d_red, nsys * 9 * sizeof(double));
   if (e == cudaSuccess)
@@ -1119,15 +1327,17 @@ int nbr_batch_upload(nbr_ctx* c, size_t nsys, const size_t* offsets, const doubl
                         cudaMemcpyHostToDevice, c->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(b.d_nreal, nreal.data(), nsys * sizeof(int), cudaMemcpyHostToDevice, c->stream);
-  for (int wl = 0; wl < 3 && e == cudaSuccess; ++wl)
-    e = cudaMemcpyAsync(b.d_items[wl], lists[wl].data(), lists[wl].size() * sizeof(int2),
+  for (int wl = 0; wl < 4 && e == cudaSuccess; ++wl)
+    e = cudaMemcpyAsync(*dl[wl], lists[wl].data(), lists[wl].size() * sizeof(int2),
                         cudaMemcpyHostToDevice, c->stream);
-  if (e == cudaSuccess && !n3_tiles.empty())
-    e = cudaMemcpyAsync(b.d_n3_tiles, n3_tiles.data(), n3_tiles.size() * sizeof(int2),
-                        cudaMemcpyHostToDevice, c->stream);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(b.d_rea_off, rea_off.data(), nsys * sizeof(long long),
-                        cudaMemcpyHostToDevice, c->stream);
+  for (int q = 0; q < 2 && e == cudaSuccess; ++q) {
+    if (!n3_tiles[q].empty())
+      e = cudaMemcpyAsync(b.n3[q].d_tiles, n3_tiles[q].data(), n3_tiles[q].size() * sizeof(int2),
+                          cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(b.n3[q].d_rea_off, rea_off[q].data(), nsys * sizeof(long long),
+                          cudaMemcpyHostToDevice, c->stream);
+  }
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) {
     b.release();
@@ -1304,8 +1514,6 @@ int nbr_batch_set_config(nbr_ctx* c, int precision, int wide, int ctas_per_sm) {
     return fail(c, NBR_ERR_INVALID_ARG, "unknown precision");
   if (wide < -1 || wide > 2 || ctas_per_sm < 0)
     return fail(c, NBR_ERR_INVALID_ARG, "wide must be -1, 0, 1 or 2 and ctas_per_sm >= 0");
-  if (wide == 2 && precision != NBR_FP32C)
-    return fail(c, NBR_ERR_INVALID_ARG, "Newton-3 row blocks (wide = 2) are FP32C only");
   BatchState& b = c->bat;
   const int pi = precision == kFP32C ? 1 : 0;
   if (wide < 0) {
@@ -1330,7 +1538,7 @@ int nbr_batch_autotune(nbr_ctx* c, int precision, double eps2) {
   const int pi = precision == kFP32C ? 1 : 0;
   int best_w = -1, best_p = 0;
   float best_ms = 1e30f;
-  for (int w = 0; w < (precision == kFP32C ? 3 : 2); ++w) {
+  for (int w = 0; w < 3; ++w) {
     b.wide[pi] = w;
     b.per_sm[pi] = 0;
     b.cfg_ok[pi] = true;

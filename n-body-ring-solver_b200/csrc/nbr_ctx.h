@@ -67,20 +67,27 @@ struct BatchState {
   int* d_sys_of_tile = nullptr;      // system index of every padded tile
   // Work queues of (system | kWideItem flag, first receiver tile), cost
   // ordered: [0] one-tile items only, [1] two-tile items where a system has
-  // two tiles left, [2] (FP32C) Newton-3 row blocks (system | kN3Item, block)
-  // of the systems of three tiles or more, the others' items as in [1].
-  int2* d_items[3] = {nullptr, nullptr, nullptr};
-  int n_items[3] = {0, 0, 0};
-  // Newton-3 systems: their tiles (system, local tile) for the epilogue
-  // kernel, each system's first reaction slot (-1: none), the slot count, and
-  // the scratch (allocated at first use): action [3][n_pad], reactions
-  // [slots][3][128].
-  int2* d_n3_tiles = nullptr;
-  int n_n3_tiles = 0;
-  long long* d_rea_off = nullptr;
-  long long rea_slots = 0;
-  double* d_act = nullptr;
-  double* d_rea = nullptr;
+  // two tiles left.
+  int2* d_items[2] = {nullptr, nullptr};
+  int n_items[2] = {0, 0};
+  // Newton-3 work per precision ([0] FP64: one-tile row blocks of the systems
+  // of two tiles or more, the others' items as in list 0; [1] FP32C: two-tile
+  // row blocks of the systems of three tiles or more, the others' items as in
+  // list 1): the queue of (system | kN3Item, row block) and other items, the
+  // Newton-3 systems' tiles (system, local tile) for the epilogue kernel, each
+  // system's first reaction slot (-1: none), the slot count, and the slots
+  // [slots][3][128] (allocated at first use).
+  struct N3List {
+    int2* d_items = nullptr;
+    int n_items = 0;
+    int2* d_tiles = nullptr;
+    int n_tiles = 0;
+    long long* d_rea_off = nullptr;
+    long long slots = 0;
+    double* d_rea = nullptr;
+  };
+  N3List n3[2];
+  double* d_act = nullptr;           // Newton-3 action sums [3][n_pad] (at first use)
   int max_ns = 0;                    // largest system
   unsigned* d_head = nullptr;        // work-queue heads
   double* d_red = nullptr;           // per-system diagnostic sums

@@ -55,7 +55,7 @@ with nbr.Context(0) as ctx:
     st = {k: np.concatenate([nbr.plummer(m, 20 + i)[k] for i, m in enumerate(sizes)]) for k in nbr.KEYS}
     ctx.batch_upload(off, st)
     for prec in (FP64, FP32C):
-        for wide in ((0, 1) if prec == FP64 else (0, 1, 2)):
+        for wide in (0, 1, 2):
             ctx.batch_set_config(prec, wide, 0)
             a = ctx.batch_forces(prec, eps2=1e-6)
             ctx.batch_run(prec, dt=1e-4, steps=2, eps2=1e-6)

@@ -55,7 +55,7 @@ def test_batch_autotune(ctx, nbr, oracle, prec):
     cache = _cache()
     assert key in cache
     ni, warps, per_sm = cache[key][:3]
-    assert ni in ((4, 8) if prec == FP64 else (3, 4, 8)) and per_sm >= 1
+    assert ni in (3, 4, 8) and per_sm >= 1
     a = ctx.batch_forces(prec, eps2=eps2)
     for s in range(len(sizes)):
         sub = system(st, off, s)

@@ -33,9 +33,10 @@ def system(st, off, s):
     return {k: st[k][off[s]:off[s + 1]] for k in st}
 
 
-# work lists: one-tile items, two-tile items, Newton-3 row blocks (FP32C)
-WORK = [(FP64, 0), (FP64, 1), (FP32C, 0), (FP32C, 1), (FP32C, 2)]
-WORK_IDS = ["fp64-one-tile", "fp64-two-tile", "fp32c-one-tile", "fp32c-two-tile", "fp32c-newton3"]
+# work lists: one-tile items, two-tile items, Newton-3 row blocks
+WORK = [(FP64, 0), (FP64, 1), (FP64, 2), (FP32C, 0), (FP32C, 1), (FP32C, 2)]
+WORK_IDS = ["fp64-one-tile", "fp64-two-tile", "fp64-newton3", "fp32c-one-tile", "fp32c-two-tile",
+            "fp32c-newton3"]
 
 
 @pytest.mark.parametrize("prec,wide", WORK, ids=WORK_IDS)
@@ -89,11 +90,35 @@ def test_batch_newton3_row_blocks(ctx, nbr, oracle, eps2):
     assert rel_err(a, w).max() <= 1e-4
 
 
-def test_batch_newton3_is_fp32c_only(ctx, nbr):
+@pytest.mark.parametrize("eps2", [1e-6, 0.0])
+def test_batch_newton3_row_blocks_fp64(ctx, nbr, oracle, eps2):
+    """The FP64 Newton-3 work list (one-tile row blocks for systems of two
+    tiles or more, one-tile items for the rest): every particle within 1e-12
+    of the oracle, the run repeated bit for bit, and within 1e-13 of the
+    one-tile list (only the summation order differs)."""
+    sizes = [5, 128, 129, 200, 256, 300, 385, 640, 1000, 2049]
+    off, st = make_batch(nbr, sizes, seed=23)
+    ctx.batch_upload(off, st)
+    ctx.batch_set_config(FP64, 2, 0)
+    a = ctx.batch_forces(FP64, eps2=eps2)
+    b = ctx.batch_forces(FP64, eps2=eps2)
+    np.testing.assert_array_equal(a, b)
+    for s, n in enumerate(sizes):
+        sub = system(st, off, s)
+        ref = oracle.accel(sub["x"], sub["y"], sub["z"], sub["m"], eps2=eps2, extended=True)
+        e = rel_err(a[:, off[s]:off[s + 1]], ref)
+        assert e.max() <= 1e-12, (n, e.max())
+    ctx.batch_set_config(FP64, 0, 0)
+    w = ctx.batch_forces(FP64, eps2=eps2)
+    assert rel_err(a, w).max() <= 1e-13
+
+
+def test_batch_set_config_rejects_bad_values(ctx, nbr):
     off, st = make_batch(nbr, [300, 400])
     ctx.batch_upload(off, st)
-    with pytest.raises(nbr.NbrError):
-        ctx.batch_set_config(FP64, 2, 0)
+    for wide, per in ((3, 0), (-2, 0), (1, -1)):
+        with pytest.raises(nbr.NbrError):
+            ctx.batch_set_config(FP64, wide, per)
 
 
 def test_batch_systems_do_not_interact(ctx, nbr):
@@ -173,20 +198,21 @@ def test_batch_full_workload(ctx, nbr, oracle, wide):
     assert stats["pairs"] == 2 * float((sizes * (sizes - 1)).sum())
 
 
-@pytest.mark.parametrize("wide", [1, 2], ids=["two-tile", "newton3"])
-def test_batch_bounded_wait_expires_cleanly(nbr, wide):
+@pytest.mark.parametrize("prec,wide", [(FP32C, 1), (FP32C, 2), (FP64, 2)],
+                         ids=["fp32c-two-tile", "fp32c-newton3", "fp64-newton3"])
+def test_batch_bounded_wait_expires_cleanly(nbr, prec, wide):
     """Tile 2 of every item never arrives (a test hook; for a Newton-3 row
-    block, its first later column tile): the wait gives up, the call reports
+    block, a later column tile): the wait gives up, the call reports
     NBR_ERR_TIMEOUT and the context keeps working."""
     off, st = make_batch(nbr, [700, 900], seed=2)
     with nbr.Context(0) as c:
         c.batch_upload(off, st)
-        c.batch_set_config(FP32C, wide, 0)
+        c.batch_set_config(prec, wide, 0)
         os.environ["NBR_WAIT_LIMIT_MS"] = "100"
         os.environ["NBR_TEST_SKIP_TILE"] = "2"
         try:
             with pytest.raises(nbr.NbrError) as ei:
-                c.batch_forces(FP32C, eps2=1e-6)
+                c.batch_forces(prec, eps2=1e-6)
             assert ei.value.status == 4
         finally:
             del os.environ["NBR_TEST_SKIP_TILE"]
