@@ -501,6 +501,9 @@ class Context:
                 "kernels": st.kernels}
 
     def batch_set_config(self, precision, wide=-1, ctas_per_sm=0):
+        """Work list of the batched kernel: 0 one-tile items, 1 two-tile items,
+        2 Newton-3 row blocks for the larger systems (the default), -1 back to
+        the autotune cache or the default; ctas_per_sm 0 = occupancy limit."""
         self._chk(self.L.nbr_batch_set_config(self.h, precision, wide, ctas_per_sm), "batch_set_config")
 
     def batch_autotune(self, precision, eps2=0.0):
