@@ -39,6 +39,11 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <functional>
+#include <map>
+#include <mutex>
+#include <queue>
+#include <vector>
 
 namespace nbr {
 
@@ -1782,6 +1787,63 @@ size_t n3_smem_bytes(int precision, int warps) {
   return precision == kFP32C
              ? kSmemHead + (size_t)kStages * kStage32 + (size_t)warps * 3 * kN3Block * sizeof(float)
              : kSmemHead + (size_t)kStages * kStage64 + (size_t)kN3F64Warps * 3 * kN3Block * sizeof(double);
+}
+
+// The column-chunk width of the Newton-3 grid.  A CTA (row group g, chunk k)
+// costs a fixed 0.15 plus, per column block of its chunk, 1 (0.8 for the
+// group's first 8 blocks, where the diagonal leaves warps idle), in units of
+// one column block's pair work; the CTAs are handed to the SMs in launch
+// order as SMs free up (list scheduling, one CTA per SM).  Both constants were
+// fitted on B200 to 27 timed (N, width) pairs from N = 32768 to 2^20, which
+// the model reproduces to 1 % (0.2 % on average).  Narrow chunks cut the last
+// wave's idle time, wide ones the per-CTA cost: the best widths are 8 at
+// N = 32768, 15 at 65536, 6 at 131072, 18 at 262144 and 32 from ~2^20 up.
+double n3_makespan(long long nb, int cols, int sms) {
+  constexpr double kCtaCost = 0.15, kDiagBlock = 0.8;
+  std::priority_queue<double, std::vector<double>, std::greater<double>> free_at;
+  for (int i = 0; i < sms; ++i) free_at.push(0.0);
+  double end = 0.0;
+  for (long long r0 = 0; r0 < nb; r0 += kN3Warps) {
+    for (long long cs = r0; cs < nb; cs += cols) {
+      const long long ce = std::min(cs + cols, nb);
+      const long long diag = std::max(0LL, std::min(ce, r0 + kN3Warps) - cs);  // blocks < r0 + 8
+      const double t = kCtaCost + kDiagBlock * (double)diag + (double)(ce - cs - diag);
+      const double start = free_at.top();
+      free_at.pop();
+      free_at.push(start + t);
+      end = std::max(end, start + t);
+    }
+  }
+  return end;
+}
+
+int n3_cols(long long nb) {
+  if (nb <= 1) return 1;
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
+    sms = 148;
+  static std::mutex mu;
+  static std::map<std::pair<long long, int>, int> memo;
+  std::lock_guard<std::mutex> lock(mu);
+  const auto key = std::make_pair(nb, sms);
+  const auto it = memo.find(key);
+  if (it != memo.end()) return it->second;
+  int best = kN3MaxCols;
+  // many waves at the widest chunk: the last wave's idle time is negligible
+  if (n3_ctas(nb, kN3MaxCols) < 64LL * sms) {
+    double best_t = n3_makespan(nb, kN3MaxCols, sms);
+    for (int c = kN3MaxCols - 1; c >= 1; --c) {
+      if (n3_ctas(nb, c) > 128LL * sms) break;  // narrower still: only more CTA cost
+      const double t = n3_makespan(nb, c, sms);
+      if (t < best_t * (1.0 - 1e-3)) {  // ties keep the wider chunk (fewer partial sums)
+        best_t = t;
+        best = c;
+      }
+    }
+  }
+  memo[key] = best;
+  return best;
 }
 
 cudaError_t configure_kernels() {

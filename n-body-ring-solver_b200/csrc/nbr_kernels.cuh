@@ -121,12 +121,14 @@ __host__ __device__ inline int n3_chunks(long long nb, int cols, int g) {
   const long long left = nb - (long long)g * kN3Warps;
   return left <= 0 ? 0 : (int)((left + cols - 1) / cols);
 }
-// Column blocks per CTA: kN3MaxCols, or fewer so that a small system still
-// gets about 600 CTAs (4 waves of one CTA per SM).
-inline int n3_cols(long long nb) {
-  const long long c = nb * nb / (16LL * 600);
-  return (int)(c < 1 ? 1 : c > kN3MaxCols ? kN3MaxCols : c);
-}
+// Column blocks per CTA (1 .. kN3MaxCols) for nb blocks on the current
+// device: the width whose grid a model of the launch finishes first (see
+// nbr_kernels.cu).  Memoized per (nb, SM count); a host function.
+int n3_cols(long long nb);
+// The model's finishing time of the Newton-3 grid for nb blocks in chunks of
+// `cols`, on `sms` SMs (one CTA each at a time), in units of one column
+// block's pair work.
+double n3_makespan(long long nb, int cols, int sms);
 // CTAs of a Newton-3 launch and the doubles its partial sums need.
 inline long long n3_ctas(long long nb, int cols) {
   long long t = 0;
