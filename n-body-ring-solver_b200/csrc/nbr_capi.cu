@@ -87,7 +87,7 @@ bool RunKey::operator==(const RunKey& o) const {
       cfg.tile != o.cfg.tile || cfg.unroll != o.cfg.unroll ||
       wait_ns != o.wait_ns || skip_tile != o.skip_tile)
     return false;
-  for (int i = 0; i < 6; ++i)
+  for (int i = 0; i < 7; ++i)
     if (ptr[i] != o.ptr[i]) return false;
   return true;
 }
@@ -380,6 +380,33 @@ long long n3_banded_doubles(long long nb, int V, long long n_pad, long long* acc
   return *acc_off + 3 * n_pad;
 }
 
+// The launch-order table of the whole-system Newton-3 grid for nb blocks
+// (n3_launch_order) followed by its inverse, written when nb changes.  Called
+// outside stream capture (prepare_split runs before nbr_run captures).
+cudaError_t n3_order_prepare(nbr_ctx* c, long long nb) {
+  if (c->n3_order && c->n3_order_nb == nb) return cudaSuccess;
+  std::vector<int> order;
+  n3_launch_order(nb, n3_cols(nb), order);
+  const size_t C = order.size();
+  order.resize(2 * C);
+  for (size_t i = 0; i < C; ++i) order[C + order[i]] = (int)i;
+  cudaError_t e = cudaSuccess;
+  if ((long long)order.size() > c->n3_order_cap) {
+    dfree(c->n3_order);
+    c->n3_order = nullptr;
+    c->n3_order_cap = 0;
+    c->n3_order_nb = -1;
+    e = dalloc((void**)&c->n3_order, order.size() * sizeof(int));
+    if (e != cudaSuccess) return e;
+    c->n3_order_cap = (long long)order.size();
+  }
+  e = cudaMemcpyAsync(c->n3_order, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice,
+                      c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  c->n3_order_nb = e == cudaSuccess ? nb : -1;
+  return e;
+}
+
 int prepare_split(nbr_ctx* c, const ForceConfig& cfg, long long n_pad_i) {
   if (cfg.ni == 3) {  // Newton-3 (the context's whole system only): its own partial sums
     (void)n_pad_i;
@@ -389,6 +416,7 @@ int prepare_split(nbr_ctx* c, const ForceConfig& cfg, long long n_pad_i) {
     const long long need =
         V == 1 ? n3_scratch_doubles(nb) : n3_banded_doubles(nb, V, (long long)c->sys.n_pad, &acc_off);
     cudaError_t e = c->scr.need_part((size_t)need);
+    if (e == cudaSuccess && V == 1) e = n3_order_prepare(c, nb);
     return e == cudaSuccess ? NBR_OK : cuda_fail(c, e, "Newton-3 scratch");
   }
   if (cfg.split <= 1) return NBR_OK;
@@ -500,7 +528,7 @@ int eval_system(nbr_ctx* c, int precision, double G, double eps2, int mode, doub
     const int V = n3_bands(nb);
     if (V == 1) {
       e = launch_force_n3(precision, cfg.warps, eps2, ip, js, ep, c->scr.part,
-                          (long long)c->scr.part_cap, c->stream);
+                          (long long)c->scr.part_cap, c->n3_order, c->stream);
       if (kernels) *kernels += 2;
     } else {
       // banded: the slices' partial accelerations accumulate in slice order in
@@ -714,6 +742,7 @@ int nbr_ctx_destroy(nbr_ctx* c) {
   c->bat.release();
   c->scr.release();
   c->ij.release();
+  dfree(c->n3_order);
   dfree(c->d_err);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
@@ -1173,6 +1202,7 @@ int nbr_run(nbr_ctx* c, int precision, int scheme, int order, double dt, size_t 
     }
     key.ptr[0] = s.pos[0][0]; key.ptr[1] = s.rec[0]; key.ptr[2] = s.vel[0];
     key.ptr[3] = c->scr.part; key.ptr[4] = c->scr.cnt; key.ptr[5] = c->d_err;
+    key.ptr[6] = c->n3_order;
     RunGraph& rg = c->run_graph;
     int kernels = 0;
     double evals = 0;

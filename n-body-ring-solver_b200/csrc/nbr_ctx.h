@@ -150,7 +150,7 @@ struct RunKey {
   ForceConfig cfg{0, 0, 0};
   unsigned long long wait_ns = 0;
   int skip_tile = -1;
-  const void* ptr[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  const void* ptr[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   bool operator==(const RunKey& o) const;
 };
 // The last nbr_run graph, replayed while the key matches.
@@ -184,4 +184,10 @@ struct nbr_ctx {
   double acc_G = 0.0, acc_eps2 = 0.0;
   nbr::ForceConfig override_cfg[2] = {{0, 0, 0}, {0, 0, 0}};
   nbr::RunGraph run_graph;
+  // Launch order of the whole-system Newton-3 grid (longest CTA first) for
+  // n3_order_nb blocks, then its inverse; written before any graph capture
+  // (n3_order_prepare, the only writer), read by the pair and reduce kernels.
+  int* n3_order = nullptr;
+  long long n3_order_cap = 0;    // ints allocated
+  long long n3_order_nb = -1;    // blocks the table holds the order of
 };

@@ -694,7 +694,10 @@ __global__ void __launch_bounds__(kN3Warps * 32)
   unsigned char* stages = smem + kSmemHead;
   float* red = reinterpret_cast<float*>(stages + kStages * kStage32);  // [warp][3][256]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int g = RANGED ? p3.g0 : 0, k = blockIdx.x;
+  // (row group, chunk) from the CTA's group-major number (whole-system
+  // launches run in the longest-first order of p3.order); the partial sums are
+  // indexed by blockIdx.x (a register-free index in the hot loop)
+  int g = RANGED ? p3.g0 : 0, k = RANGED ? (int)blockIdx.x : p3.order[blockIdx.x];
   // row groups [g0, g1) of this launch
   const int groups = RANGED ? p3.g1 : (int)((p3.nb + kN3Warps - 1) / kN3Warps);
   while (g < groups) {  // the grid has exactly sum_g n3_chunks(nb, cols, g) CTAs
@@ -924,7 +927,7 @@ __global__ void __launch_bounds__(kN3F64Warps * 32, 1)
   float* red = reinterpret_cast<float*>(stages + kStages * kStage32);  // [warp][3][256]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int rb = warp >> 1, hf = warp & 1;  // row block in the group, its receiver half
-  int g = p3.g0, k = blockIdx.x;
+  int g = p3.g0, k = p3.order ? p3.order[blockIdx.x] : (int)blockIdx.x;  // group-major number
   const int groups = p3.g1;  // row groups [g0, g1) of this launch
   while (g < groups) {  // the grid has exactly sum_g n3_chunks(nb, cols, g) CTAs
     const int K = n3_chunks(p3.nb, p3.cols, g);
@@ -1153,7 +1156,7 @@ __global__ void __launch_bounds__(kN3F64Warps * 32)
   double* red = reinterpret_cast<double*>(stages + kStages * kStage64);  // [warp][3][256]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int rb = warp >> 1, hf = warp & 1;  // row block in the group, its receiver half
-  int g = p3.g0, k = blockIdx.x;
+  int g = p3.g0, k = p3.order ? p3.order[blockIdx.x] : (int)blockIdx.x;  // group-major number
   const int groups = p3.g1;  // row groups [g0, g1) of this launch
   while (g < groups) {  // the grid has exactly sum_g n3_chunks(nb, cols, g) CTAs
     const int K = n3_chunks(p3.nb, p3.cols, g);
@@ -1320,7 +1323,8 @@ __global__ void __launch_bounds__(128)
     const int K = n3_chunks(p3.nb, p3.cols, gp);
     if (gp == g) {
       for (int k = 0; k < K; ++k) {
-        const double* A = p3.act + ((size_t)(prefix + k) * kN3Warps + w) * 3 * kN3Block;
+        const long long sk = p3.slot ? p3.slot[prefix + k] : prefix + k;  // partial-sum index
+        const double* A = p3.act + ((size_t)sk * kN3Warps + w) * 3 * kN3Block;
         if (!NBR_IN((A - p3.act) + 3 * kN3Block - 1, p3.act_len, ep.err)) continue;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
@@ -1332,7 +1336,8 @@ __global__ void __launch_bounds__(128)
     const long long cs0 = (long long)gp * kN3Warps;
     const int kk = (int)((b - cs0) / p3.cols);
     const int col = (int)(b - (cs0 + (long long)kk * p3.cols));
-    const double* Rr = p3.rea + ((size_t)(prefix + kk) * p3.cols + col) * 3 * kN3Block;
+    const long long skk = p3.slot ? p3.slot[prefix + kk] : prefix + kk;
+    const double* Rr = p3.rea + ((size_t)skk * p3.cols + col) * 3 * kN3Block;
     if (!NBR_IN((Rr - p3.act) + 3 * kN3Block - 1, p3.act_len, ep.err)) {
       prefix += K;
       continue;
@@ -1789,30 +1794,48 @@ size_t n3_smem_bytes(int precision, int warps) {
              : kSmemHead + (size_t)kStages * kStage64 + (size_t)kN3F64Warps * 3 * kN3Block * sizeof(double);
 }
 
-// The column-chunk width of the Newton-3 grid.  A CTA (row group g, chunk k)
-// costs a fixed 0.15 plus, per column block of its chunk, 1 (0.8 for the
-// group's first 8 blocks, where the diagonal leaves warps idle), in units of
-// one column block's pair work; the CTAs are handed to the SMs in launch
-// order as SMs free up (list scheduling, one CTA per SM).  Both constants were
-// fitted on B200 to 27 timed (N, width) pairs from N = 32768 to 2^20, which
-// the model reproduces to 1 % (0.2 % on average).  Narrow chunks cut the last
-// wave's idle time, wide ones the per-CTA cost: the best widths are 8 at
-// N = 32768, 15 at 65536, 6 at 131072, 18 at 262144 and 32 from ~2^20 up.
-double n3_makespan(long long nb, int cols, int sms) {
+// The column-chunk width and launch order of the Newton-3 grid.  A CTA (row
+// group g, chunk k) costs a fixed 0.15 plus, per column block of its chunk, 1
+// (0.8 for the group's first 8 blocks, where the diagonal leaves warps idle),
+// in units of one column block's pair work; the CTAs are handed to the SMs in
+// launch order as SMs free up (list scheduling, one CTA per SM).  Both
+// constants were fitted on B200 to 27 timed (N, width) pairs from N = 32768 to
+// 2^20 in group-major order, which the model reproduces to 1 % (0.2 % on
+// average).  Narrow chunks cut the last wave's idle time, wide ones the
+// per-CTA cost; launching the longest CTAs first (the diagonal and partial
+// chunks last) leaves the short ones for the last wave.
+void n3_cta_costs(long long nb, int cols, std::vector<double>& cost) {
   constexpr double kCtaCost = 0.15, kDiagBlock = 0.8;
+  cost.clear();
+  for (long long r0 = 0; r0 < nb; r0 += kN3Warps) {
+    for (long long cs = r0; cs < nb; cs += cols) {
+      const long long ce = std::min(cs + (long long)cols, nb);
+      const long long diag = std::max(0LL, std::min(ce, r0 + kN3Warps) - cs);  // blocks < r0 + 8
+      cost.push_back(kCtaCost + kDiagBlock * (double)diag + (double)(ce - cs - diag));
+    }
+  }
+}
+
+void n3_launch_order(long long nb, int cols, std::vector<int>& order) {
+  std::vector<double> cost;
+  n3_cta_costs(nb, cols, cost);
+  order.resize(cost.size());
+  for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+}
+
+double n3_makespan(long long nb, int cols, int sms) {
+  std::vector<double> cost;
+  n3_cta_costs(nb, cols, cost);
+  std::stable_sort(cost.begin(), cost.end(), std::greater<double>());
   std::priority_queue<double, std::vector<double>, std::greater<double>> free_at;
   for (int i = 0; i < sms; ++i) free_at.push(0.0);
   double end = 0.0;
-  for (long long r0 = 0; r0 < nb; r0 += kN3Warps) {
-    for (long long cs = r0; cs < nb; cs += cols) {
-      const long long ce = std::min(cs + cols, nb);
-      const long long diag = std::max(0LL, std::min(ce, r0 + kN3Warps) - cs);  // blocks < r0 + 8
-      const double t = kCtaCost + kDiagBlock * (double)diag + (double)(ce - cs - diag);
-      const double start = free_at.top();
-      free_at.pop();
-      free_at.push(start + t);
-      end = std::max(end, start + t);
-    }
+  for (const double t : cost) {
+    const double start = free_at.top();
+    free_at.pop();
+    free_at.push(start + t);
+    end = std::max(end, start + t);
   }
   return end;
 }
@@ -1874,7 +1897,7 @@ cudaError_t configure_kernels() {
 
 cudaError_t launch_force_n3(int precision, int warps, double eps2, const IParticles& ip,
                             const JStream& js, const Epilogue& ep, double* scratch,
-                            long long scratch_len, cudaStream_t st) {
+                            long long scratch_len, const int* order, cudaStream_t st) {
   (void)scratch_len;
   if (ip.n <= 0 || js.ntiles <= 0) return cudaSuccess;
   N3Params p3;
@@ -1886,6 +1909,8 @@ cudaError_t launch_force_n3(int precision, int warps, double eps2, const IPartic
   p3.g1 = (int)((p3.nb + kN3Warps - 1) / kN3Warps);
   p3.act = scratch;
   p3.rea = scratch + (size_t)ctas * kN3Warps * 3 * kN3Block;
+  p3.order = order;
+  p3.slot = order ? order + ctas : nullptr;
   NBR_CHECKED_ONLY(p3.act_len = scratch_len;)
   const bool w2 = precision == kFP32C && warps == kN3F64Warps;
   const size_t smem = n3_smem_bytes(precision, precision == kFP32C ? warps : kN3F64Warps);
@@ -1896,6 +1921,12 @@ cudaError_t launch_force_n3(int precision, int warps, double eps2, const IPartic
       k_force_n3_f32c_w2<true><<<grid, block, smem, st>>>(ip, js, p3, 0.f, ep.err);
     else
       k_force_n3_f32c_w2<false><<<grid, block, smem, st>>>(ip, js, p3, (float)eps2, ep.err);
+  } else if (precision == kFP32C && !order) {
+    // no launch order: the range form over all row groups (group-major order)
+    if (eps2 == 0.0)
+      k_force_n3_f32c<true, true><<<grid, block, smem, st>>>(ip, js, p3, 0.f, ep.err);
+    else
+      k_force_n3_f32c<false, true><<<grid, block, smem, st>>>(ip, js, p3, (float)eps2, ep.err);
   } else if (precision == kFP32C) {
     if (eps2 == 0.0)
       k_force_n3_f32c<true, false><<<grid, block, smem, st>>>(ip, js, p3, 0.f, ep.err);

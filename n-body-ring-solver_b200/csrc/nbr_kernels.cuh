@@ -3,6 +3,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <vector>
 
 namespace nbr {
 
@@ -102,6 +103,12 @@ struct N3Params {
   int g0, g1;    // row groups [g0, g1) of this launch (all: 0, ceil(nb / kN3Warps))
   double* act;   // action partials [cta][row block][3][kN3Block]
   double* rea;   // reaction partials [cta][column block][3][kN3Block]
+  // Launch order of a whole-system launch: CTA blockIdx.x does (row group,
+  // chunk) number order[blockIdx.x] of the group-major numbering and writes
+  // its partial sums at index blockIdx.x; slot[] is the inverse (group-major
+  // number -> partial-sum index) for the reduction.  nullptr: identity.
+  const int* order;
+  const int* slot;
   NBR_CHECKED_FIELD(long long act_len)  // doubles from act (through rea's end)
   NBR_CHECKED_FIELD(long long dst_len)  // doubles of a slice reduction's destination
 };
@@ -125,10 +132,14 @@ __host__ __device__ inline int n3_chunks(long long nb, int cols, int g) {
 // device: the width whose grid a model of the launch finishes first (see
 // nbr_kernels.cu).  Memoized per (nb, SM count); a host function.
 int n3_cols(long long nb);
-// The model's finishing time of the Newton-3 grid for nb blocks in chunks of
-// `cols`, on `sms` SMs (one CTA each at a time), in units of one column
-// block's pair work.
+// The model's cost of every CTA of the Newton-3 grid for nb blocks in chunks
+// of `cols` (group-major order), in units of one column block's pair work.
+void n3_cta_costs(long long nb, int cols, std::vector<double>& cost);
+// The model's finishing time of that grid launched longest CTA first (ties in
+// group-major order) on `sms` SMs, one CTA each at a time.
 double n3_makespan(long long nb, int cols, int sms);
+// That launch order: order[launch index] = group-major CTA index.
+void n3_launch_order(long long nb, int cols, std::vector<int>& order);
 // CTAs of a Newton-3 launch and the doubles its partial sums need.
 inline long long n3_ctas(long long nb, int cols) {
   long long t = 0;
@@ -176,11 +187,12 @@ inline long long n3_slice_scratch_doubles(long long nb, int v, int V) {
 // One Newton-3 force evaluation over all n_pad receivers of ip against the
 // same particles in js (FP32C: their records; FP64: their x, y, z, m arrays),
 // with the epilogue ep: the pair kernel, then the per-particle reduction.
-// scratch holds n3_scratch_doubles(ceil(n / kN3Block)) doubles.
+// scratch holds n3_scratch_doubles(ceil(n / kN3Block)) doubles; order is the
+// grid's launch order (n3_launch_order, on the device).
 // FP32C: warps = kN3Warps (one warp per row block) or kN3F64Warps (two).
 cudaError_t launch_force_n3(int precision, int warps, double eps2, const IParticles& ip,
                             const JStream& js, const Epilogue& ep, double* scratch,
-                            long long scratch_len, cudaStream_t stream);
+                            long long scratch_len, const int* order, cudaStream_t stream);
 // Newton-3 partial accelerations (not G-scaled) of every particle from the
 // pairs of slice `slice` of `nslices` (n3_slice_groups): stored into dst[d *
 // ld + i] (i < n rounded up to 256), or added to it (accumulate); scratch
