@@ -556,21 +556,23 @@ __device__ __forceinline__ bool run_item_n3(const BatchParams& p, u64 EPS2, Ring
             const u64 y3 = mul2(y2, y);
             const u64 sj = mul2(y3, fma2(SA, pr, SBv));       // m_j (1 + 3e/2) y^3
             const u64 si = mul2(y3, fma2(AI[q], pr, BI[q]));  // m_i (1 + 3e/2) y^3
-            AX[q] = fma2(sj, dx, AX[q]);
-            AY[q] = fma2(sj, dy, AY[q]);
-            AZ[q] = fma2(sj, dz, AZ[q]);
+            // reaction first, and its shuffles before the sources' (as in
+            // k_force_n3_f32c: the faster schedule, +0.6 % here)
             RX = fma2(si, dx, RX);
             RY = fma2(si, dy, RY);
             RZ = fma2(si, dz, RZ);
+            AX[q] = fma2(sj, dx, AX[q]);
+            AY[q] = fma2(sj, dy, AY[q]);
+            AZ[q] = fma2(sj, dz, AZ[q]);
           }
+          RX = __shfl_sync(0xffffffffu, RX, from);
+          RY = __shfl_sync(0xffffffffu, RY, from);
+          RZ = __shfl_sync(0xffffffffu, RZ, from);
           sx = __shfl_sync(0xffffffffu, sx, from);
           sy = __shfl_sync(0xffffffffu, sy, from);
           sz = __shfl_sync(0xffffffffu, sz, from);
           sa = __shfl_sync(0xffffffffu, sa, from);
           sb = __shfl_sync(0xffffffffu, sb, from);
-          RX = __shfl_sync(0xffffffffu, RX, from);
-          RY = __shfl_sync(0xffffffffu, RY, from);
-          RZ = __shfl_sync(0xffffffffu, RZ, from);
         }
         // back at its own lane: the acceleration of source j is -sum m_i y^3 d
         if (NBR_IN((slot - p.rea) + 2 * kTile + j, p.rea_len, p.err)) {
