@@ -79,6 +79,12 @@ __device__ __forceinline__ void red_release_add_u64(unsigned long long* p, unsig
 // arrival is one release add and nothing is reset.  Returns false in every
 // thread of the CTA if the barrier did not complete within the limit or an
 // error was already recorded (the CTA then leaves the kernel).
+// Ordering: the CTA's writes precede thread 0's release add through the
+// bar.sync (a CTA-scope synchronization), and the acquire load that sees the
+// last arrival precedes the other threads' reads through the second bar.sync;
+// causality order is transitive, so no separate fence is needed (two
+// __threadfence() here cost 0.45 us per barrier).  The error word and the
+// timer are checked every 32 polls.
 __device__ bool grid_barrier(unsigned long long* bar, int* err, unsigned long long limit_ns,
                              unsigned long long k) {
   __shared__ int s_ok;
@@ -86,18 +92,18 @@ __device__ bool grid_barrier(unsigned long long* bar, int* err, unsigned long lo
   if (threadIdx.x == 0) {
     int ok = 1;
     const unsigned long long target = (k + 1) * gridDim.x;
-    __threadfence();
     red_release_add_u64(bar, 1ull);
     if (ld_acquire_u64(bar) < target) {
       const unsigned long long t0 = global_ns();
+      unsigned polls = 0;
       while (ld_acquire_u64(bar) < target) {
-        if (*reinterpret_cast<volatile int*>(err) != 0 || global_ns() - t0 > limit_ns) {
+        if ((++polls & 31u) == 0 &&
+            (*reinterpret_cast<volatile int*>(err) != 0 || global_ns() - t0 > limit_ns)) {
           ok = 0;
           break;
         }
       }
     }
-    __threadfence();
     if (!ok) record_error(err, kErrGridWait);
     s_ok = ok;
   }
