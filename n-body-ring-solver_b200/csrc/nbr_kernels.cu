@@ -1246,20 +1246,22 @@ __global__ void __launch_bounds__(kN3F64Warps * 32)
             if (EXCL) y = r2 > 0.0 ? y : 0.0;
             const double y3 = y * y * y;
             const double sj = ms * y3, si = mi[q] * y3;
-            AX[q] = fma(sj, dx, AX[q]);
-            AY[q] = fma(sj, dy, AY[q]);
-            AZ[q] = fma(sj, dz, AZ[q]);
+            // reaction first, and its shuffles before the sources': the faster
+            // schedule (+1.7 % at N = 262144), as in k_force_n3_f32c
             RX = fma(si, dx, RX);
             RY = fma(si, dy, RY);
             RZ = fma(si, dz, RZ);
+            AX[q] = fma(sj, dx, AX[q]);
+            AY[q] = fma(sj, dy, AY[q]);
+            AZ[q] = fma(sj, dz, AZ[q]);
           }
+          RX = __shfl_sync(0xffffffffu, RX, from);
+          RY = __shfl_sync(0xffffffffu, RY, from);
+          RZ = __shfl_sync(0xffffffffu, RZ, from);
           xs = __shfl_sync(0xffffffffu, xs, from);
           ys = __shfl_sync(0xffffffffu, ys, from);
           zs = __shfl_sync(0xffffffffu, zs, from);
           ms = __shfl_sync(0xffffffffu, ms, from);
-          RX = __shfl_sync(0xffffffffu, RX, from);
-          RY = __shfl_sync(0xffffffffu, RY, from);
-          RZ = __shfl_sync(0xffffffffu, RZ, from);
         }
         // back at its own lane: the force on source j is -sum m_i y^3 d
         myred[bt * 32 + lane] = -RX;
