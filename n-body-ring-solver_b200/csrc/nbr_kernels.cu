@@ -43,6 +43,7 @@
 #include <map>
 #include <mutex>
 #include <queue>
+#include <tuple>
 #include <vector>
 
 namespace nbr {
@@ -1871,6 +1872,81 @@ int n3_cols(long long nb) {
   return best;
 }
 
+namespace {
+// Modeled finishing time of the group-major grid of row groups [g0, g1) (the
+// cost model of n3_cta_costs; list scheduling in launch order).
+double n3_range_makespan(long long nb, int cols, int g0, int g1, int sms) {
+  constexpr double kCtaCost = 0.15, kDiagBlock = 0.8;
+  std::priority_queue<double, std::vector<double>, std::greater<double>> free_at;
+  for (int i = 0; i < sms; ++i) free_at.push(0.0);
+  double end = 0.0;
+  for (long long g = g0; g < g1; ++g) {
+    const long long r0 = g * kN3Warps;
+    for (long long cs = r0; cs < nb; cs += cols) {
+      const long long ce = std::min(cs + (long long)cols, nb);
+      const long long diag = std::max(0LL, std::min(ce, r0 + kN3Warps) - cs);
+      const double t = kCtaCost + kDiagBlock * (double)diag + (double)(ce - cs - diag);
+      const double start = free_at.top();
+      free_at.pop();
+      free_at.push(start + t);
+      end = std::max(end, start + t);
+    }
+  }
+  return end;
+}
+}  // namespace
+
+int n3_slice_cols(long long nb, int V) {
+  if (nb <= 1 || V < 1) return 1;
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
+    sms = 148;
+  static std::mutex mu;
+  static std::map<std::tuple<long long, int, int>, int> memo;
+  std::lock_guard<std::mutex> lock(mu);
+  const auto key = std::make_tuple(nb, V, sms);
+  const auto it = memo.find(key);
+  if (it != memo.end()) return it->second;
+  std::vector<int> worlds;
+  for (int W : {2, 4, 8})
+    if (W <= V) worlds.push_back(W);
+  if (V != 2 && V != 4 && V != 8) worlds.push_back(V);
+  // the ideal time per rank: the widest chunks' total cost (the least per-CTA
+  // cost) spread evenly over all SMs of the W ranks
+  double total = 0.0;
+  {
+    std::vector<double> cost;
+    n3_cta_costs(nb, kN3MaxCols, cost);
+    for (const double t : cost) total += t;
+  }
+  int best = kN3MaxCols;
+  double best_eff = -1.0;
+  for (int c = kN3MaxCols; c >= 1; --c) {
+    if (c < kN3MaxCols && n3_ctas(nb, c) > 64LL * sms * V) break;  // only more CTA cost
+    // worst-case efficiency over the world sizes: ideal time / slowest rank
+    double eff = 1e30;
+    for (const int W : worlds) {
+      double worst = 0.0;
+      for (int r = 0; r < W; ++r) {
+        const int v0 = (int)((long long)V * r / W), v1 = (int)((long long)V * (r + 1) / W);
+        if (v1 <= v0) continue;
+        int g0 = 0, g1 = 0, g = 0;
+        n3_slice_groups(nb, c, v0, V, &g0, &g);
+        n3_slice_groups(nb, c, v1 - 1, V, &g, &g1);
+        worst = std::max(worst, n3_range_makespan(nb, c, g0, g1, sms));
+      }
+      if (worst > 0.0) eff = std::min(eff, total / ((double)sms * W) / worst);
+    }
+    if (eff > best_eff * (1.0 + 1e-3)) {  // ties keep the wider chunk
+      best_eff = eff;
+      best = c;
+    }
+  }
+  memo[key] = best;
+  return best;
+}
+
 cudaError_t configure_kernels() {
   // The Newton-3 kernels need more than the default 48 KB of dynamic shared
   // memory; set once per device, outside any stream capture.
@@ -1978,7 +2054,7 @@ cudaError_t launch_n3_slices(int precision, int warps, double eps2, const IParti
   if (ip.n <= 0 || js.ntiles <= 0 || v1 <= v0) return cudaSuccess;
   N3Params p3{};
   p3.nb = (ip.n + kN3Block - 1) / kN3Block;
-  p3.cols = n3_cols(p3.nb);
+  p3.cols = n3_slice_cols(p3.nb, nslices);
   // one pair launch over the slices' consecutive row groups: a CTA's partial
   // sums depend on its (row group, chunk) only, so they equal those of
   // per-slice launches, with fewer partly filled waves

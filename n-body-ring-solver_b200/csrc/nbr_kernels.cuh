@@ -140,6 +140,13 @@ void n3_cta_costs(long long nb, int cols, std::vector<double>& cost);
 double n3_makespan(long long nb, int cols, int sms);
 // That launch order: order[launch index] = group-major CTA index.
 void n3_launch_order(long long nb, int cols, std::vector<int>& order);
+// Column blocks per CTA of the row-group slices of V (the multi-GPU partition
+// and the banded evaluation): the width whose slices the model finishes with
+// the best worst-case efficiency when W = 2, 4, 8 or V ranks (those <= V)
+// each launch their consecutive share of the slices (group-major order).
+// The same for every world size of one V, so the sums stay bit-identical
+// across world sizes.  Memoized per (nb, V, SM count); a host function.
+int n3_slice_cols(long long nb, int V);
 // CTAs of a Newton-3 launch and the doubles its partial sums need.
 inline long long n3_ctas(long long nb, int cols) {
   long long t = 0;
@@ -175,7 +182,7 @@ inline void n3_slice_groups(long long nb, int cols, int v, int V, int* g0, int* 
 }
 // Doubles of partial-sum scratch of slices [v0, v1) of V (one launch).
 inline long long n3_slices_scratch_doubles(long long nb, int v0, int v1, int V) {
-  const int cols = n3_cols(nb);
+  const int cols = n3_slice_cols(nb, V);
   int g0 = 0, g1 = 0, g = 0;
   n3_slice_groups(nb, cols, v0, V, &g0, &g);
   n3_slice_groups(nb, cols, v1 - 1, V, &g, &g1);
