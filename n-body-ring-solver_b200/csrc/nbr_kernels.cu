@@ -668,8 +668,9 @@ __global__ void __launch_bounds__(kSmallWarps * 32)
 // 1137-1561).  Particles form blocks of kN3Block = 256 (2 tiles).  A CTA of
 // kN3Warps warps owns row group g (row blocks 8g .. 8g+7, one per warp, 8
 // receivers per lane as in k_force_f32c) and a chunk of up to p3.cols column
-// blocks starting at the group's first block (n3_cols: 32, fewer on small
-// systems); the column tiles stream through the bulk-copy ring.  Warp a and column block c:
+// blocks (group g's chunks tile its column blocks 8g .. nb - 1; the width from
+// the grid model of n3_cols / n3_slice_cols); the column tiles stream through
+// the bulk-copy ring.  Warp a and column block c:
 //   c < a   nothing (the pair of blocks belongs to warp c);
 //   c == a  every ordered pair of the block, action only (the k_force_f32c body);
 //   c > a   each unordered pair once: the 32 sources of a batch sit one per

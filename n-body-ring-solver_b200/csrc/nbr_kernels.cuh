@@ -92,7 +92,7 @@ constexpr int kSmallWarps = 4;
 constexpr int kSmallNI = 4;
 // The Newton-3 kernels (ForceConfig ni = 3, FP32C and FP64): blocks of kN3Block
 // particles, kN3Warps row blocks per CTA (one per warp), up to `cols` column
-// blocks per CTA (n3_cols: fewer on small systems, for enough CTAs).
+// blocks per CTA (n3_cols, n3_slice_cols: at most kN3MaxCols).
 constexpr int kN3Warps = 8;
 constexpr int kN3F64Warps = 2 * kN3Warps;  // FP64: two warps per row block
 constexpr int kN3Block = 256;
