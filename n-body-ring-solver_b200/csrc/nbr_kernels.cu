@@ -1909,6 +1909,12 @@ int n3_slice_cols(long long nb, int V) {
   const auto key = std::make_tuple(nb, V, sms);
   const auto it = memo.find(key);
   if (it != memo.end()) return it->second;
+  // 32 waves or more per slice at the widest chunk: the last wave's idle time
+  // is negligible (and the model would simulate millions of CTAs)
+  if (n3_ctas(nb, kN3MaxCols) >= 32LL * sms * V) {
+    memo[key] = kN3MaxCols;
+    return kN3MaxCols;
+  }
   std::vector<int> worlds;
   for (int W : {2, 4, 8})
     if (W <= V) worlds.push_back(W);
