@@ -329,6 +329,14 @@ ForceConfig choose_config(nbr_ctx* c, int precision, double eps2, long long n_i,
     // best other kernel: FP32C +24 % at N = 262144 and +28 % at 2^20; FP64
     // +16 % at 16384, +20 % at 32768, +30 % at 262144, +33 % at 2^20).
     if (n_i >= kN3MinN && n_i <= kN3MaxN) dflt = ForceConfig{3, kN3Warps, 0};
+    // From 8192 up: the Newton-3 kernels where the grid model gives them a good
+    // last wave.  Their advantage followed the modeled grid efficiency on B200
+    // (N = 8192 .. 15360 in steps of 1024): efficiency >= 0.70, FP32C +28 to
+    // +31 % and FP64 +12 to +17 %; 0.60 - 0.63, FP32C +6 to +11 %, FP64 -0.2 to
+    // +3 %; <= 0.55, a loss.
+    else if (n_i >= 8192 &&
+             n3_grid_efficiency((n_i + kN3Block - 1) / kN3Block) >= (precision == kFP32C ? 0.60 : 0.65))
+      dflt = ForceConfig{3, kN3Warps, 0};
     else if (F) dflt = ForceConfig{1, F, 0};
     cfg = it != g_tune->end() ? it->second : dflt;
   }

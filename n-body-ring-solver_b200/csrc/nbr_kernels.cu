@@ -1954,6 +1954,18 @@ int n3_slice_cols(long long nb, int V) {
   return best;
 }
 
+double n3_grid_efficiency(long long nb) {
+  if (nb < 1) return 0.0;
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
+    sms = 148;
+  // one unit: a CTA's 8 warps against one column block; (row block, column
+  // block >= it) pairs / 8 units in all
+  const double units = (double)nb * (double)(nb + 1) / 2.0 / kN3Warps;
+  return units / (double)sms / n3_makespan(nb, n3_cols(nb), sms);
+}
+
 cudaError_t configure_kernels() {
   // The Newton-3 kernels need more than the default 48 KB of dynamic shared
   // memory; set once per device, outside any stream capture.

@@ -140,6 +140,10 @@ void n3_cta_costs(long long nb, int cols, std::vector<double>& cost);
 double n3_makespan(long long nb, int cols, int sms);
 // That launch order: order[launch index] = group-major CTA index.
 void n3_launch_order(long long nb, int cols, std::vector<int>& order);
+// The model's efficiency of the whole-system Newton-3 grid for nb blocks on
+// the current device: the pair work spread evenly over the SMs divided by the
+// grid's finishing time (1 at best).  A host function.
+double n3_grid_efficiency(long long nb);
 // Column blocks per CTA of the row-group slices of V (the multi-GPU partition
 // and the banded evaluation): the width whose slices the model finishes with
 // the best worst-case efficiency when W = 2, 4, 8 or V ranks (those <= V)
