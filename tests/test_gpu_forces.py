@@ -423,3 +423,21 @@ def test_newton3_kernel_fp64(ctx, nbr, oracle, n, eps2):
                 assert np.abs(got[k] - want[k]).max() <= 1e-11, k
     finally:
         ctx.set_force_config(FP64, 0)
+
+
+@pytest.mark.parametrize("n", [9216, 10240, 11264, 12288, 15360, 17408])
+def test_default_kernel_between_8k_and_18k(ctx, nbr, oracle, n):
+    """Sizes where the default switches between the large kernels and the
+    Newton-3 kernel by the grid model's efficiency (and one just above
+    16384): whichever it takes, every sampled receiver within the tolerances
+    against the extended-precision oracle, FP64 and FP32C."""
+    s = nbr.plummer(n, 31)
+    upload(ctx, s)
+    eps2 = 1e-6
+    idx = np.random.default_rng(n).choice(n, 256, replace=False)
+    ref = oracle.accel_subset(s["x"], s["y"], s["z"], s["m"], idx, eps2=eps2)
+    a64 = ctx.forces(FP64, eps2=eps2)
+    assert rel_err(a64[:, idx], ref).max() <= 1e-12
+    a32 = ctx.forces(FP32C, eps2=eps2)
+    e = rel_err(a32[:, idx], ref)
+    assert np.median(e) <= 1e-6 and e.max() <= 1e-4, (np.median(e), e.max())
