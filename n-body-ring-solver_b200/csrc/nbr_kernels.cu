@@ -1960,10 +1960,19 @@ double n3_grid_efficiency(long long nb) {
   if (cudaGetDevice(&dev) != cudaSuccess ||
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
     sms = 148;
+  const int cols = n3_cols(nb);  // before taking the lock (n3_cols has its own)
+  static std::mutex mu;
+  static std::map<std::pair<long long, int>, double> memo;  // the choice runs per evaluation
+  std::lock_guard<std::mutex> lock(mu);
+  const auto key = std::make_pair(nb, sms);
+  const auto it = memo.find(key);
+  if (it != memo.end()) return it->second;
   // one unit: a CTA's 8 warps against one column block; (row block, column
   // block >= it) pairs / 8 units in all
   const double units = (double)nb * (double)(nb + 1) / 2.0 / kN3Warps;
-  return units / (double)sms / n3_makespan(nb, n3_cols(nb), sms);
+  const double eff = units / (double)sms / n3_makespan(nb, cols, sms);
+  memo[key] = eff;
+  return eff;
 }
 
 cudaError_t configure_kernels() {
