@@ -1236,7 +1236,7 @@ __global__ void __launch_bounds__(kN3F64Warps * 32)
         const int j = bt * 32 + lane;
         double xs = sx[j], ys = sy[j], zs = sz[j], ms = sm[j];
         double RX = 0.0, RY = 0.0, RZ = 0.0;
-#pragma unroll 2
+#pragma unroll 1  // 3 % faster than unrolled by 2 or 4 (N = 262144)
         for (int step = 0; step < 32; ++step) {
 #pragma unroll
           for (int q = 0; q < NI; ++q) {
