@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(W * 32, 1) k_run_small_f64(const PersistArgs A
         zi[k] = real ? sz[i] : 0.0;
         ax[k] = ay[k] = az[k] = 0.0;
       }
-#pragma unroll 2
+#pragma unroll 4
       for (int j = warp * F + grp; j < n; j += S) {
         const double xj = sx[j], yj = sy[j], zj = sz[j], mj = sm[j];
 #pragma unroll
