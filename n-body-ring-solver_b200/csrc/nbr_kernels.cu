@@ -1808,16 +1808,56 @@ size_t n3_smem_bytes(int precision, int warps) {
 // average).  Narrow chunks cut the last wave's idle time, wide ones the
 // per-CTA cost; launching the longest CTAs first (the diagonal and partial
 // chunks last) leaves the short ones for the last wave.
-void n3_cta_costs(long long nb, int cols, std::vector<double>& cost) {
+namespace {
+// SM count of the current device (148 if it cannot be read).
+int device_sms() {
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
+    sms = 148;
+  return sms;
+}
+
+// Modeled cost of every CTA of row groups [g0, g1), group-major.
+void n3_cta_costs_range(long long nb, int cols, long long g0, long long g1,
+                        std::vector<double>& cost) {
   constexpr double kCtaCost = 0.15, kDiagBlock = 0.8;
   cost.clear();
-  for (long long r0 = 0; r0 < nb; r0 += kN3Warps) {
+  for (long long g = g0; g < g1; ++g) {
+    const long long r0 = g * kN3Warps;
     for (long long cs = r0; cs < nb; cs += cols) {
       const long long ce = std::min(cs + (long long)cols, nb);
       const long long diag = std::max(0LL, std::min(ce, r0 + kN3Warps) - cs);  // blocks < r0 + 8
       cost.push_back(kCtaCost + kDiagBlock * (double)diag + (double)(ce - cs - diag));
     }
   }
+}
+
+// Finishing time of CTAs of the given costs handed in that order to `sms`
+// SMs, each to the first SM free (list scheduling, one CTA per SM).
+double list_schedule(const std::vector<double>& cost, int sms) {
+  std::priority_queue<double, std::vector<double>, std::greater<double>> free_at;
+  for (int i = 0; i < sms; ++i) free_at.push(0.0);
+  double end = 0.0;
+  for (const double t : cost) {
+    const double start = free_at.top();
+    free_at.pop();
+    free_at.push(start + t);
+    end = std::max(end, start + t);
+  }
+  return end;
+}
+
+// Modeled finishing time of the group-major grid of row groups [g0, g1).
+double n3_range_makespan(long long nb, int cols, int g0, int g1, int sms) {
+  std::vector<double> cost;
+  n3_cta_costs_range(nb, cols, g0, g1, cost);
+  return list_schedule(cost, sms);
+}
+}  // namespace
+
+void n3_cta_costs(long long nb, int cols, std::vector<double>& cost) {
+  n3_cta_costs_range(nb, cols, 0, (nb + kN3Warps - 1) / kN3Warps, cost);
 }
 
 void n3_launch_order(long long nb, int cols, std::vector<int>& order) {
@@ -1832,24 +1872,12 @@ double n3_makespan(long long nb, int cols, int sms) {
   std::vector<double> cost;
   n3_cta_costs(nb, cols, cost);
   std::stable_sort(cost.begin(), cost.end(), std::greater<double>());
-  std::priority_queue<double, std::vector<double>, std::greater<double>> free_at;
-  for (int i = 0; i < sms; ++i) free_at.push(0.0);
-  double end = 0.0;
-  for (const double t : cost) {
-    const double start = free_at.top();
-    free_at.pop();
-    free_at.push(start + t);
-    end = std::max(end, start + t);
-  }
-  return end;
+  return list_schedule(cost, sms);
 }
 
 int n3_cols(long long nb) {
   if (nb <= 1) return 1;
-  int dev = 0, sms = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess ||
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
-    sms = 148;
+  const int sms = device_sms();
   static std::mutex mu;
   static std::map<std::pair<long long, int>, int> memo;
   std::lock_guard<std::mutex> lock(mu);
@@ -1873,36 +1901,10 @@ int n3_cols(long long nb) {
   return best;
 }
 
-namespace {
-// Modeled finishing time of the group-major grid of row groups [g0, g1) (the
-// cost model of n3_cta_costs; list scheduling in launch order).
-double n3_range_makespan(long long nb, int cols, int g0, int g1, int sms) {
-  constexpr double kCtaCost = 0.15, kDiagBlock = 0.8;
-  std::priority_queue<double, std::vector<double>, std::greater<double>> free_at;
-  for (int i = 0; i < sms; ++i) free_at.push(0.0);
-  double end = 0.0;
-  for (long long g = g0; g < g1; ++g) {
-    const long long r0 = g * kN3Warps;
-    for (long long cs = r0; cs < nb; cs += cols) {
-      const long long ce = std::min(cs + (long long)cols, nb);
-      const long long diag = std::max(0LL, std::min(ce, r0 + kN3Warps) - cs);
-      const double t = kCtaCost + kDiagBlock * (double)diag + (double)(ce - cs - diag);
-      const double start = free_at.top();
-      free_at.pop();
-      free_at.push(start + t);
-      end = std::max(end, start + t);
-    }
-  }
-  return end;
-}
-}  // namespace
 
 int n3_slice_cols(long long nb, int V) {
   if (nb <= 1 || V < 1) return 1;
-  int dev = 0, sms = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess ||
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
-    sms = 148;
+  const int sms = device_sms();
   static std::mutex mu;
   static std::map<std::tuple<long long, int, int>, int> memo;
   std::lock_guard<std::mutex> lock(mu);
@@ -1956,10 +1958,7 @@ int n3_slice_cols(long long nb, int V) {
 
 double n3_grid_efficiency(long long nb) {
   if (nb < 1) return 0.0;
-  int dev = 0, sms = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess ||
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
-    sms = 148;
+  const int sms = device_sms();
   const int cols = n3_cols(nb);  // before taking the lock (n3_cols has its own)
   static std::mutex mu;
   static std::map<std::pair<long long, int>, double> memo;  // the choice runs per evaluation
