@@ -243,6 +243,19 @@ int nbr_step_range(nbr_ctx* ctx, int precision, int scheme, size_t i0, size_t co
  * result does not depend on how the slices are spread over ranks. */
 int nbr_n3_slice_accel(nbr_ctx* ctx, int precision, double eps2, int slice_begin, int slice_end,
                        int nslices, double* dst, size_t ld);
+/* The Newton-3 grid the library plans for a system of n particles on a device
+ * of `sms` SMs (host only: no context or device needed).  The grid has one
+ * CTA per (row group of 8 blocks of 256 particles, chunk of column blocks);
+ * the chunk width and the launch order come from a list-scheduling model of
+ * the launch.  Outputs (any may be NULL): *cols, column blocks per CTA of the
+ * whole-system grid; *slice_cols, of its `nslices` row-group slices (the
+ * multi-GPU partition; nslices >= 1); *efficiency, the model's pair work
+ * spread evenly over the SMs / the grid's finishing time (1 at best); *ctas,
+ * the whole-system grid's CTA count; order[0 .. min(order_cap, *ctas) - 1],
+ * the launch order (launch index -> group-major CTA number, longest CTA
+ * first).  NBR_ERR_INVALID_ARG for n < 1, sms < 1 or nslices < 1. */
+int nbr_n3_grid_plan(size_t n, int sms, int nslices, int* cols, int* slice_cols,
+                     double* efficiency, long long* ctas, int* order, long long order_cap);
 int nbr_step_range_sum(nbr_ctx* ctx, int precision, int scheme, size_t i0, size_t count, double kick,
                        double drift, double G, const double* src, int nslices, size_t vstride,
                        size_t ld);

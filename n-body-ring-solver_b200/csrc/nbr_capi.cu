@@ -930,6 +930,25 @@ int nbr_step_range(nbr_ctx* c, int precision, int scheme, size_t i0, size_t coun
   return rc;
 }
 
+int nbr_n3_grid_plan(size_t n, int sms, int nslices, int* cols, int* slice_cols,
+                     double* efficiency, long long* ctas, int* order, long long order_cap) {
+  if (n < 1 || sms < 1 || nslices < 1)
+    return fail(nullptr, NBR_ERR_INVALID_ARG, "need n >= 1, sms >= 1, nslices >= 1");
+  const long long nb = ((long long)n + kN3Block - 1) / kN3Block;
+  const int c = n3_cols_for(nb, sms);
+  if (cols) *cols = c;
+  if (slice_cols) *slice_cols = n3_slice_cols_for(nb, nslices, sms);
+  if (efficiency) *efficiency = n3_grid_efficiency_for(nb, sms);
+  if (ctas) *ctas = n3_ctas(nb, c);
+  if (order && order_cap > 0) {
+    std::vector<int> o;
+    n3_launch_order(nb, c, o);
+    const size_t k = std::min((size_t)order_cap, o.size());
+    std::copy(o.begin(), o.begin() + (long)k, order);
+  }
+  return NBR_OK;
+}
+
 int nbr_n3_slice_accel(nbr_ctx* c, int precision, double eps2, int slice_begin, int slice_end,
                        int nslices, double* dst, size_t ld) {
   TraceRange trace_range("nbr_n3_slice_accel");

@@ -1875,9 +1875,13 @@ double n3_makespan(long long nb, int cols, int sms) {
   return list_schedule(cost, sms);
 }
 
-int n3_cols(long long nb) {
+int n3_cols(long long nb) { return n3_cols_for(nb, device_sms()); }
+int n3_slice_cols(long long nb, int V) { return n3_slice_cols_for(nb, V, device_sms()); }
+double n3_grid_efficiency(long long nb) { return n3_grid_efficiency_for(nb, device_sms()); }
+
+int n3_cols_for(long long nb, int sms) {
   if (nb <= 1) return 1;
-  const int sms = device_sms();
+  if (sms < 1) sms = 1;
   static std::mutex mu;
   static std::map<std::pair<long long, int>, int> memo;
   std::lock_guard<std::mutex> lock(mu);
@@ -1902,9 +1906,9 @@ int n3_cols(long long nb) {
 }
 
 
-int n3_slice_cols(long long nb, int V) {
+int n3_slice_cols_for(long long nb, int V, int sms) {
   if (nb <= 1 || V < 1) return 1;
-  const int sms = device_sms();
+  if (sms < 1) sms = 1;
   static std::mutex mu;
   static std::map<std::tuple<long long, int, int>, int> memo;
   std::lock_guard<std::mutex> lock(mu);
@@ -1956,10 +1960,10 @@ int n3_slice_cols(long long nb, int V) {
   return best;
 }
 
-double n3_grid_efficiency(long long nb) {
+double n3_grid_efficiency_for(long long nb, int sms) {
   if (nb < 1) return 0.0;
-  const int sms = device_sms();
-  const int cols = n3_cols(nb);  // before taking the lock (n3_cols has its own)
+  if (sms < 1) sms = 1;
+  const int cols = n3_cols_for(nb, sms);  // before taking the lock (it has its own)
   static std::mutex mu;
   static std::map<std::pair<long long, int>, double> memo;  // the choice runs per evaluation
   std::lock_guard<std::mutex> lock(mu);

@@ -144,6 +144,11 @@ void n3_launch_order(long long nb, int cols, std::vector<int>& order);
 // the current device: the pair work spread evenly over the SMs divided by the
 // grid's finishing time (1 at best).  A host function.
 double n3_grid_efficiency(long long nb);
+// n3_cols, n3_slice_cols and n3_grid_efficiency for a device of `sms` SMs
+// (host functions; no device needed).
+int n3_cols_for(long long nb, int sms);
+int n3_slice_cols_for(long long nb, int V, int sms);
+double n3_grid_efficiency_for(long long nb, int sms);
 // Column blocks per CTA of the row-group slices of V (the multi-GPU partition
 // and the banded evaluation): the width whose slices the model finishes with
 // the best worst-case efficiency when W = 2, 4, 8 or V ranks (those <= V)

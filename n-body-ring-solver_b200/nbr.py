@@ -113,6 +113,9 @@ def load(path: str = LIB_PATH) -> C.CDLL:
                                 C.c_void_p, _SZ], C.c_int),
         "nbr_step_range_sum": ([C.c_void_p, C.c_int, C.c_int, _SZ, _SZ, C.c_double, C.c_double,
                                 C.c_double, C.c_void_p, C.c_int, _SZ, _SZ], C.c_int),
+        "nbr_n3_grid_plan": ([_SZ, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                              C.POINTER(C.c_double), C.POINTER(C.c_longlong), C.POINTER(C.c_int),
+                              C.c_longlong], C.c_int),
         "nbr_state_pointers": ([C.c_void_p] + [C.POINTER(C.c_void_p)] * 6 + [C.POINTER(_SZ)], C.c_int),
         "nbr_state_changed": ([C.c_void_p], C.c_int),
         "nbr_snapshot_write_arrays": ([C.c_char_p, _SZ, _SZ, C.c_double] + [_D] * 10, C.c_int),
@@ -237,6 +240,24 @@ def batch_sizes(nsys: int, seed: int, nmin: int = 64, nmax: int = 4096) -> np.nd
     out = (_SZ * nsys)()
     _check(load().nbr_ic_batch_sizes(nsys, seed, nmin, nmax, out), "nbr_ic_batch_sizes")
     return np.array(out[:], dtype=np.int64)
+
+
+def n3_grid_plan(n: int, sms: int = 148, nslices: int = 8, with_order: bool = False) -> dict:
+    """The Newton-3 grid the library plans for n particles on `sms` SMs
+    (nbr_n3_grid_plan; host only)."""
+    cols, scols, ctas = C.c_int(), C.c_int(), C.c_longlong()
+    eff = C.c_double()
+    L = load()
+    _check(L.nbr_n3_grid_plan(n, sms, nslices, C.byref(cols), C.byref(scols), C.byref(eff),
+                              C.byref(ctas), None, 0), "nbr_n3_grid_plan")
+    out = {"cols": cols.value, "slice_cols": scols.value, "efficiency": eff.value,
+           "ctas": ctas.value}
+    if with_order:
+        buf = (C.c_int * ctas.value)()
+        _check(L.nbr_n3_grid_plan(n, sms, nslices, None, None, None, None, buf, ctas.value),
+               "nbr_n3_grid_plan")
+        out["order"] = np.array(buf[:], dtype=np.int64)
+    return out
 
 
 def system_seed(seed: int, s: int) -> int:

@@ -169,3 +169,53 @@ def test_cli_without_gpu_reports_and_fails():
         pytest.skip("a GPU is visible")
     out = subprocess.run([exe, "-N", "100", "-s", "1"], capture_output=True, text=True)
     assert out.returncode == 1 and "No GPU context" in out.stdout
+
+
+def _n3_costs(nb, cols):
+    """The grid model's CTA costs, group-major (a restatement of the model:
+    0.15 per CTA plus 1 per column block, 0.8 for a row group's first 8)."""
+    out = []
+    for r0 in range(0, nb, 8):
+        cs = r0
+        while cs < nb:
+            ce = min(cs + cols, nb)
+            diag = max(0, min(ce, r0 + 8) - cs)
+            out.append(0.15 + 0.8 * diag + (ce - cs - diag))
+            cs += cols
+    return out
+
+
+@pytest.mark.parametrize("n", [1, 300, 20000, 32768, 131072, 262144, 1048576])
+def test_n3_grid_plan_invariants(nbr, n):
+    """The Newton-3 grid plan (host only): widths within 1 .. 32, the CTA
+    count of that width, a launch order that is a permutation of the CTAs
+    with non-increasing modeled cost, an efficiency in (0, 1], and the same
+    answer on a second call."""
+    plan = nbr.n3_grid_plan(n, 148, 8, with_order=True)
+    assert 1 <= plan["cols"] <= 32 and 1 <= plan["slice_cols"] <= 32
+    nb = -(-n // 256)
+    cost = _n3_costs(nb, plan["cols"])
+    assert plan["ctas"] == len(cost)
+    order = plan["order"]
+    assert sorted(order.tolist()) == list(range(len(cost)))
+    c = np.array(cost)[order]
+    assert np.all(np.diff(c) <= 1e-12)
+    assert 0.0 < plan["efficiency"] <= 1.0 + 1e-9
+    again = nbr.n3_grid_plan(n, 148, 8, with_order=True)
+    assert again["cols"] == plan["cols"] and np.array_equal(again["order"], order)
+
+
+def test_n3_grid_plan_known_choices(nbr):
+    """The widths measured best on B200 (148 SMs): 28 columns for the whole
+    N = 262144 grid (a sweep of 24 .. 32 confirmed it), 31 for its 8
+    multi-GPU slices; 32 from about 2^20."""
+    assert nbr.n3_grid_plan(262144, 148, 8)["cols"] == 28
+    assert nbr.n3_grid_plan(262144, 148, 8)["slice_cols"] == 31
+    assert nbr.n3_grid_plan(1048576, 148, 8)["cols"] == 32
+
+
+def test_n3_grid_plan_rejects_bad_arguments(nbr):
+    L = nbr.load()
+    assert L.nbr_n3_grid_plan(0, 148, 8, None, None, None, None, None, 0) == 1
+    assert L.nbr_n3_grid_plan(1000, 0, 8, None, None, None, None, None, 0) == 1
+    assert L.nbr_n3_grid_plan(1000, 148, 0, None, None, None, None, None, 0) == 1
